@@ -1,0 +1,231 @@
+/*
+ * pennant_b200.h -- C ABI of the B200-native PENNANT hydro cycle.
+ *
+ * This is the drop-in boundary for the reference's Hydro::doCycle path
+ * (StanfordLegion/pennant-legion).  Each entry point names the reference
+ * interface it replaces (file:line within that project).  All signatures
+ * use plain C types: pointers, sizes, POD structs.  Every call returns a
+ * pnt_status (0 = success) and never exits the process; pnt_last_error()
+ * gives the message of the last failure on the calling thread.
+ *
+ * Ownership: host buffers passed in are owned by the caller and only read
+ * (or written, for downloads) during the call.  Device memory is owned by
+ * the library object that allocated it.  One CUDA stream per pnt_hydro;
+ * calls on one object are not thread-safe, distinct objects may be driven
+ * concurrently from different threads.
+ */
+#ifndef PENNANT_B200_H
+#define PENNANT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PNT_ABI_VERSION 1
+
+typedef int32_t pnt_status;
+enum {
+    PNT_OK = 0,
+    PNT_ERR_INVALID_ARG = 1,  /* bad pointer, size or value */
+    PNT_ERR_DECK = 2,         /* malformed .pnt deck (InputFile.cc:28-50, GenMesh.cc:89-127) */
+    PNT_ERR_BADSIDES = 3,     /* negative side volumes (Mesh.cc:1531-1550) */
+    PNT_ERR_CUDA = 4,         /* CUDA runtime failure */
+    PNT_ERR_UNSUPPORTED = 5,  /* feature outside this build (e.g. hex meshes) */
+    PNT_ERR_TIMEOUT = 6,      /* a bounded device-side wait gave up */
+    PNT_ERR_NOMEM = 7,        /* host or device allocation failed */
+    PNT_ERR_NO_DEVICE = 8,    /* no CUDA device, or the kernels are not loadable */
+    PNT_ERR_STATE = 9         /* call not valid in the object's current state */
+};
+
+const char* pnt_status_string(pnt_status st);
+/* Message of the last failing call on this thread ("" if none). */
+const char* pnt_last_error(void);
+int32_t pnt_abi_version(void);
+
+/* ------------------------------------------------------------------ */
+/* Input deck: replaces InputFile (InputFile.hh:21-42, InputFile.cc:24-104) */
+/* ------------------------------------------------------------------ */
+typedef struct pnt_deck pnt_deck;
+
+/* InputFile::InputFile(filename): `key value...` lines, '#' comments,
+ * duplicate key is an error (PNT_ERR_DECK). */
+pnt_status pnt_deck_load(const char* path, pnt_deck** out);
+/* Same, from the deck's text in memory. */
+pnt_status pnt_deck_parse(const char* text, pnt_deck** out);
+/* Set or replace one key (the value is the text after the key). */
+pnt_status pnt_deck_set(pnt_deck* deck, const char* key, const char* value);
+int32_t pnt_deck_has(const pnt_deck* deck, const char* key);
+/* InputFile::getInt / getDouble / getString / getDoubleList (InputFile.cc:63-104) */
+int32_t pnt_deck_get_int(const pnt_deck* deck, const char* key, int32_t dflt);
+double pnt_deck_get_double(const pnt_deck* deck, const char* key, double dflt);
+/* Copies the first token (or dflt) into buf; returns its length. */
+int32_t pnt_deck_get_string(const pnt_deck* deck, const char* key, const char* dflt,
+                            char* buf, size_t buflen);
+/* Returns the number of values (written up to maxn), or -1 if absent. */
+int32_t pnt_deck_get_double_list(const pnt_deck* deck, const char* key, double* out,
+                                 int32_t maxn);
+void pnt_deck_destroy(pnt_deck* deck);
+
+/* ------------------------------------------------------------------ */
+/* Mesh: replaces Mesh(inp, numpcs) + GenMesh (Mesh.cc:211-652,        */
+/* GenMesh.cc:87-129, 790-1282) for a single piece, reference numbering */
+/* ------------------------------------------------------------------ */
+typedef struct pnt_mesh pnt_mesh;
+
+/* Connectivity in the reference's numbering: zones, sides 4z+k (rect),
+ * points j*(nzx+1)+i (rect).  Sides of a zone are contiguous and circulate
+ * (mapsp2[s] == mapsp1[mapss4[s]]).  px is double2 interleaved (x, y). */
+typedef struct {
+    int32_t nump, numz, nums;
+    const double* px;        /* [2*nump] initial point coordinates */
+    const int32_t* znump;    /* [numz]   sides (= points) per zone, 3 or 4 */
+    const int32_t* mapsp1;   /* [nums]   side -> first point  (FID_MAPSP1) */
+    const int32_t* mapsp2;   /* [nums]   side -> second point (FID_MAPSP2) */
+    const int32_t* mapsz;    /* [nums]   side -> zone         (FID_MAPSZ)  */
+    const int32_t* mapss3;   /* [nums]   previous side in zone (FID_MAPSS3) */
+    const int32_t* mapss4;   /* [nums]   next side in zone     (FID_MAPSS4) */
+} pnt_mesh_desc;
+
+/* GenMesh::generate{Points,Zones,Sides}Parallel for meshtype rect or pie
+ * (GenMesh.cc:528-665) with one piece.  meshtype hex: PNT_ERR_UNSUPPORTED
+ * (the reference's parallel hex generator asserts, GenMesh.cc:875-896). */
+pnt_status pnt_mesh_generate(const pnt_deck* deck, pnt_mesh** out);
+/* Mesh from caller-provided connectivity (validated; copied). */
+pnt_status pnt_mesh_create(const pnt_mesh_desc* desc, pnt_mesh** out);
+/* Pointers stay owned by the mesh and valid until pnt_mesh_destroy. */
+pnt_status pnt_mesh_describe(const pnt_mesh* mesh, pnt_mesh_desc* out);
+/* Point -> corner CSR used by the deterministic force/mass gather:
+ * sides[offsets[p] .. offsets[p+1]) are the sides s with mapsp1[s] == p in
+ * ascending order (the serial summation order of Hydro.cc:1100-1116,
+ * :1175-1192). offsets has nump+1 entries. */
+pnt_status pnt_mesh_point_corners(const pnt_mesh* mesh, const int32_t** offsets,
+                                  const int32_t** sides);
+void pnt_mesh_destroy(pnt_mesh* mesh);
+
+/* ------------------------------------------------------------------ */
+/* Parameters: deck keys and defaults of Driver (Driver.cc:78-87),       */
+/* Hydro (Hydro.cc:206-214), PolyGas (PolyGas.cc:57-60), TTS             */
+/* (TTS.cc:45-48), QCS (QCS.cc:83-86), HydroBC planes (Hydro.cc:220-225) */
+/* ------------------------------------------------------------------ */
+#define PNT_MAX_BC 16
+
+enum { PNT_PREC_FP64 = 0, PNT_PREC_MIXED = 1 };
+
+typedef struct {
+    /* Driver */
+    int32_t cstop, dtreport;
+    double tstop, dtmax, dtinit, dtfac;
+    /* Hydro */
+    double cfl, cflv, rinit, einit, rinitsub, einitsub, uinitradial;
+    int32_t has_subregion;
+    double subregion[4];
+    int32_t nbcx, nbcy;
+    double bcx[PNT_MAX_BC], bcy[PNT_MAX_BC];
+    /* PolyGas */
+    double gamma, pgas_ssmin;
+    /* TTS */
+    double alfa, tts_ssmin;
+    /* QCS */
+    double qgamma, q1, q2;
+    /* Project-only keys (ignored by the reference): arithmetic of the
+     * side pass, cycles per captured CUDA graph in pnt_hydro_run. */
+    int32_t precision;
+    int32_t graph_cycles;
+    int32_t reserved[14];
+} pnt_params;
+
+pnt_status pnt_params_default(pnt_params* out);
+/* Reads every key above from the deck (missing keys keep defaults);
+ * "precision fp64|mixed" and "graphcycles N" are the project-only keys. */
+pnt_status pnt_params_from_deck(const pnt_deck* deck, pnt_params* out);
+
+/* ------------------------------------------------------------------ */
+/* Hydro on one GPU: replaces Hydro(inp, mesh) + Hydro::init()           */
+/* (Hydro.cc:200-339) and the Driver loop around Hydro::doCycle          */
+/* (Driver.cc:102-187, Hydro.cc:342-983)                                 */
+/* ------------------------------------------------------------------ */
+typedef struct pnt_hydro pnt_hydro;
+
+typedef struct {
+    int32_t cycle;      /* completed cycles */
+    int32_t done;       /* 1 once cycle >= cstop, time >= tstop, or error */
+    pnt_status status;  /* PNT_ERR_BADSIDES after negative side volumes */
+    int32_t nbad;       /* negative side count behind that error */
+    double time;        /* simulation time after the last completed cycle */
+    double dt;          /* dt used by the last completed cycle */
+    double dtrec;       /* hydro-recommended dt (Hydro::calcDtTask) */
+    double dtnew;       /* Courant limit (calcDtNewTask) of the last cycle */
+    double dvovmax;     /* max |dV/V| (calcDvolTask) of the last cycle */
+} pnt_scalars;
+
+/* Allocates device state on `device`, uploads the mesh and runs
+ * Hydro::init (subregion, zm, zetot, radial velocity). */
+pnt_status pnt_hydro_create(const pnt_mesh* mesh, const pnt_params* params, int32_t device,
+                            pnt_hydro** out);
+void pnt_hydro_destroy(pnt_hydro* hydro);
+
+/* One iteration of Driver::run: calcGlobalDt (Driver.cc:213-245),
+ * Hydro::doCycle, time/cycle update; blocks until done.  Stops (no-op)
+ * once done, as the predicated reference does (Driver.cc:140-144). */
+pnt_status pnt_hydro_cycle(pnt_hydro* hydro, pnt_scalars* out);
+
+/* Report callback, called at cycle 1 and every dtreport cycles with the
+ * state of Driver::reportMeasurementTask (Driver.cc:329-347). */
+typedef void (*pnt_report_fn)(const pnt_scalars* s, double wall_us, void* user);
+
+/* Runs up to max_cycles more cycles (<= 0: until cstop/tstop) as replays
+ * of a captured CUDA graph; the host only synchronises at report points. */
+pnt_status pnt_hydro_run(pnt_hydro* hydro, int32_t max_cycles, pnt_report_fn report,
+                         void* user, pnt_scalars* out);
+/* Enqueues `ncycles` cycles on the object's stream without waiting
+ * (graph replay); read the result with pnt_hydro_get_scalars. */
+pnt_status pnt_hydro_enqueue(pnt_hydro* hydro, int32_t ncycles);
+pnt_status pnt_hydro_synchronize(pnt_hydro* hydro);
+pnt_status pnt_hydro_get_scalars(pnt_hydro* hydro, pnt_scalars* out);
+
+/* Instrumentation (the role of the reference's TimingLauncher,
+ * Driver.cc:117-168): runs `ncycles` cycles launching each pass separately
+ * with CUDA events around it and writes the mean milliseconds of pass i to
+ * kernel_ms[i] for i < nkernels (0 pass A zone predictor, 1 pass B point
+ * update, 2 pass C zone corrector, 3 finalize). */
+pnt_status pnt_hydro_time_kernels(pnt_hydro* hydro, int32_t ncycles, double* kernel_ms,
+                                  int32_t nkernels);
+/* Enqueues `ncycles` cycles (graph replay) between two CUDA events on the
+ * object's stream, waits, and returns the elapsed device milliseconds. */
+pnt_status pnt_hydro_time_cycles(pnt_hydro* hydro, int32_t ncycles, double* elapsed_ms);
+
+/* Field ids for upload/download, reference numbering and field names
+ * (Mesh.cc:258-423).  double2 fields are interleaved (x, y). */
+enum {
+    PNT_FIELD_PX = 0,     /* double2 [nump] point position */
+    PNT_FIELD_PU = 1,     /* double2 [nump] point velocity */
+    PNT_FIELD_ZR = 2,     /* double  [numz] density */
+    PNT_FIELD_ZE = 3,     /* double  [numz] specific internal energy */
+    PNT_FIELD_ZP = 4,     /* double  [numz] half-step pressure of the last cycle */
+    PNT_FIELD_ZM = 5,     /* double  [numz] zone mass */
+    PNT_FIELD_ZETOT = 6,  /* double  [numz] zone total internal energy */
+    PNT_FIELD_ZVOL = 7,   /* double  [numz] zone volume (RZ, per radian) */
+    PNT_FIELD_ZWRATE = 8, /* double  [numz] work rate */
+    PNT_FIELD_SMF = 9,    /* double  [nums] side mass fraction (constant) */
+    PNT_FIELD_COUNT = 10
+};
+/* bytes must equal the field's size (element count x element size). */
+pnt_status pnt_hydro_download(pnt_hydro* hydro, int32_t field, void* host_dst, size_t bytes);
+pnt_status pnt_hydro_upload(pnt_hydro* hydro, int32_t field, const void* host_src, size_t bytes);
+/* Device address of the current copy of a field (valid until the next
+ * cycle swaps the point buffers) and the object's cudaStream_t. */
+pnt_status pnt_hydro_device_ptr(pnt_hydro* hydro, int32_t field, void** dptr);
+pnt_status pnt_hydro_stream(pnt_hydro* hydro, void** cuda_stream);
+
+/* Output writers: WriteXY::write (WriteXY.cc:28-52) and ExportGold::write
+ * (ExportGold.cc:31-307) of the current state. */
+pnt_status pnt_hydro_write_xy(pnt_hydro* hydro, const char* path);
+pnt_status pnt_hydro_write_gold(pnt_hydro* hydro, const char* basename);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PENNANT_B200_H */

@@ -1,0 +1,625 @@
+// hydro.cu -- the pnt_hydro object: device state of one mesh on one GPU,
+// Hydro::init, the cycle driver with CUDA-graph replay, field transfer and
+// the output writers.  C ABI in include/pennant_b200.h.
+#include "hydro_dev.h"
+#include "pnt_internal.h"
+
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <new>
+#include <vector>
+
+using namespace pnt;
+
+namespace {
+
+#define CUDA_TRY(expr)                                                                  \
+    do {                                                                                \
+        const cudaError_t e_ = (expr);                                                  \
+        if (e_ != cudaSuccess)                                                          \
+            return fail(PNT_ERR_CUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_),  \
+                        __FILE__, __LINE__);                                            \
+    } while (0)
+
+// Makes `dev` current for the scope and restores the caller's device.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int now = -1;
+        if (prev >= 0 && cudaGetDevice(&now) == cudaSuccess && now != prev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+struct pnt_hydro {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    pnt_params params{};
+    HydroConst hc{};
+    DevArrays a{};
+    Ctl* ctl_host = nullptr;   // pinned mirror of the device Ctl
+    std::vector<void*> allocs;
+    // host copies needed by the output writers
+    std::vector<int32_t> znump, mapsp1;
+    int32_t nump = 0, numz = 0, nums = 0;
+    // captured CUDA graph of graph_cycles cycles
+    cudaGraphExec_t graph = nullptr;
+    int graph_cycles = 0;
+
+    ~pnt_hydro() {
+        DeviceGuard dg(device);
+        if (graph) cudaGraphExecDestroy(graph);
+        for (void* p : allocs) cudaFree(p);
+        if (ctl_host) cudaFreeHost(ctl_host);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    template <typename T>
+    pnt_status alloc(T** out, size_t count) {
+        void* p = nullptr;
+        const cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(e == cudaErrorMemoryAllocation ? PNT_ERR_NOMEM : PNT_ERR_CUDA,
+                        "cudaMalloc of %zu bytes: %s", count * sizeof(T), cudaGetErrorString(e));
+        }
+        allocs.push_back(p);
+        *out = static_cast<T*>(p);
+        return PNT_OK;
+    }
+
+    pnt_status launch_cycles(int n) {
+        for (int i = 0; i < n; ++i) {
+            const cudaError_t e = launch_cycle_fp64(a, hc, stream);
+            if (e != cudaSuccess) return fail(PNT_ERR_CUDA, "cycle launch: %s", cudaGetErrorString(e));
+        }
+        return PNT_OK;
+    }
+
+    pnt_status ensure_graph() {
+        if (graph) return PNT_OK;
+        graph_cycles = params.graph_cycles > 0 ? params.graph_cycles : 16;
+        cudaGraph_t g = nullptr;
+        CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        for (int i = 0; i < graph_cycles; ++i) {
+            const cudaError_t e = launch_cycle_fp64(a, hc, stream);
+            if (e != cudaSuccess) {
+                cudaStreamEndCapture(stream, &g);
+                if (g) cudaGraphDestroy(g);
+                return fail(PNT_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+            }
+        }
+        CUDA_TRY(cudaStreamEndCapture(stream, &g));
+        const cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            graph = nullptr;
+            return fail(PNT_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+        }
+        return PNT_OK;
+    }
+
+    // Enqueue n cycles: whole graphs, then single-cycle launches.
+    pnt_status enqueue(int n) {
+        pnt_status st = ensure_graph();
+        if (st) return st;
+        while (n >= graph_cycles) {
+            CUDA_TRY(cudaGraphLaunch(graph, stream));
+            n -= graph_cycles;
+        }
+        return launch_cycles(n);
+    }
+
+    pnt_status fetch_ctl() {
+        CUDA_TRY(cudaMemcpyAsync(ctl_host, a.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        return PNT_OK;
+    }
+
+    void scalars(pnt_scalars* out) const {
+        if (!out) return;
+        out->cycle = ctl_host->cycle;
+        out->done = ctl_host->done;
+        out->status = ctl_host->status;
+        out->nbad = ctl_host->nbad;
+        out->time = ctl_host->time;
+        out->dt = ctl_host->dtlast;
+        out->dtrec = ctl_host->dtrec;
+        out->dtnew = ctl_host->dtnew;
+        out->dvovmax = ctl_host->dvovmax;
+    }
+
+    pnt_status set_stop_at(int32_t stop_at) {
+        CUDA_TRY(cudaMemcpyAsync(&a.ctl->stop_at, &stop_at, sizeof(int32_t), cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        ctl_host->stop_at = stop_at;
+        return PNT_OK;
+    }
+};
+
+namespace {
+
+struct FieldInfo {
+    void* dev;
+    size_t bytes;
+};
+
+FieldInfo field_info(pnt_hydro* h, int32_t field, int cur) {
+    const size_t np = (size_t)h->nump, nz = (size_t)h->numz, ns = (size_t)h->nums;
+    switch (field) {
+        case PNT_FIELD_PX: return {h->a.px[cur], np * sizeof(double2)};
+        case PNT_FIELD_PU: return {h->a.pu[cur], np * sizeof(double2)};
+        case PNT_FIELD_ZR: return {h->a.zr, nz * sizeof(double)};
+        case PNT_FIELD_ZE: return {h->a.ze, nz * sizeof(double)};
+        case PNT_FIELD_ZP: return {h->a.zp, nz * sizeof(double)};
+        case PNT_FIELD_ZM: return {h->a.zm, nz * sizeof(double)};
+        case PNT_FIELD_ZETOT: return {h->a.zetot, nz * sizeof(double)};
+        case PNT_FIELD_ZVOL: return {h->a.zvol, nz * sizeof(double)};
+        case PNT_FIELD_ZWRATE: return {h->a.zwrate, nz * sizeof(double)};
+        case PNT_FIELD_SMF: return {const_cast<double*>(h->a.smf), ns * sizeof(double)};
+        default: return {nullptr, 0};
+    }
+}
+
+// Hydro::init (Hydro.cc:241-339) and the constants of the cycle.
+pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
+    const int64_t np = m.nump, nz = m.numz, ns = m.nums;
+    HydroConst& c = h->hc;
+    c.cfl = p.cfl;
+    c.cflv = p.cflv;
+    c.gm1 = p.gamma - 1.;
+    c.ssmin2 = std::max(p.pgas_ssmin * p.pgas_ssmin, 1.e-99);
+    c.alfa = p.alfa;
+    c.tts_ssmin = p.tts_ssmin;
+    c.gammap1 = p.qgamma + 1.0;
+    c.q1 = p.q1;
+    c.q2 = p.q2;
+    c.dtmax = p.dtmax;
+    c.dtinit = p.dtinit;
+    c.dtfac = p.dtfac;
+    c.tstop = p.tstop;
+    c.cstop = p.cstop;
+    c.nbc = p.nbcx + p.nbcy;
+    if (c.nbc > kMaxBC) return fail(PNT_ERR_UNSUPPORTED, "more than %d boundary planes", kMaxBC);
+
+    // Boundary planes in deck order, bcx then bcy (Hydro.cc:220-225); a
+    // point belongs to a plane when its coordinate is within 1e-12 of it
+    // (HydroBC.cc:63-144, 222-326).
+    std::vector<uint16_t> bcmask(np, 0);
+    const double eps = 1.e-12;
+    for (int b = 0; b < c.nbc; ++b) {
+        const bool xplane = b < p.nbcx;
+        const double bound = xplane ? p.bcx[b] : p.bcy[b - p.nbcx];
+        c.vfix[b][0] = xplane ? 1. : 0.;
+        c.vfix[b][1] = xplane ? 0. : 1.;
+        for (int64_t q = 0; q < np; ++q) {
+            const double coord = xplane ? m.px[2 * q] : m.px[2 * q + 1];
+            if (fabs(coord - bound) < eps) bcmask[q] |= (uint16_t)(1u << b);
+        }
+    }
+
+    std::vector<double> zr(nz, p.rinit), ze(nz, p.einit), zwrate(nz, 0.), zm(nz), zetot(nz);
+    if (p.has_subregion) {   // initSubrgnTask (Hydro.cc:1738-1762)
+        const double* sr = p.subregion;
+        for (int64_t z = 0; z < nz; ++z) {
+            const double zxx = m.zx[2 * z], zxy = m.zx[2 * z + 1];
+            if (zxx > (sr[0] - eps) && zxx < (sr[1] + eps) && zxy > (sr[2] - eps) && zxy < (sr[3] + eps)) {
+                zr[z] = p.rinitsub;
+                ze[z] = p.einitsub;
+            }
+        }
+    }
+    for (int64_t z = 0; z < nz; ++z) {   // initHydroTask (Hydro.cc:1765-1784)
+        zm[z] = zr[z] * m.zvol[z];
+        zetot[z] = ze[z] * zm[z];
+    }
+    std::vector<double> pu(2 * np, 0.);
+    if (p.uinitradial != 0.) {   // initRadialVelTask (Hydro.cc:1787-1807)
+        for (int64_t q = 0; q < np; ++q) {
+            const double x = m.px[2 * q], y = m.px[2 * q + 1];
+            const double pmag = sqrt(x * x + y * y);
+            if (pmag > eps) {
+                const double rinv = 1. / pmag;
+                pu[2 * q] = (x * p.uinitradial) * rinv;
+                pu[2 * q + 1] = (y * p.uinitradial) * rinv;
+            }
+        }
+    }
+
+    DevArrays& a = h->a;
+    a.nump = (int32_t)np;
+    a.numz = (int32_t)nz;
+    a.nums = (int32_t)ns;
+    a.quads = m.all_quads ? 1 : 0;
+    int32_t *zfirst, *znump, *mapsp1, *poff, *pcorner;
+    double* smf;
+    uint16_t* mask;
+    const int64_t nzb = zone_blocks((int32_t)nz);
+    pnt_status st = PNT_OK;
+    if ((st = h->alloc(&zfirst, nz)) || (st = h->alloc(&znump, nz)) || (st = h->alloc(&mapsp1, ns)) ||
+        (st = h->alloc(&smf, ns)) || (st = h->alloc(&poff, np + 1)) || (st = h->alloc(&pcorner, ns)) ||
+        (st = h->alloc(&mask, np)) || (st = h->alloc(&a.px[0], np)) || (st = h->alloc(&a.px[1], np)) ||
+        (st = h->alloc(&a.pu[0], np)) || (st = h->alloc(&a.pu[1], np)) || (st = h->alloc(&a.zm, nz)) ||
+        (st = h->alloc(&a.zr, nz)) || (st = h->alloc(&a.ze, nz)) || (st = h->alloc(&a.zetot, nz)) ||
+        (st = h->alloc(&a.zwrate, nz)) || (st = h->alloc(&a.zvol, nz)) || (st = h->alloc(&a.zp, nz)) ||
+        (st = h->alloc(&a.cmass, ns)) || (st = h->alloc(&a.cforce, ns)) || (st = h->alloc(&a.sftot, ns)) ||
+        (st = h->alloc(&a.part_dtnew, nzb)) || (st = h->alloc(&a.part_badA, nzb)) ||
+        (st = h->alloc(&a.part_dvov, nzb)) || (st = h->alloc(&a.part_badC, nzb)) ||
+        (st = h->alloc(&a.ctl, 1)))
+        return st;
+    a.zfirst = zfirst;
+    a.znump = znump;
+    a.mapsp1 = mapsp1;
+    a.smf = smf;
+    a.poff = poff;
+    a.pcorner = pcorner;
+    a.bcmask = mask;
+
+    // Driver::run start: time 0, cycle 0 and calcGlobalDt for cycle 0
+    // (Driver.cc:213-245).
+    Ctl ctl{};
+    double dt = p.dtmax;
+    if (p.dtinit < dt) dt = p.dtinit;
+    if ((p.tstop - 0.) < dt) dt = p.tstop - 0.;
+    ctl.dt = dt;
+    ctl.cycle = 0;
+    ctl.time = 0.;
+    ctl.done = (p.cstop <= 0 || !(0. < p.tstop)) ? 1 : 0;
+    ctl.stop_at = INT_MAX;
+
+    cudaStream_t s = h->stream;
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+    };
+    cudaError_t e = cudaSuccess;
+    if ((e = up(zfirst, m.zfirst.data(), nz * 4)) || (e = up(znump, m.znump.data(), nz * 4)) ||
+        (e = up(mapsp1, m.mapsp1.data(), ns * 4)) || (e = up(smf, m.smf.data(), ns * 8)) ||
+        (e = up(poff, m.poff.data(), (np + 1) * 4)) || (e = up(pcorner, m.pcorner.data(), ns * 4)) ||
+        (e = up(mask, bcmask.data(), np * 2)) || (e = up(a.px[0], m.px.data(), np * 16)) ||
+        (e = up(a.pu[0], pu.data(), np * 16)) || (e = up(a.zm, zm.data(), nz * 8)) ||
+        (e = up(a.zr, zr.data(), nz * 8)) || (e = up(a.ze, ze.data(), nz * 8)) ||
+        (e = up(a.zetot, zetot.data(), nz * 8)) || (e = up(a.zwrate, zwrate.data(), nz * 8)) ||
+        (e = up(a.zvol, m.zvol.data(), nz * 8)) || (e = up(a.ctl, &ctl, sizeof(Ctl))))
+        return fail(PNT_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
+    if ((e = cudaMemsetAsync(a.zp, 0, nz * 8, s)) || (e = cudaMemsetAsync(a.px[1], 0, np * 16, s)) ||
+        (e = cudaMemsetAsync(a.pu[1], 0, np * 16, s)))
+        return fail(PNT_ERR_CUDA, "memset: %s", cudaGetErrorString(e));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    *h->ctl_host = ctl;
+    return PNT_OK;
+}
+
+pnt_status write_xy(const char* path, const std::vector<double>& zr, const std::vector<double>& ze,
+                    const std::vector<double>& zp) {
+    FILE* f = fopen(path, "w");
+    if (!f) return fail(PNT_ERR_INVALID_ARG, "cannot open %s", path);
+    const std::vector<double>* v[3] = {&zr, &ze, &zp};
+    const char* nm[3] = {"zr", "ze", "zp"};
+    for (int k = 0; k < 3; ++k) {
+        fprintf(f, "#  %s\n", nm[k]);
+        for (size_t z = 0; z < v[k]->size(); ++z) fprintf(f, "%5d%18.8e\n", (int)z + 1, (*v[k])[z]);
+    }
+    fclose(f);
+    return PNT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+pnt_status pnt_hydro_create(const pnt_mesh* mesh, const pnt_params* params, int32_t device, pnt_hydro** out) {
+    if (!mesh || !params || !out) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    if (params->precision != PNT_PREC_FP64 && params->precision != PNT_PREC_MIXED)
+        return fail(PNT_ERR_INVALID_ARG, "unknown precision %d", params->precision);
+    if (params->precision == PNT_PREC_MIXED)
+        return fail(PNT_ERR_UNSUPPORTED, "precision mixed is not available in this build");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return fail(PNT_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev) return fail(PNT_ERR_INVALID_ARG, "device %d out of range", device);
+    DeviceGuard dg(device);
+    pnt_hydro* h = new (std::nothrow) pnt_hydro();
+    if (!h) return fail(PNT_ERR_NOMEM, "out of memory");
+    h->device = device;
+    h->params = *params;
+    pnt_status st = PNT_OK;
+    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&h->ctl_host, sizeof(Ctl));
+    if (e != cudaSuccess) {
+        delete h;
+        return fail(PNT_ERR_CUDA, "stream/host alloc: %s", cudaGetErrorString(e));
+    }
+    const Mesh& m = mesh->m;
+    h->nump = m.nump;
+    h->numz = m.numz;
+    h->nums = m.nums;
+    try {
+        h->znump = m.znump;
+        h->mapsp1 = m.mapsp1;
+        st = init_hydro(h, m, *params);
+    } catch (const std::bad_alloc&) {
+        st = fail(PNT_ERR_NOMEM, "out of host memory");
+    }
+    if (st) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return PNT_OK;
+}
+
+void pnt_hydro_destroy(pnt_hydro* h) { delete h; }
+
+pnt_status pnt_hydro_cycle(pnt_hydro* h, pnt_scalars* out) {
+    if (!h) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    DeviceGuard dg(h->device);
+    pnt_status st = h->launch_cycles(1);
+    if (!st) st = h->fetch_ctl();
+    if (st) return st;
+    h->scalars(out);
+    if (h->ctl_host->status) return fail(h->ctl_host->status, "%d negative side volumes on cycle %d",
+                                         h->ctl_host->nbad, h->ctl_host->cycle);
+    return PNT_OK;
+}
+
+pnt_status pnt_hydro_run(pnt_hydro* h, int32_t max_cycles, pnt_report_fn report, void* user, pnt_scalars* out) {
+    if (!h) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    DeviceGuard dg(h->device);
+    pnt_status st = h->fetch_ctl();
+    if (st) return st;
+    const int32_t start = h->ctl_host->cycle;
+    const int32_t stop_at =
+        (max_cycles > 0 && (int64_t)start + max_cycles < INT_MAX) ? start + max_cycles : INT_MAX;
+    if ((st = h->set_stop_at(stop_at))) return st;
+    if ((st = h->ensure_graph())) return st;
+    const int dtreport = h->params.dtreport > 0 ? h->params.dtreport : 10;
+    auto t_prev = std::chrono::steady_clock::now();
+    while (!h->ctl_host->done && h->ctl_host->cycle < stop_at) {
+        const int32_t cyc = h->ctl_host->cycle;
+        int64_t target;
+        if (report) target = (cyc < 1) ? 1 : ((int64_t)cyc / dtreport + 1) * dtreport;
+        else target = (int64_t)cyc + 64LL * h->graph_cycles;   // poll the done flag now and then
+        target = std::min<int64_t>(target, stop_at);
+        if ((st = h->enqueue((int)(target - cyc)))) break;
+        if ((st = h->fetch_ctl())) break;
+        if (report && !h->ctl_host->status && h->ctl_host->cycle == target &&
+            (target == 1 || target % dtreport == 0)) {
+            const auto t_now = std::chrono::steady_clock::now();
+            const double us = std::chrono::duration<double, std::micro>(t_now - t_prev).count();
+            t_prev = t_now;
+            pnt_scalars sc;
+            h->scalars(&sc);
+            report(&sc, us, user);
+        }
+    }
+    if (!st) st = h->set_stop_at(INT_MAX);
+    if (st) return st;
+    h->scalars(out);
+    if (h->ctl_host->status) return fail(h->ctl_host->status, "%d negative side volumes on cycle %d",
+                                         h->ctl_host->nbad, h->ctl_host->cycle);
+    return PNT_OK;
+}
+
+pnt_status pnt_hydro_enqueue(pnt_hydro* h, int32_t ncycles) {
+    if (!h || ncycles < 0) return fail(PNT_ERR_INVALID_ARG, "bad argument");
+    DeviceGuard dg(h->device);
+    return h->enqueue(ncycles);
+}
+
+pnt_status pnt_hydro_time_kernels(pnt_hydro* h, int32_t ncycles, double* kernel_ms, int32_t nkernels) {
+    if (!h || !kernel_ms || ncycles <= 0 || nkernels <= 0) return fail(PNT_ERR_INVALID_ARG, "bad argument");
+    DeviceGuard dg(h->device);
+    std::vector<cudaEvent_t> ev((size_t)ncycles * (kNumPasses + 1), nullptr);
+    pnt_status st = PNT_OK;
+    for (auto& e : ev) {
+        if (cudaEventCreate(&e) != cudaSuccess) { st = fail(PNT_ERR_CUDA, "cudaEventCreate failed"); break; }
+    }
+    for (int32_t i = 0; i < ncycles && !st; ++i) {
+        const cudaError_t e = launch_cycle_fp64(h->a, h->hc, h->stream, &ev[(size_t)i * (kNumPasses + 1)]);
+        if (e != cudaSuccess) st = fail(PNT_ERR_CUDA, "cycle launch: %s", cudaGetErrorString(e));
+    }
+    if (!st && cudaStreamSynchronize(h->stream) != cudaSuccess) st = fail(PNT_ERR_CUDA, "synchronize failed");
+    if (!st) {
+        for (int k = 0; k < nkernels; ++k) kernel_ms[k] = 0.;
+        for (int32_t i = 0; i < ncycles; ++i) {
+            for (int k = 0; k < kNumPasses && k < nkernels; ++k) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ev[(size_t)i * (kNumPasses + 1) + k], ev[(size_t)i * (kNumPasses + 1) + k + 1]);
+                kernel_ms[k] += ms / ncycles;
+            }
+        }
+    }
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    if (!st) st = h->fetch_ctl();
+    return st;
+}
+
+pnt_status pnt_hydro_time_cycles(pnt_hydro* h, int32_t ncycles, double* elapsed_ms) {
+    if (!h || !elapsed_ms || ncycles < 0) return fail(PNT_ERR_INVALID_ARG, "bad argument");
+    DeviceGuard dg(h->device);
+    pnt_status st = h->ensure_graph();
+    if (st) return st;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        return fail(PNT_ERR_CUDA, "cudaEventCreate failed");
+    }
+    cudaError_t e = cudaEventRecord(e0, h->stream);
+    if (e == cudaSuccess) st = h->enqueue(ncycles);
+    if (e == cudaSuccess && !st) e = cudaEventRecord(e1, h->stream);
+    if (e == cudaSuccess && !st) e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess && !st) e = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st) return st;
+    if (e != cudaSuccess) return fail(PNT_ERR_CUDA, "cycle timing: %s", cudaGetErrorString(e));
+    *elapsed_ms = ms;
+    return h->fetch_ctl();
+}
+
+pnt_status pnt_hydro_synchronize(pnt_hydro* h) {
+    if (!h) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    DeviceGuard dg(h->device);
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return PNT_OK;
+}
+
+pnt_status pnt_hydro_get_scalars(pnt_hydro* h, pnt_scalars* out) {
+    if (!h || !out) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    DeviceGuard dg(h->device);
+    const pnt_status st = h->fetch_ctl();
+    if (st) return st;
+    h->scalars(out);
+    return PNT_OK;
+}
+
+pnt_status pnt_hydro_download(pnt_hydro* h, int32_t field, void* dst, size_t bytes) {
+    if (!h || !dst) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    DeviceGuard dg(h->device);
+    pnt_status st = h->fetch_ctl();
+    if (st) return st;
+    const FieldInfo fi = field_info(h, field, h->ctl_host->cycle & 1);
+    if (!fi.dev) return fail(PNT_ERR_INVALID_ARG, "unknown field %d", field);
+    if (bytes != fi.bytes) return fail(PNT_ERR_INVALID_ARG, "field %d has %zu bytes, got %zu", field, fi.bytes, bytes);
+    CUDA_TRY(cudaMemcpyAsync(dst, fi.dev, bytes, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return PNT_OK;
+}
+
+pnt_status pnt_hydro_upload(pnt_hydro* h, int32_t field, const void* src, size_t bytes) {
+    if (!h || !src) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    DeviceGuard dg(h->device);
+    pnt_status st = h->fetch_ctl();
+    if (st) return st;
+    const FieldInfo fi = field_info(h, field, h->ctl_host->cycle & 1);
+    if (!fi.dev || field == PNT_FIELD_SMF) return fail(PNT_ERR_INVALID_ARG, "field %d is not writable", field);
+    if (bytes != fi.bytes) return fail(PNT_ERR_INVALID_ARG, "field %d has %zu bytes, got %zu", field, fi.bytes, bytes);
+    CUDA_TRY(cudaMemcpyAsync(fi.dev, src, bytes, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return PNT_OK;
+}
+
+pnt_status pnt_hydro_device_ptr(pnt_hydro* h, int32_t field, void** dptr) {
+    if (!h || !dptr) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    DeviceGuard dg(h->device);
+    pnt_status st = h->fetch_ctl();
+    if (st) return st;
+    const FieldInfo fi = field_info(h, field, h->ctl_host->cycle & 1);
+    if (!fi.dev) return fail(PNT_ERR_INVALID_ARG, "unknown field %d", field);
+    *dptr = fi.dev;
+    return PNT_OK;
+}
+
+pnt_status pnt_hydro_stream(pnt_hydro* h, void** stream) {
+    if (!h || !stream) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    *stream = (void*)h->stream;
+    return PNT_OK;
+}
+
+pnt_status pnt_hydro_write_xy(pnt_hydro* h, const char* path) {
+    if (!h || !path) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    std::vector<double> zr(h->numz), ze(h->numz), zp(h->numz);
+    pnt_status st;
+    if ((st = pnt_hydro_download(h, PNT_FIELD_ZR, zr.data(), zr.size() * 8)) ||
+        (st = pnt_hydro_download(h, PNT_FIELD_ZE, ze.data(), ze.size() * 8)) ||
+        (st = pnt_hydro_download(h, PNT_FIELD_ZP, zp.data(), zp.size() * 8)))
+        return st;
+    return write_xy(path, zr, ze, zp);
+}
+
+// ExportGold::write (ExportGold.cc:31-307): case file, geometry with the
+// zones sorted into triangles / quads / others, and per-zone variables.
+pnt_status pnt_hydro_write_gold(pnt_hydro* h, const char* base) {
+    if (!h || !base) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    const int64_t nz = h->numz, np = h->nump;
+    std::vector<double> zr(nz), ze(nz), zp(nz), px(2 * np);
+    pnt_status st;
+    if ((st = pnt_hydro_download(h, PNT_FIELD_ZR, zr.data(), nz * 8)) ||
+        (st = pnt_hydro_download(h, PNT_FIELD_ZE, ze.data(), nz * 8)) ||
+        (st = pnt_hydro_download(h, PNT_FIELD_ZP, zp.data(), nz * 8)) ||
+        (st = pnt_hydro_download(h, PNT_FIELD_PX, px.data(), np * 16)))
+        return st;
+    std::vector<int64_t> mapzs(nz);
+    std::vector<int64_t> tris, quads, others;
+    int64_t sc = 0;
+    for (int64_t z = 0; z < nz; ++z) {
+        const int n = h->znump[z];
+        (n == 3 ? tris : n == 4 ? quads : others).push_back(z);
+        mapzs[z] = sc;
+        sc += n;
+    }
+    const std::string b(base);
+    FILE* f = fopen((b + ".case").c_str(), "w");
+    if (!f) return fail(PNT_ERR_INVALID_ARG, "cannot open %s.case", base);
+    fprintf(f,
+            "#\n# Created by PENNANT\n#\nFORMAT\ntype: ensight gold\nGEOMETRY\nmodel: %s.geo\n"
+            "VARIABLE\nscalar per element: zr %s.zr\nscalar per element: ze %s.ze\n"
+            "scalar per element: zp %s.zp\n",
+            base, base, base, base);
+    fclose(f);
+    f = fopen((b + ".geo").c_str(), "w");
+    if (!f) return fail(PNT_ERR_INVALID_ARG, "cannot open %s.geo", base);
+    fprintf(f, "cycle = %8d\nt = %15.8e\nnode id assign\nelement id given\npart\n%10d\nuniverse\n"
+               "coordinates\n%10lld\n",
+            h->ctl_host->cycle, h->ctl_host->time, 1, (long long)np);
+    for (int64_t q = 0; q < np; ++q) fprintf(f, "%12.5e\n", px[2 * q]);
+    for (int64_t q = 0; q < np; ++q) fprintf(f, "%12.5e\n", px[2 * q + 1]);
+    for (int64_t q = 0; q < np; ++q) fprintf(f, "%12.5e\n", 0.);
+    const std::vector<int64_t>* groups[2] = {&tris, &quads};
+    const char* tags[2] = {"tria3", "quad4"};
+    for (int k = 0; k < 2; ++k) {
+        const auto& gz = *groups[k];
+        if (gz.empty()) continue;
+        fprintf(f, "%s\n%10lld\n", tags[k], (long long)gz.size());
+        for (int64_t z : gz) fprintf(f, "%10lld\n", (long long)z + 1);
+        for (int64_t z : gz) {
+            for (int i = 0; i < h->znump[z]; ++i) fprintf(f, "%10d", h->mapsp1[mapzs[z] + i] + 1);
+            fprintf(f, "\n");
+        }
+    }
+    if (!others.empty()) {
+        fprintf(f, "nsided\n%10lld\n", (long long)others.size());
+        for (int64_t z : others) fprintf(f, "%10lld\n", (long long)z + 1);
+        for (int64_t z : others) fprintf(f, "%10d\n", h->znump[z]);
+        for (int64_t z : others) {
+            for (int i = 0; i < h->znump[z]; ++i) fprintf(f, "%10d", h->mapsp1[mapzs[z] + i] + 1);
+            fprintf(f, "\n");
+        }
+    }
+    fclose(f);
+    const std::vector<double>* vars[3] = {&zr, &ze, &zp};
+    const char* vn[3] = {"zr", "ze", "zp"};
+    for (int v = 0; v < 3; ++v) {
+        f = fopen((b + "." + vn[v]).c_str(), "w");
+        if (!f) return fail(PNT_ERR_INVALID_ARG, "cannot open %s.%s", base, vn[v]);
+        fprintf(f, "%s\npart\n%10d\n", vn[v], 1);
+        for (int k = 0; k < 2; ++k) {
+            if (groups[k]->empty()) continue;
+            fprintf(f, "%s\n", tags[k]);
+            for (int64_t z : *groups[k]) fprintf(f, "%12.5e\n", (*vars[v])[z]);
+        }
+        if (!others.empty()) {
+            fprintf(f, "nsided\n");
+            for (int64_t z : others) fprintf(f, "%12.5e\n", (*vars[v])[z]);
+        }
+        fclose(f);
+    }
+    return PNT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,89 @@
+// hydro_dev.h -- device-side data of one hydro instance and the launch
+// entry points of the cycle kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pnt {
+
+constexpr int kMaxBC = 16;
+
+// Run state the kernels read and the finalize step updates; it lives in
+// device memory so the whole cycle can be replayed from a CUDA graph.
+struct Ctl {
+    double dt;       // dt of the next cycle to run
+    double dtlast;   // dt of the last completed cycle
+    double time;     // simulation time after the last completed cycle
+    double dtrec;    // Hydro::calcDtTask result of the last cycle
+    double dtnew;    // calcDtNew of the last cycle
+    double dvovmax;  // calcDvol of the last cycle
+    int32_t cycle;   // completed cycles; the current point buffer is cycle & 1
+    int32_t done;    // cstop/tstop reached or an error
+    int32_t status;  // pnt_status of a failure
+    int32_t nbad;    // negative side count of a failure
+    int32_t stop_at; // kernels skip once cycle >= stop_at
+    int32_t pad;
+};
+
+// Per-run constants (deck values and the quantities the reference
+// computes once per task from them).
+struct HydroConst {
+    double cfl, cflv;
+    double gm1, ssmin2;           // PolyGas: gamma - 1, max(ssmin^2, 1e-99)
+    double alfa, tts_ssmin;       // TTS
+    double gammap1, q1, q2;       // QCS: qgamma + 1
+    double dtmax, dtinit, dtfac, tstop;
+    int32_t cstop;
+    int32_t nbc;
+    double vfix[kMaxBC][2];
+};
+
+// Device arrays of one mesh + state, reference numbering.
+struct DevArrays {
+    int32_t nump, numz, nums;
+    int32_t quads;               // all zones are quads at sides 4z..4z+3
+    const int32_t* zfirst;       // [numz]
+    const int32_t* znump;        // [numz]
+    const int32_t* mapsp1;       // [nums]
+    const double* smf;           // [nums]
+    const int32_t* poff;         // [nump+1]
+    const int32_t* pcorner;      // [nums]
+    const uint16_t* bcmask;      // [nump] bit b: point on BC plane b
+    double2* px[2];              // point position, double buffered by cycle parity
+    double2* pu[2];              // point velocity
+    double* zm;
+    double* zr;
+    double* ze;
+    double* zetot;
+    double* zwrate;
+    double* zvol;
+    double* zp;
+    // per-side intermediates written by pass A
+    double* cmass;               // corner mass of side s at point mapsp1[s]
+    double2* cforce;             // corner force of side s at point mapsp1[s]
+    double2* sftot;              // sfp + sfq of side s (calcWork)
+    // per-block partial reductions
+    double* part_dtnew;
+    int32_t* part_badA;
+    double* part_dvov;
+    int32_t* part_badC;
+    Ctl* ctl;
+};
+
+constexpr int kZoneThreads = 256;   // 64 zones x 4 side lanes per block
+constexpr int kPointThreads = 256;
+
+inline int64_t zone_blocks(int32_t numz) {
+    return (4 * (int64_t)numz + kZoneThreads - 1) / kZoneThreads;
+}
+
+constexpr int kNumPasses = 4;   // A, B, C, finalize
+
+// One hydro cycle (passes A, B, C and the finalize step) on `stream`.  With
+// `ev` non-null, ev[i] is recorded before pass i and ev[kNumPasses] after
+// the last one.
+cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStream_t stream,
+                              cudaEvent_t* ev = nullptr);
+
+}  // namespace pnt

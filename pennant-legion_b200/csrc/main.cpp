@@ -1,0 +1,77 @@
+// main.cpp -- `pennant [-n numpcs] -f deck.pnt`: the reference's command line
+// (main.cc:46-107) and Driver::run (Driver.cc:65-187) on the GPU library.
+//
+// Output: the reference's report lines (Driver.cc:344-345), the run summary
+// (Driver.cc:170-180) and <probname>.xy plus the EnSight Gold files
+// (Mesh::write, Mesh.cc:670-691).  The run stops once time >= tstop or
+// cycle >= cstop, as the reference's predicated build does.
+#include "pennant.hh"
+
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+namespace {
+
+void report(const pnt_scalars* s, double wall_us, void*) {
+    printf("End cycle %6d, time = %11.5g, dt = %11.5g, wall = %11lld us\n", s->cycle, s->time, s->dt,
+           (long long)wall_us);
+    fflush(stdout);
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    int numpcs = 1;
+    const char* filename = nullptr;
+    int device = 0;
+    bool warn = true;
+    for (int i = 1; i < argc;) {
+        if (!strcmp(argv[i], "-f") && i + 1 < argc) { filename = argv[i + 1]; i += 2; }
+        else if (!strcmp(argv[i], "-n") && i + 1 < argc) { numpcs = atoi(argv[i + 1]); i += 2; }
+        else if (!strcmp(argv[i], "-g") && i + 1 < argc) { device = atoi(argv[i + 1]); i += 2; }
+        else {
+            if (warn) fprintf(stderr, "Usage: pennant [-n <numpcs>] [-g <gpu>] -f <filename>\n");
+            warn = false;
+            ++i;
+        }
+    }
+    if (!filename) {
+        fprintf(stderr, "No Pennant input file specified. Exiting...\n");
+        return 1;
+    }
+    std::string probname(filename);
+    if (probname.size() >= 4 && probname.substr(probname.size() - 4) == ".pnt")
+        probname = probname.substr(0, probname.size() - 4);
+    try {
+        printf("********************\nRunning PENNANT (B200)\n********************\n\n");
+        pnt::InputFile inp(filename);
+        pnt::Mesh mesh(&inp, numpcs);
+        printf("--- Mesh Information ---\nPoints:  %d\nZones:   %d\nSides:   %d\n------------------------\n",
+               mesh.nump, mesh.numz, mesh.nums);
+        pnt::Hydro hydro(&inp, &mesh, device);
+        pnt_scalars s{};
+        const auto t0 = std::chrono::steady_clock::now();
+        const pnt_status st = pnt_hydro_run(hydro.handle(), 0, report, nullptr, &s);
+        const auto t1 = std::chrono::steady_clock::now();
+        if (st == PNT_ERR_BADSIDES) {
+            fprintf(stderr, "Error: %d negative side volumes on cycle %d\nExiting...\n", s.nbad, s.cycle);
+            return 1;
+        }
+        pnt::check(st);
+        const double wall = std::chrono::duration<double, std::micro>(t1 - t0).count();
+        printf("\nRun complete\ncycle = %6d,        cstop = %8d\ntime = %14.6g, tstop = %8.6g\n\n", s.cycle,
+               hydro.params.cstop, s.time, hydro.params.tstop);
+        printf("************************************\nhydro cycle run time= %14.8g us\n"
+               "************************************\n",
+               wall);
+        pnt::check(pnt_hydro_write_xy(hydro.handle(), (probname + ".xy").c_str()));
+        pnt::check(pnt_hydro_write_gold(hydro.handle(), probname.c_str()));
+    } catch (const pnt::Error& e) {
+        fprintf(stderr, "Error: %s\n", e.what());
+        return 1;
+    }
+    return 0;
+}

@@ -1,0 +1,334 @@
+"""ctypes binding of libpennant_b200.so (C ABI: include/pennant_b200.h).
+
+The compute path is the CUDA library; this module only marshals arguments.
+Importing it loads the in-tree shared library and raises if it is missing:
+there is no CPU fallback.
+
+Objects mirror the reference's classes: ``Deck`` (InputFile), ``Mesh``
+(Mesh + GenMesh, one piece), ``Hydro`` (Hydro + the Driver loop).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_PKG_DIR), "libpennant_b200.so")
+
+PNT_OK = 0
+PNT_ERR_INVALID_ARG = 1
+PNT_ERR_DECK = 2
+PNT_ERR_BADSIDES = 3
+PNT_ERR_CUDA = 4
+PNT_ERR_UNSUPPORTED = 5
+PNT_ERR_TIMEOUT = 6
+PNT_ERR_NOMEM = 7
+PNT_ERR_NO_DEVICE = 8
+PNT_ERR_STATE = 9
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+MAX_BC = 16
+
+FIELDS = {"px": 0, "pu": 1, "zr": 2, "ze": 3, "zp": 4, "zm": 5, "zetot": 6,
+          "zvol": 7, "zwrate": 8, "smf": 9}
+_POINT2 = {"px", "pu"}
+_SIDE = {"smf"}
+
+
+class PntError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"pnt status {status}: {msg}")
+        self.status = status
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("cstop", C.c_int32), ("dtreport", C.c_int32),
+        ("tstop", C.c_double), ("dtmax", C.c_double), ("dtinit", C.c_double), ("dtfac", C.c_double),
+        ("cfl", C.c_double), ("cflv", C.c_double), ("rinit", C.c_double), ("einit", C.c_double),
+        ("rinitsub", C.c_double), ("einitsub", C.c_double), ("uinitradial", C.c_double),
+        ("has_subregion", C.c_int32), ("subregion", C.c_double * 4),
+        ("nbcx", C.c_int32), ("nbcy", C.c_int32),
+        ("bcx", C.c_double * MAX_BC), ("bcy", C.c_double * MAX_BC),
+        ("gamma", C.c_double), ("pgas_ssmin", C.c_double),
+        ("alfa", C.c_double), ("tts_ssmin", C.c_double),
+        ("qgamma", C.c_double), ("q1", C.c_double), ("q2", C.c_double),
+        ("precision", C.c_int32), ("graph_cycles", C.c_int32),
+        ("reserved", C.c_int32 * 14),
+    ]
+
+
+class Scalars(C.Structure):
+    _fields_ = [
+        ("cycle", C.c_int32), ("done", C.c_int32), ("status", C.c_int32), ("nbad", C.c_int32),
+        ("time", C.c_double), ("dt", C.c_double), ("dtrec", C.c_double),
+        ("dtnew", C.c_double), ("dvovmax", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [
+        ("nump", C.c_int32), ("numz", C.c_int32), ("nums", C.c_int32),
+        ("px", C.POINTER(C.c_double)), ("znump", C.POINTER(C.c_int32)),
+        ("mapsp1", C.POINTER(C.c_int32)), ("mapsp2", C.POINTER(C.c_int32)),
+        ("mapsz", C.POINTER(C.c_int32)), ("mapss3", C.POINTER(C.c_int32)),
+        ("mapss4", C.POINTER(C.c_int32)),
+    ]
+
+
+REPORT_FN = C.CFUNCTYPE(None, C.POINTER(Scalars), C.c_double, C.c_void_p)
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C pennant-legion_b200` "
+                          "(or __graft_entry__.build()); there is no fallback path")
+    lib = C.CDLL(LIB_PATH)
+    vp, i32, dbl, sz = C.c_void_p, C.c_int32, C.c_double, C.c_size_t
+    pp = C.POINTER(C.c_void_p)
+    sig = {
+        "pnt_status_string": (C.c_char_p, [i32]),
+        "pnt_last_error": (C.c_char_p, []),
+        "pnt_abi_version": (i32, []),
+        "pnt_deck_load": (i32, [C.c_char_p, pp]),
+        "pnt_deck_parse": (i32, [C.c_char_p, pp]),
+        "pnt_deck_set": (i32, [vp, C.c_char_p, C.c_char_p]),
+        "pnt_deck_has": (i32, [vp, C.c_char_p]),
+        "pnt_deck_get_int": (i32, [vp, C.c_char_p, i32]),
+        "pnt_deck_get_double": (dbl, [vp, C.c_char_p, dbl]),
+        "pnt_deck_get_string": (i32, [vp, C.c_char_p, C.c_char_p, C.c_char_p, sz]),
+        "pnt_deck_get_double_list": (i32, [vp, C.c_char_p, C.POINTER(C.c_double), i32]),
+        "pnt_deck_destroy": (None, [vp]),
+        "pnt_mesh_generate": (i32, [vp, pp]),
+        "pnt_mesh_create": (i32, [C.POINTER(MeshDesc), pp]),
+        "pnt_mesh_describe": (i32, [vp, C.POINTER(MeshDesc)]),
+        "pnt_mesh_point_corners": (i32, [vp, C.POINTER(C.POINTER(C.c_int32)),
+                                         C.POINTER(C.POINTER(C.c_int32))]),
+        "pnt_mesh_destroy": (None, [vp]),
+        "pnt_params_default": (i32, [C.POINTER(Params)]),
+        "pnt_params_from_deck": (i32, [vp, C.POINTER(Params)]),
+        "pnt_hydro_create": (i32, [vp, C.POINTER(Params), i32, pp]),
+        "pnt_hydro_destroy": (None, [vp]),
+        "pnt_hydro_cycle": (i32, [vp, C.POINTER(Scalars)]),
+        "pnt_hydro_run": (i32, [vp, i32, REPORT_FN, vp, C.POINTER(Scalars)]),
+        "pnt_hydro_enqueue": (i32, [vp, i32]),
+        "pnt_hydro_synchronize": (i32, [vp]),
+        "pnt_hydro_time_kernels": (i32, [vp, i32, C.POINTER(C.c_double), i32]),
+        "pnt_hydro_time_cycles": (i32, [vp, i32, C.POINTER(C.c_double)]),
+        "pnt_hydro_get_scalars": (i32, [vp, C.POINTER(Scalars)]),
+        "pnt_hydro_download": (i32, [vp, i32, vp, sz]),
+        "pnt_hydro_upload": (i32, [vp, i32, vp, sz]),
+        "pnt_hydro_device_ptr": (i32, [vp, i32, pp]),
+        "pnt_hydro_stream": (i32, [vp, pp]),
+        "pnt_hydro_write_xy": (i32, [vp, C.c_char_p]),
+        "pnt_hydro_write_gold": (i32, [vp, C.c_char_p]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def check(status: int) -> None:
+    if status != PNT_OK:
+        raise PntError(status, (lib.pnt_last_error() or b"").decode())
+
+
+def _b(s: str) -> bytes:
+    return s.encode()
+
+
+class Deck:
+    """InputFile: a parsed .pnt deck."""
+
+    def __init__(self, path: str | None = None, text: str | None = None):
+        h = C.c_void_p()
+        if text is not None:
+            check(lib.pnt_deck_parse(_b(text), C.byref(h)))
+        else:
+            check(lib.pnt_deck_load(_b(path), C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.pnt_deck_destroy(self.h)
+            self.h = None
+
+    def set(self, key: str, value) -> "Deck":
+        check(lib.pnt_deck_set(self.h, _b(key), _b(str(value))))
+        return self
+
+    def get_int(self, key, dflt=0):
+        return lib.pnt_deck_get_int(self.h, _b(key), dflt)
+
+    def get_double(self, key, dflt=0.0):
+        return lib.pnt_deck_get_double(self.h, _b(key), dflt)
+
+    def get_string(self, key, dflt=""):
+        buf = C.create_string_buffer(4096)
+        lib.pnt_deck_get_string(self.h, _b(key), _b(dflt), buf, 4096)
+        return buf.value.decode()
+
+    def get_double_list(self, key):
+        n = lib.pnt_deck_get_double_list(self.h, _b(key), None, 0)
+        if n < 0:
+            return None
+        arr = (C.c_double * max(n, 1))()
+        lib.pnt_deck_get_double_list(self.h, _b(key), arr, n)
+        return list(arr[:n])
+
+    def params(self) -> Params:
+        p = Params()
+        check(lib.pnt_params_from_deck(self.h, C.byref(p)))
+        return p
+
+
+class Mesh:
+    """Mesh + GenMesh for one piece, reference numbering."""
+
+    def __init__(self, deck: Deck | None = None, desc: dict | None = None):
+        h = C.c_void_p()
+        if deck is not None:
+            check(lib.pnt_mesh_generate(deck.h, C.byref(h)))
+        else:
+            arrs = {k: np.ascontiguousarray(desc[k], dtype=np.float64 if k == "px" else np.int32)
+                    for k in ("px", "znump", "mapsp1", "mapsp2", "mapsz", "mapss3", "mapss4")}
+            d = MeshDesc()
+            d.nump = len(arrs["px"]) // 2 if arrs["px"].ndim == 1 else arrs["px"].shape[0]
+            d.numz = len(arrs["znump"])
+            d.nums = len(arrs["mapsp1"])
+            d.px = arrs["px"].ctypes.data_as(C.POINTER(C.c_double))
+            for k in ("znump", "mapsp1", "mapsp2", "mapsz", "mapss3", "mapss4"):
+                setattr(d, k, arrs[k].ctypes.data_as(C.POINTER(C.c_int32)))
+            check(lib.pnt_mesh_create(C.byref(d), C.byref(h)))
+        self.h = h
+        d = MeshDesc()
+        check(lib.pnt_mesh_describe(self.h, C.byref(d)))
+        self.nump, self.numz, self.nums = d.nump, d.numz, d.nums
+        self._desc = d
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.pnt_mesh_destroy(self.h)
+            self.h = None
+
+    def array(self, name: str) -> np.ndarray:
+        """Copy of a connectivity array (px as (nump, 2))."""
+        d = self._desc
+        if name == "px":
+            return np.ctypeslib.as_array(d.px, shape=(2 * d.nump,)).reshape(-1, 2).copy()
+        n = d.numz if name == "znump" else d.nums
+        return np.ctypeslib.as_array(getattr(d, name), shape=(n,)).copy()
+
+    def point_corners(self):
+        off = C.POINTER(C.c_int32)()
+        sides = C.POINTER(C.c_int32)()
+        check(lib.pnt_mesh_point_corners(self.h, C.byref(off), C.byref(sides)))
+        return (np.ctypeslib.as_array(off, shape=(self.nump + 1,)).copy(),
+                np.ctypeslib.as_array(sides, shape=(self.nums,)).copy())
+
+
+class Hydro:
+    """Hydro state on one GPU plus the Driver loop."""
+
+    def __init__(self, mesh: Mesh, params: Params, device: int = 0):
+        h = C.c_void_p()
+        check(lib.pnt_hydro_create(mesh.h, C.byref(params), device, C.byref(h)))
+        self.h = h
+        self.mesh = mesh
+        self.params = params
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.pnt_hydro_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def cycle(self) -> dict:
+        s = Scalars()
+        check(lib.pnt_hydro_cycle(self.h, C.byref(s)))
+        return s.as_dict()
+
+    def run(self, max_cycles: int = 0, report=None) -> dict:
+        s = Scalars()
+        if report is None:
+            cb = REPORT_FN()
+        else:
+            cb = REPORT_FN(lambda sp, us, _u: report(sp.contents.as_dict(), us))
+        check(lib.pnt_hydro_run(self.h, max_cycles, cb, None, C.byref(s)))
+        return s.as_dict()
+
+    def enqueue(self, ncycles: int) -> None:
+        check(lib.pnt_hydro_enqueue(self.h, ncycles))
+
+    def time_kernels(self, ncycles: int) -> list:
+        """Mean ms of passes A, B, C, finalize over `ncycles` (these cycles advance the run)."""
+        out = (C.c_double * 4)()
+        check(lib.pnt_hydro_time_kernels(self.h, ncycles, out, 4))
+        return list(out)
+
+    def time_cycles(self, ncycles: int) -> float:
+        """Device milliseconds of `ncycles` graph-replayed cycles (CUDA events on the stream)."""
+        ms = C.c_double()
+        check(lib.pnt_hydro_time_cycles(self.h, ncycles, C.byref(ms)))
+        return ms.value
+
+    def synchronize(self) -> None:
+        check(lib.pnt_hydro_synchronize(self.h))
+
+    def scalars(self) -> dict:
+        s = Scalars()
+        check(lib.pnt_hydro_get_scalars(self.h, C.byref(s)))
+        return s.as_dict()
+
+    def _shape(self, name):
+        if name in _POINT2:
+            return (self.mesh.nump, 2)
+        if name in _SIDE:
+            return (self.mesh.nums,)
+        return (self.mesh.numz,)
+
+    def download(self, name: str) -> np.ndarray:
+        out = np.empty(self._shape(name), dtype=np.float64)
+        check(lib.pnt_hydro_download(self.h, FIELDS[name], out.ctypes.data, out.nbytes))
+        return out
+
+    def upload(self, name: str, arr) -> None:
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(self._shape(name))
+        check(lib.pnt_hydro_upload(self.h, FIELDS[name], a.ctypes.data, a.nbytes))
+
+    def device_ptr(self, name: str) -> int:
+        p = C.c_void_p()
+        check(lib.pnt_hydro_device_ptr(self.h, FIELDS[name], C.byref(p)))
+        return p.value
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        check(lib.pnt_hydro_stream(self.h, C.byref(p)))
+        return p.value or 0
+
+    def write_xy(self, path: str) -> None:
+        check(lib.pnt_hydro_write_xy(self.h, _b(path)))
+
+    def write_gold(self, base: str) -> None:
+        check(lib.pnt_hydro_write_gold(self.h, _b(base)))
+
+
+def exported_symbols_from_header(header_path: str) -> list[str]:
+    """Function names declared in include/pennant_b200.h."""
+    import re
+    txt = open(header_path).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(pnt_[a-z0-9_]+)\s*\(", txt)))

@@ -1,0 +1,71 @@
+"""The C-ABI library loads and exports every symbol include/*.h declares."""
+import ctypes
+import glob
+import os
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+import pennant_b200 as pb
+
+
+def _header_symbols():
+    syms = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        syms.update(pb.exported_symbols_from_header(h))
+    return sorted(syms)
+
+
+def test_every_declared_symbol_is_exported():
+    syms = _header_symbols()
+    assert len(syms) >= 30
+    lib = ctypes.CDLL(pb.LIB_PATH)
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_dynamic_symbol_table_has_c_linkage():
+    out = subprocess.run(["nm", "-D", "--defined-only", pb.LIB_PATH], capture_output=True, text=True,
+                         check=True).stdout
+    names = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    for s in _header_symbols():
+        assert s in names, s
+
+
+def test_status_strings():
+    for st in range(0, 10):
+        assert pb.lib.pnt_status_string(st)
+    assert pb.lib.pnt_status_string(999) == b"unknown status"
+
+
+def test_null_arguments_are_rejected():
+    assert pb.lib.pnt_deck_parse(None, None) == pb.PNT_ERR_INVALID_ARG
+    assert b"null" in pb.lib.pnt_last_error()
+    assert pb.lib.pnt_hydro_cycle(None, None) == pb.PNT_ERR_INVALID_ARG
+    assert pb.lib.pnt_mesh_generate(None, None) == pb.PNT_ERR_INVALID_ARG
+
+
+def test_cli_binary_exists():
+    exe = os.path.join(ROOT, "pennant-legion_b200", "pennant")
+    assert os.access(exe, os.X_OK)
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 1 and "No Pennant input file" in r.stderr
+
+
+def _has_device():
+    n = ctypes.c_int(0)
+    try:
+        rt = ctypes.CDLL("libcudart.so.12")
+    except OSError:
+        return False
+    return rt.cudaGetDeviceCount(ctypes.byref(n)) == 0 and n.value > 0
+
+
+@pytest.mark.skipif(_has_device(), reason="checks the no-device error path")
+def test_hydro_create_without_device_fails_loudly():
+    d = pb.Deck(path=os.path.join(ROOT, "tests", "golden", "sedovsmall.pnt"))
+    m = pb.Mesh(deck=d)
+    with pytest.raises(pb.PntError) as e:
+        pb.Hydro(m, d.params())
+    assert e.value.status == pb.PNT_ERR_NO_DEVICE

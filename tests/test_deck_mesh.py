@@ -1,0 +1,199 @@
+"""Host-side parity (no GPU): deck parsing, mesh generation, derived maps.
+
+The product's mesh builder (libpennant_b200.so, C++) and the oracle (C)
+restate GenMesh independently; connectivity, coordinates, boundary point
+sets and the point->corner CSR must agree bit for bit.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import golden
+from oracle import Oracle, OracleError
+import pennant_b200 as pb
+
+DECKS = ["sedov.pnt", "sedovsmall.pnt", "noh.pnt", "nohsmall.pnt", "leblanc.pnt", "nohsquare.pnt"]
+
+
+def test_abi_version():
+    assert pb.lib.pnt_abi_version() == 1
+
+
+# ---------------------------------------------------------------- deck
+def test_deck_values_and_defaults():
+    d = pb.Deck(text="# comment\ncstop 10\n  tstop   1.0e-1 trailing\nmeshparams 4 5 1.5 2.0\n"
+                     "meshtype rect\n\nbcx 0.0 1.5\nq1 .25\n")
+    assert d.get_int("cstop", 0) == 10
+    assert d.get_double("tstop", 0) == pytest.approx(0.1)
+    assert d.get_double_list("meshparams") == [4.0, 5.0, 1.5, 2.0]
+    assert d.get_string("meshtype") == "rect"
+    assert d.get_double_list("missing") is None
+    assert d.get_int("missing", 7) == 7
+    p = d.params()
+    assert (p.cstop, p.nbcx, p.nbcy) == (10, 2, 0)
+    assert p.q1 == 0.25 and p.q2 == 2.0 and p.alfa == 0.5     # QCS/TTS defaults
+    assert p.cfl == 0.6 and p.cflv == 0.1 and p.dtfac == 1.2  # Hydro/Driver defaults
+    assert p.gamma == pytest.approx(5.0 / 3.0)
+
+
+def test_deck_get_int_truncates_like_stream_extraction():
+    d = pb.Deck(text="cstop 12.7\n")
+    assert d.get_int("cstop", 0) == 12
+
+
+def test_deck_duplicate_key_is_an_error():
+    with pytest.raises(pb.PntError) as e:
+        pb.Deck(text="cstop 1\ncstop 2\n")
+    assert e.value.status == pb.PNT_ERR_DECK
+    with pytest.raises(OracleError):
+        Oracle(text="cstop 1\ncstop 2\nmeshtype rect\nmeshparams 2\n")
+
+
+def test_deck_unterminated_last_line_is_dropped():
+    # InputFile's getline loop stops at EOF before storing the last line
+    d = pb.Deck(text="cstop 5\ntstop 2.0")
+    assert d.get_double("tstop", -1.0) == -1.0
+
+
+def test_deck_needs_stop_condition():
+    d = pb.Deck(text="meshtype rect\nmeshparams 2\n")
+    with pytest.raises(pb.PntError) as e:
+        d.params()
+    assert e.value.status == pb.PNT_ERR_DECK
+
+
+def test_deck_missing_file():
+    with pytest.raises(pb.PntError) as e:
+        pb.Deck(path="/nonexistent/deck.pnt")
+    assert e.value.status == pb.PNT_ERR_DECK
+
+
+@pytest.mark.parametrize("text,status", [
+    ("cstop 1\nmeshparams 2\n", pb.PNT_ERR_DECK),                      # no meshtype
+    ("cstop 1\nmeshtype tri\nmeshparams 2\n", pb.PNT_ERR_DECK),        # invalid meshtype
+    ("cstop 1\nmeshtype rect\n", pb.PNT_ERR_DECK),                     # no meshparams
+    ("cstop 1\nmeshtype rect\nmeshparams 1 2 3 4 5\n", pb.PNT_ERR_DECK),
+    ("cstop 1\nmeshtype rect\nmeshparams 0 2\n", pb.PNT_ERR_DECK),
+    ("cstop 1\nmeshtype pie\nmeshparams 4 4 360\n", pb.PNT_ERR_DECK),  # theta must be < 360
+    ("cstop 1\nmeshtype hex\nmeshparams 4\n", pb.PNT_ERR_UNSUPPORTED),
+])
+def test_mesh_generate_rejects_bad_decks(text, status):
+    d = pb.Deck(text=text)
+    with pytest.raises(pb.PntError) as e:
+        pb.Mesh(deck=d)
+    assert e.value.status == status
+
+
+def test_subregion_needs_four_values():
+    d = pb.Deck(text="cstop 1\nmeshtype rect\nmeshparams 2\nsubregion 0 1 0\n")
+    with pytest.raises(pb.PntError):
+        d.params()
+
+
+# ---------------------------------------------------------------- mesh
+@pytest.mark.parametrize("name", DECKS)
+def test_mesh_connectivity_bit_exact_vs_oracle(name):
+    d = pb.Deck(path=golden(name))
+    m = pb.Mesh(deck=d)
+    o = Oracle(golden(name))
+    assert (m.nump, m.numz, m.nums) == (o.nump, o.numz, o.nums)
+    for k in ("znump", "mapsp1", "mapsp2", "mapsz", "mapss3", "mapss4"):
+        np.testing.assert_array_equal(m.array(k), o.field(k), err_msg=k)
+    px = m.array("px")
+    assert px.tobytes() == o.field("px").tobytes()
+
+
+def test_rect_numbering_matches_reference_layout():
+    m = pb.Mesh(deck=pb.Deck(text="cstop 1\nmeshtype rect\nmeshparams 3 2 3.0 2.0\n"))
+    assert (m.nump, m.numz, m.nums) == (12, 6, 24)
+    # zone 4 = row 1, col 1: sides bottom, right, top, left
+    np.testing.assert_array_equal(m.array("mapsp1")[16:20], [5, 6, 10, 9])
+    np.testing.assert_array_equal(m.array("mapsp2")[16:20], [6, 10, 9, 5])
+    np.testing.assert_array_equal(m.array("px")[6], [2.0, 1.0])
+
+
+def test_pie_mesh_structure():
+    m = pb.Mesh(deck=pb.Deck(path=golden("nohsmall.pnt")))   # pie 2 x 20
+    z = m.array("znump")
+    assert (z[:2] == 3).all() and (z[2:] == 4).all()
+    assert m.nums == 3 * 2 + 4 * 2 * 19
+    assert m.nump == 3 * 20 + 1
+    # every triangle touches the origin
+    sp1 = m.array("mapsp1")
+    assert (sp1[[0, 3]] == 0).all()
+
+
+@pytest.mark.parametrize("name", ["sedov.pnt", "noh.pnt", "leblanc.pnt"])
+def test_point_corner_csr(name):
+    m = pb.Mesh(deck=pb.Deck(path=golden(name)))
+    off, sides = m.point_corners()
+    sp1 = m.array("mapsp1")
+    assert off[0] == 0 and off[-1] == m.nums
+    ref_order = np.argsort(sp1, kind="stable")      # ascending side within each point
+    np.testing.assert_array_equal(sides, ref_order)
+    np.testing.assert_array_equal(np.diff(off), np.bincount(sp1, minlength=m.nump))
+
+
+def test_mesh_invariants_circulate():
+    m = pb.Mesh(deck=pb.Deck(path=golden("noh.pnt")))
+    sp1, sp2, ss4 = m.array("mapsp1"), m.array("mapsp2"), m.array("mapss4")
+    np.testing.assert_array_equal(sp2, sp1[ss4])
+
+
+def test_mesh_create_from_arrays_round_trip():
+    src = pb.Mesh(deck=pb.Deck(path=golden("nohsmall.pnt")))
+    desc = {k: src.array(k) for k in ("znump", "mapsp1", "mapsp2", "mapsz", "mapss3", "mapss4")}
+    desc["px"] = src.array("px").reshape(-1)
+    m = pb.Mesh(desc=desc)
+    for k in ("znump", "mapsp1", "mapss4"):
+        np.testing.assert_array_equal(m.array(k), src.array(k))
+
+
+def test_mesh_create_rejects_broken_connectivity():
+    src = pb.Mesh(deck=pb.Deck(path=golden("sedovsmall.pnt")))
+    desc = {k: src.array(k) for k in ("znump", "mapsp1", "mapsp2", "mapsz", "mapss3", "mapss4")}
+    desc["px"] = src.array("px").reshape(-1)
+    bad = dict(desc)
+    bad["mapss4"] = desc["mapss4"].copy()
+    bad["mapss4"][5] = 0
+    with pytest.raises(pb.PntError) as e:
+        pb.Mesh(desc=bad)
+    assert e.value.status == pb.PNT_ERR_INVALID_ARG
+    bad = dict(desc)
+    bad["mapsp1"] = desc["mapsp1"].copy()
+    bad["mapsp1"][3] = 10 ** 6
+    with pytest.raises(pb.PntError):
+        pb.Mesh(desc=bad)
+    bad = dict(desc)
+    bad["znump"] = desc["znump"].copy()
+    bad["znump"][0] = 5
+    with pytest.raises(pb.PntError) as e:
+        pb.Mesh(desc=bad)
+    assert e.value.status in (pb.PNT_ERR_UNSUPPORTED, pb.PNT_ERR_INVALID_ARG)
+
+
+def test_inverted_initial_mesh_reports_bad_sides():
+    src = pb.Mesh(deck=pb.Deck(path=golden("sedovsmall.pnt")))
+    desc = {k: src.array(k) for k in ("znump", "mapsp1", "mapsp2", "mapsz", "mapss3", "mapss4")}
+    px = src.array("px")
+    px[:, 1] = -px[:, 1]   # mirror in y: zones turn clockwise, r stays >= 0
+    desc["px"] = px.reshape(-1)
+    with pytest.raises(pb.PntError) as e:
+        pb.Mesh(desc=desc)
+    assert e.value.status == pb.PNT_ERR_BADSIDES
+
+
+@pytest.mark.parametrize("name", ["sedov.pnt", "noh.pnt", "leblanc.pnt", "nohsquare.pnt"])
+def test_bc_point_sets_match_oracle(name):
+    """Boundary point lists (HydroBC) are the points within 1e-12 of each
+    plane, ascending; the oracle builds them the reference's way."""
+    o = Oracle(golden(name))
+    d = pb.Deck(path=golden(name))
+    p = d.params()
+    px = pb.Mesh(deck=d).array("px")
+    planes = [(0, v) for v in p.bcx[:p.nbcx]] + [(1, v) for v in p.bcy[:p.nbcy]]
+    assert o.num("nbc") == len(planes)
+    for b, (axis, bound) in enumerate(planes):
+        mine = np.nonzero(np.abs(px[:, axis] - bound) < 1e-12)[0]
+        np.testing.assert_array_equal(mine, o.field(f"bcpts{b}"))
