@@ -58,6 +58,7 @@ DECKS = {
     "sedov48.pnt": sedov(48),      # CPU-runnable case, FP64, t = 1.0
     "sedov480.pnt": sedov(480),    # FP64 drop-in parity case, t = 1.0
     "sedov1920.pnt": sedov(1920),  # headline case
+    "sedov1024.pnt": sedov(1024),  # profiling case: ~0.4 GB on the device, > L2
     "leblanc2880x288.pnt": leblanc(),
 }
 
