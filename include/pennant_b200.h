@@ -220,6 +220,21 @@ pnt_status pnt_hydro_upload(pnt_hydro* hydro, int32_t field, const void* host_sr
 pnt_status pnt_hydro_device_ptr(pnt_hydro* hydro, int32_t field, void** dptr);
 pnt_status pnt_hydro_stream(pnt_hydro* hydro, void** cuda_stream);
 
+/* ------------------------------------------------------------------ */
+/* Per-task operators on caller-owned device arrays                     */
+/* ------------------------------------------------------------------ */
+
+/* Hydro::calcDtNewTask + calcDvolTask + calcDtTask (Hydro.cc:1591-1667;
+ * GPU variants gpu_calc_dt_new / gpu_calc_dvol, Hydro.cu:563-681) over
+ * numz zones of caller device arrays: out[0] = dtrec, out[1] = dtnew
+ * (Courant minimum), out[2] = dvovmax, written to device memory on
+ * `stream` (a cudaStream_t; NULL = default stream).  Asynchronous; per-block
+ * partial results go to stream-ordered scratch (cudaMallocAsync /
+ * cudaFreeAsync on `stream`).  numz may be 0 (dtnew = 1e99, dvovmax = 1e-99). */
+pnt_status pnt_op_calc_dt(const double* zdl, const double* zdu, const double* zss,
+                          const double* zvol, const double* zvol0, int64_t numz, double cfl,
+                          double cflv, double dtlast, double* out, void* stream);
+
 /* Output writers: WriteXY::write (WriteXY.cc:28-52) and ExportGold::write
  * (ExportGold.cc:31-307) of the current state. */
 pnt_status pnt_hydro_write_xy(pnt_hydro* hydro, const char* path);

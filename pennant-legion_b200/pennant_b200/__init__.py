@@ -126,6 +126,7 @@ def _load():
         "pnt_hydro_upload": (i32, [vp, i32, vp, sz]),
         "pnt_hydro_device_ptr": (i32, [vp, i32, pp]),
         "pnt_hydro_stream": (i32, [vp, pp]),
+        "pnt_op_calc_dt": (i32, [vp, vp, vp, vp, vp, C.c_int64, dbl, dbl, dbl, vp, vp]),
         "pnt_hydro_write_xy": (i32, [vp, C.c_char_p]),
         "pnt_hydro_write_gold": (i32, [vp, C.c_char_p]),
     }
@@ -324,6 +325,12 @@ class Hydro:
 
     def write_gold(self, base: str) -> None:
         check(lib.pnt_hydro_write_gold(self.h, _b(base)))
+
+
+def op_calc_dt(zdl: int, zdu: int, zss: int, zvol: int, zvol0: int, numz: int, cfl: float,
+               cflv: float, dtlast: float, out: int, stream: int = 0) -> None:
+    """pnt_op_calc_dt on device addresses (ints); out receives dtrec, dtnew, dvovmax."""
+    check(lib.pnt_op_calc_dt(zdl, zdu, zss, zvol, zvol0, numz, cfl, cflv, dtlast, out, stream))
 
 
 def exported_symbols_from_header(header_path: str) -> list[str]:
