@@ -235,6 +235,21 @@ pnt_status pnt_op_calc_dt(const double* zdl, const double* zdu, const double* zs
                           const double* zvol, const double* zvol0, int64_t numz, double cfl,
                           double cflv, double dtlast, double* out, void* stream);
 
+/* pnt_op_calc_dt for callers that must not allocate device memory (no
+ * counterpart in the reference).  Same arguments and results; it calls no
+ * allocator.  Its scratch is a fixed 128 KiB device array that each GPU
+ * holds from library load until process exit, which limits numz to
+ * PNT_OP_CALC_DT_NOALLOC_MAX_ZONES (larger numz: PNT_ERR_INVALID_ARG).
+ * Runs on the calling thread's current device.  The first call on a
+ * device looks up the array's address: make it before any stream capture.
+ * All calls on a device share the array, so calls that overlap on the GPU
+ * race; serialise them. */
+#define PNT_OP_CALC_DT_NOALLOC_MAX_ZONES 16777216
+pnt_status pnt_op_calc_dt_noalloc(const double* zdl, const double* zdu, const double* zss,
+                                  const double* zvol, const double* zvol0, int64_t numz,
+                                  double cfl, double cflv, double dtlast, double* out,
+                                  void* stream);
+
 /* Output writers: WriteXY::write (WriteXY.cc:28-52) and ExportGold::write
  * (ExportGold.cc:31-307) of the current state. */
 pnt_status pnt_hydro_write_xy(pnt_hydro* hydro, const char* path);

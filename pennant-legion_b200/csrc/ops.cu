@@ -10,6 +10,8 @@
 
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 using namespace pnt;
 
 namespace {
@@ -136,5 +138,83 @@ extern "C" pnt_status pnt_op_calc_dt(const double* zdl, const double* zdu, const
     e = cudaGetLastError();
     if (partial) cudaFreeAsync(partial, s);
     if (e != cudaSuccess) return fail(PNT_ERR_CUDA, "pnt_op_calc_dt launch: %s", cudaGetErrorString(e));
+    return PNT_OK;
+}
+
+// ---------------------------------------------------------------------
+// pnt_op_calc_dt_noalloc: the same two kernels with their per-block
+// partials in a fixed device array instead of allocated scratch.
+//
+// Who needs it: code that must not allocate device memory itself.  A
+// Legion GPU task is the reference's own case: the runtime's mapper owns
+// every instance and a task body is expected to take memory only through
+// the runtime.  Others are latency-critical loops where an allocation can
+// stall on device synchronisation or fail under memory pressure, and
+// processes whose device memory is capped by a pool they do not control.
+//
+// The array below exists once per GPU that loads this library and stays
+// resident until the process exits (128 KiB).  Every call on a device uses
+// the same array and overwrites the partials it later reads, so nothing
+// needs clearing between calls; calls that overlap on the GPU (different
+// streams, or different host threads on one device) race on it and must be
+// serialised by the caller.  The first call on each device looks up the
+// array's device address (cudaGetSymbolAddress); make that first call
+// before any stream capture.
+// ---------------------------------------------------------------------
+namespace {
+
+constexpr int kNoAllocMaxBlocks = 8192;
+constexpr int64_t kNoAllocMaxZones = (int64_t)kNoAllocMaxBlocks * kDtZonesPerBlock;   // 16,777,216
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) double g_dt_scratch[2 * kNoAllocMaxBlocks];
+
+std::mutex g_scratch_mu;
+void* g_scratch_addr[kMaxDevices] = {};
+
+// Device address of g_dt_scratch on the current device.  In host code the
+// symbol name is only a host-side stand-in, never a device address.
+pnt_status noalloc_scratch(double** out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(PNT_ERR_NO_DEVICE, "no current CUDA device: %s", cudaGetErrorString(e));
+    }
+    if (dev < 0 || dev >= kMaxDevices) return fail(PNT_ERR_UNSUPPORTED, "device ordinal %d >= %d", dev, kMaxDevices);
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_dt_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            return fail(PNT_ERR_CUDA, "cudaGetSymbolAddress of the no-allocation scratch: %s",
+                        cudaGetErrorString(e));
+        }
+        g_scratch_addr[dev] = p;
+    }
+    *out = static_cast<double*>(g_scratch_addr[dev]);
+    return PNT_OK;
+}
+
+}  // namespace
+
+extern "C" pnt_status pnt_op_calc_dt_noalloc(const double* zdl, const double* zdu, const double* zss,
+                                             const double* zvol, const double* zvol0, int64_t numz, double cfl,
+                                             double cflv, double dtlast, double* out, void* stream) {
+    pnt_status st = check_dt_args(zdl, zdu, zss, zvol, zvol0, numz, out);
+    if (st) return st;
+    if (numz > kNoAllocMaxZones)
+        return fail(PNT_ERR_INVALID_ARG,
+                    "numz %lld exceeds the no-allocation limit of %lld zones (use pnt_op_calc_dt)",
+                    (long long)numz, (long long)kNoAllocMaxZones);
+    double* scratch = nullptr;
+    if ((st = noalloc_scratch(&scratch))) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nblocks = (int)((numz + kDtZonesPerBlock - 1) / kDtZonesPerBlock);
+    if (nblocks > 0) dt_partials<<<nblocks, kDtThreads, 0, s>>>(zdl, zdu, zss, zvol, zvol0, numz, cfl, scratch);
+    dt_finish<<<1, kDtFinThreads, 0, s>>>(scratch, nblocks, dtlast, cflv, out);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(PNT_ERR_CUDA, "pnt_op_calc_dt_noalloc launch: %s", cudaGetErrorString(e));
     return PNT_OK;
 }

@@ -127,6 +127,7 @@ def _load():
         "pnt_hydro_device_ptr": (i32, [vp, i32, pp]),
         "pnt_hydro_stream": (i32, [vp, pp]),
         "pnt_op_calc_dt": (i32, [vp, vp, vp, vp, vp, C.c_int64, dbl, dbl, dbl, vp, vp]),
+        "pnt_op_calc_dt_noalloc": (i32, [vp, vp, vp, vp, vp, C.c_int64, dbl, dbl, dbl, vp, vp]),
         "pnt_hydro_write_xy": (i32, [vp, C.c_char_p]),
         "pnt_hydro_write_gold": (i32, [vp, C.c_char_p]),
     }
