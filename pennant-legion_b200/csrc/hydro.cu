@@ -272,6 +272,7 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
     if (p.dtinit < dt) dt = p.dtinit;
     if ((p.tstop - 0.) < dt) dt = p.tstop - 0.;
     ctl.dt = dt;
+    ctl.dtinv = 1. / dt;
     ctl.cycle = 0;
     ctl.time = 0.;
     ctl.done = (p.cstop <= 0 || !(0. < p.tstop)) ? 1 : 0;

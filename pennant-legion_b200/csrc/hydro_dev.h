@@ -13,6 +13,7 @@ constexpr int kMaxBC = 16;
 // device memory so the whole cycle can be replayed from a CUDA graph.
 struct Ctl {
     double dt;       // dt of the next cycle to run
+    double dtinv;    // 1/dt, as calcWorkRate forms it (Hydro.cc:1496)
     double dtlast;   // dt of the last completed cycle
     double time;     // simulation time after the last completed cycle
     double dtrec;    // Hydro::calcDtTask result of the last cycle

@@ -18,7 +18,14 @@
 // Zone passes map four lanes to a zone (one lane per side/corner, zones
 // with 3 sides leave one lane idle).  Zone-local side data moves between
 // lanes with warp shuffles; zone sums are formed by every lane in the
-// reference's serial side order.  This file is compiled with -fmad=false
+// reference's serial side order.  Quotients the reference forms once per
+// zone are split over the zone's lanes, one division each, and shared;
+// 1/elen is formed once per side and shared with the neighbouring corner;
+// QCS terms the reference computes and then discards (evol and du unless
+// cdiv < 0, zkur when cdiv > 0) are not computed, which leaves every stored
+// value unchanged.  Pass A is capped at 80 registers (3 blocks per SM): it
+// is latency bound and gains more from the extra warps than it loses to
+// the few spilled registers.  This file is compiled with -fmad=false
 // and every expression keeps the reference's operation order, including
 // Vec2.hh's `v / r` = v * (1/r) (Vec2.hh:145-149), so the results match a
 // serial CPU run of the reference bit for bit.
@@ -124,7 +131,7 @@ __device__ __forceinline__ void block_fold(double v, double* out) {
 // Pass A: predictor zone pass
 // ---------------------------------------------------------------------
 template <bool kQuads>
-__global__ void __launch_bounds__(kZoneThreads) pass_a(DevArrays a, HydroConst c) {
+__global__ void __launch_bounds__(kZoneThreads, 3) pass_a(DevArrays a, HydroConst c) {
     const Ctl* ctl = a.ctl;
     if (skip_cycle(ctl)) return;
     const int cur = ctl->cycle & 1;
@@ -178,28 +185,33 @@ __global__ void __launch_bounds__(kZoneThreads) pass_a(DevArrays a, HydroConst c
     // calcSurfVecs (Mesh.cc:1104-1123), calcEdgeLen (:1151-1179)
     const double2 ssurf = rotateCCW(sub(ex, zxp));
     const double elen = length(sub(xp2, xp));
+    const double rinv_el = 1. / elen;       // shared by QCS cqe1/cqe2/sfq
     // calcCharLen (Mesh.cc:1216-1244)
     const double fac = (n == 3 ? 3. : 4.);
     const double zdl = zmin_fold(1.e99, fac * sa / elen, g, n);
-    // calcRho (Hydro.cc:1034-1054)
-    const double zrp = zm / zvolp;
-    // calcCrnrMass (Hydro.cc:1083-1117)
-    const double mf3 = shfl(mf, lp);
-    const double cmass = zrp * zareap * 0.5 * (mf + mf3);
-
-    // PolyGas::calcStateHalf (PolyGas.cc:63-109)
+    // PolyGas::calcStateHalf (PolyGas.cc:63-109) with calcRho: the four
+    // zone quotients are split over the zone's lanes (one division each)
     const double e = dmax(ze, 0.);
     const double p = c.gm1 * zr * e;
     const double pre = c.gm1 * e;
     const double per = c.gm1 * zr;
-    const double csqd = dmax(c.ssmin2, pre + per * p / (zr * zr));
+    const double rA = ((k == 0) ? per * p : 1.) / ((k == 0) ? zr * zr : zm);
+    const double q = shfl(rA, g);            // per*p/(r*r)
+    const double minv = shfl(rA, g + 1);     // 1/zm
+    const double csqd = dmax(c.ssmin2, pre + q);
     const double zss = sqrt(csqd);
-    const double minv = 1. / zm;
     const double dv = (zvolp - zvol0) * minv;
     const double bulk = zr * csqd;
     const double denom = 1. + 0.5 * per * dv;
     const double src = zwrate * dth * minv;
-    const double zp = p + (per * src - zr * bulk * dv) / denom;
+    const double rB = ((k == 0) ? zm : per * src - zr * bulk * dv) / ((k == 0) ? zvolp : denom);
+    const double zrp = shfl(rB, g);          // zm/zvolp
+    const double zp = p + shfl(rB, g + 1);
+
+    // calcCrnrMass (Hydro.cc:1083-1117)
+    const double mf3 = shfl(mf, lp);
+    if (act) a.cmass[s] = zrp * zareap * 0.5 * (mf + mf3);
+    if (zok && k == 0) a.zp[z] = zp;
 
     // PolyGas::calcForce (PolyGas.cc:164-184)
     const double2 sfp = smul(-zp, ssurf);
@@ -227,37 +239,44 @@ __global__ void __launch_bounds__(kZoneThreads) pass_a(DevArrays a, HydroConst c
     const double2 v1 = sub(xq3, xq0);
     const double2 v2 = sub(xq1, xq0);
     const double de1 = shfl(elen, lp);      // elen[s]
+    const double rinv_de1 = shfl(rinv_el, lp);
     const double de2 = elen;                // elen[s2]
     const double minelen = dmin(de1, de2);
     double ccos = ((minelen < 1.e-12) ? 0. : 4. * dot(v1, v2) / (de1 * de2));
     const double cdiv = (cross(sub(up2, up0), sub(xq3, xq1)) - cross(sub(up3, up1), sub(xq2, xq0))) /
                         (2.0 * cvolume);
-    const double2 dxx1 = smul(0.5, sub(sub(add(xq1, xq2), xq0), xq3));
-    const double2 dxx2 = smul(0.5, sub(sub(add(xq2, xq3), xq0), xq1));
-    const double dx1 = length(dxx1);
-    const double dx2 = length(dxx2);
-    const double2 duav = smul(0.25, add(add(add(up0, up1), up2), up3));
-    const double test1 = fabs(dot(dxx1, duav) * dx2);
-    const double test2 = fabs(dot(dxx2, duav) * dx1);
-    const double num = (test1 > test2 ? dx1 : dx2);
-    const double den = (test1 > test2 ? dx2 : dx1);
-    const double r = num / den;
-    double evol = sqrt(4.0 * cvolume * r);
-    evol = dmin(evol, 2.0 * minelen);
-    const double dv1 = length2(sub(sub(add(up1, up2), up0), up3));
-    const double dv2 = length2(sub(sub(add(up2, up3), up0), up1));
-    double du = sqrt(dmax(dv1, dv2));
-    evol = (cdiv < 0.0 ? evol : 0.);
-    du = (cdiv < 0.0 ? du : 0.);
+    // evol and du are kept by the reference only where cdiv < 0
+    double evol = 0., du = 0.;
+    if (cdiv < 0.0) {
+        const double2 dxx1 = smul(0.5, sub(sub(add(xq1, xq2), xq0), xq3));
+        const double2 dxx2 = smul(0.5, sub(sub(add(xq2, xq3), xq0), xq1));
+        const double dx1 = length(dxx1);
+        const double dx2 = length(dxx2);
+        const double2 duav = smul(0.25, add(add(add(up0, up1), up2), up3));
+        const double test1 = fabs(dot(dxx1, duav) * dx2);
+        const double test2 = fabs(dot(dxx2, duav) * dx1);
+        const double num = (test1 > test2 ? dx1 : dx2);
+        const double den = (test1 > test2 ? dx2 : dx1);
+        const double r = num / den;
+        evol = sqrt(4.0 * cvolume * r);
+        evol = dmin(evol, 2.0 * minelen);
+        const double dv1 = length2(sub(sub(add(up1, up2), up0), up3));
+        const double dv2 = length2(sub(sub(add(up2, up3), up0), up1));
+        du = sqrt(dmax(dv1, dv2));
+    }
 
-    // QCS::setQCnForce (QCS.cc:246-327)
-    const double ztmp2 = c.q2 * 0.25 * c.gammap1 * du;
-    const double ztmp1 = c.q1 * zss;
-    const double zkur = ztmp2 + sqrt(ztmp2 * ztmp2 + ztmp1 * ztmp1);
-    double crmu = zkur * zrp * evol;
-    crmu = ((cdiv > 0.0) ? 0. : crmu);
-    const double2 cqe1 = sdiv(smul(crmu, sub(up0, upp)), de1);
-    const double2 cqe2 = sdiv(smul(crmu, sub(u02, up0)), de2);
+    // QCS::setQCnForce (QCS.cc:246-327): crmu is 0 wherever cdiv > 0
+    double crmu = 0.;
+    if (!(cdiv > 0.0)) {
+        const double ztmp2 = c.q2 * 0.25 * c.gammap1 * du;
+        const double ztmp1 = c.q1 * zss;
+        const double zkur = ztmp2 + sqrt(ztmp2 * ztmp2 + ztmp1 * ztmp1);
+        crmu = zkur * zrp * evol;
+    }
+    const double2 t1 = smul(crmu, sub(up0, upp));
+    const double2 cqe1 = mk(t1.x * rinv_de1, t1.y * rinv_de1);   // / elen[s]
+    const double2 t2 = smul(crmu, sub(u02, up0));
+    const double2 cqe2 = mk(t2.x * rinv_el, t2.y * rinv_el);     // / elen[s2]
 
     // QCS::setForce (QCS.cc:331-380): side s uses corners s and mapss4[s]
     const double csin2 = 1.0 - ccos * ccos;
@@ -267,9 +286,8 @@ __global__ void __launch_bounds__(kZoneThreads) pass_a(DevArrays a, HydroConst c
     const double ccos2 = shfl(ccos, ln);
     const double2 cqe12 = shfl2(cqe1, ln);
     const double2 cqe22 = shfl2(cqe2, ln);
-    const double2 sfq = sdiv(add(smul(cw, add(cqe2, smul(ccos, cqe1))),
-                                 smul(cw2, add(cqe12, smul(ccos2, cqe22)))),
-                             elen);
+    const double2 fs = add(smul(cw, add(cqe2, smul(ccos, cqe1))), smul(cw2, add(cqe12, smul(ccos2, cqe22))));
+    const double2 sfq = mk(fs.x * rinv_el, fs.y * rinv_el);      // / elen[s]
 
     // QCS::setVelDiff (QCS.cc:384-448)
     const double2 dxs = sub(xp2, xp);
@@ -290,11 +308,9 @@ __global__ void __launch_bounds__(kZoneThreads) pass_a(DevArrays a, HydroConst c
     const double2 cf = sub(ftot, ftot3);
 
     if (act) {
-        a.cmass[s] = cmass;
         a.cforce[s] = cf;
         a.sftot[s] = add(sfp, sfq);
     }
-    if (zok && k == 0) a.zp[z] = zp;
 
     const int nbad = __syncthreads_count(bad);
     block_fold<true>(zdthyd, a.part_dtnew + blockIdx.x);
@@ -406,20 +422,20 @@ __global__ void __launch_bounds__(kZoneThreads) pass_c(DevArrays a, HydroConst c
     const double zetot = zsum_from(zetot0, dwork, g, n);
     const double zw = zsum(dwork, g, n);
     // calcWorkRate (Hydro.cc:1483-1510), calcEnergy (:1545-1564), calcRho (:1034-1054)
-    const double dtinv = 1. / dt;
+    const double dtinv = ctl->dtinv;   // 1./dt, formed once per cycle
     const double dvol = zvol - zvol0;
     const double zwrate = (zw + zp * dvol) * dtinv;
-    const double ze = zetot / (zm + 1.e-99);
-    const double zr = zm / zvol;
-    // calcDvol (Hydro.cc:1622-1644), per zone
-    const double zdvov = zok ? fabs((zvol - zvol0) / zvol0) : 1.e-99;
+    // calcRho, calcEnergy and calcDvol (Hydro.cc:1622-1644) quotients, one
+    // per lane: lane 0 zr, lane 1 ze, lane 2 dV/V0
+    const double qv = ((k == 0) ? zm : (k == 1 ? zetot : zvol - zvol0)) /
+                      ((k == 0) ? zvol : (k == 1 ? zm + 1.e-99 : zvol0));
+    const double zdvov = (zok && k == 2) ? fabs(qv) : 1.e-99;
 
     __syncwarp();   // every lane's zone loads precede the in-place stores
     if (zok) {
-        if (k == 0) a.zvol[z] = zvol;
-        else if (k == 1) a.zetot[z] = zetot;
+        if (k == 0) { a.zvol[z] = zvol; a.zr[z] = qv; }
+        else if (k == 1) { a.zetot[z] = zetot; a.ze[z] = qv; }
         else if (k == 2) a.zwrate[z] = zwrate;
-        else { a.ze[z] = ze; a.zr[z] = zr; }
     }
     const int nbad = __syncthreads_count(bad);
     block_fold<false>(zdvov, a.part_dvov + blockIdx.x);
@@ -494,6 +510,7 @@ __global__ void __launch_bounds__(kFinThreads) finalize(DevArrays a, HydroConst 
     if ((c.tstop - time) < ndt) ndt = c.tstop - time;
     if (dtrec < ndt) ndt = dtrec;
     ctl->dt = ndt;
+    ctl->dtinv = 1. / ndt;
 }
 
 }  // namespace
