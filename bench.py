@@ -10,6 +10,11 @@ barrier + synchronize on both sides, max over ranks).  With N > 1 (torchrun,
 one rank per GPU) each rank runs an independent replica: the single-mesh
 path has no multi-GPU decomposition in this build, so scaling is weak.
 
+The headline path is the mixed-precision cycle (FP32 side forces, FP64
+kinematics/volumes/work/dt; `--precision fp64` selects the plain cycle); the
+plain FP64 cycle is timed beside it on the same deck and the headline path's
+relative L1 errors against it are reported.
+
 `e2e` runs the same K cycles through the C ABI from host buffers: state
 uploaded from pinned host memory, one pnt_hydro_cycle call per step (each
 returns that step's dt/time to the host), final fields downloaded.
@@ -183,6 +188,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--deck", default=DEFAULT_DECK)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="path of the headline value; the plain FP64 cycle is always timed beside it")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()
@@ -205,12 +212,14 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
 
-    deck = pb.Deck(path=args.deck)
-    params = deck.params()
-    mesh = pb.Mesh(deck=deck)
-    h = pb.Hydro(mesh, params, device=local_rank)
+    mesh = pb.Mesh(deck=pb.Deck(path=args.deck))
     nump, numz, nums = mesh.nump, mesh.numz, mesh.nums
     ab = algorithmic_bytes(nump, nums, numz)
+
+    def make(precision):
+        d = pb.Deck(path=args.deck)
+        d.set("precision", precision)
+        return pb.Hydro(mesh, d.params(), device=local_rank)
 
     def barrier_sync():
         torch.cuda.synchronize()
@@ -218,76 +227,120 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    # warm-up: graph capture + W cycles
-    h.time_cycles(args.warmup)
-    barrier_sync()
-    gpu_index = os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)).split(",")[local_rank if world > 1 else 0]
-    with ClockSampler(gpu_index) as clk:
-        barrier_sync()
-        ms = h.time_cycles(args.steps)
-        barrier_sync()
-    clocks = clk.summary()
-    s = h.scalars()
-    if s["status"] or s["cycle"] < args.warmup + args.steps:
-        raise SystemExit(f"run stopped early: {s}")
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * numz * args.steps / (ms_max / 1e3)
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
 
-    # per-pass device times (CUDA events around each pass, separate launches)
-    kms = h.time_kernels(10)
+    gpu_index = os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)).split(",")[local_rank if world > 1 else 0]
+
+    def timed(h, sample_clocks):
+        h.time_cycles(args.warmup)      # graph capture + W cycles
+        barrier_sync()
+        clocks = None
+        if sample_clocks:
+            with ClockSampler(gpu_index) as clk:
+                barrier_sync()
+                ms = h.time_cycles(args.steps)
+                barrier_sync()
+            clocks = clk.summary()
+        else:
+            barrier_sync()
+            ms = h.time_cycles(args.steps)
+            barrier_sync()
+        s = h.scalars()
+        if s["status"] or s["cycle"] < args.warmup + args.steps:
+            raise SystemExit(f"run stopped early: {s}")
+        return max_over_ranks(ms), clocks
+
     names = ["A", "B", "C", "finalize"]
-    dom = int(np.argmax(kms[:3]))
+    head = make(args.precision)
+    ms_head, clocks = timed(head, True)
+    kms_head = head.time_kernels(10)
+    if args.precision == "fp64":
+        ref64, ms_64, kms_64 = head, ms_head, kms_head
+    else:
+        ref64 = make("fp64")
+        ms_64, _ = timed(ref64, False)
+        kms_64 = ref64.time_kernels(10)
+    value = world * numz * args.steps / (ms_head / 1e3)
+    value_64 = world * numz * args.steps / (ms_64 / 1e3)
+
+    # accuracy of the headline path against the FP64 cycle after the same
+    # number of cycles (the FP64 cycle is bit-identical to the CPU oracle)
+    def l1(a, b):
+        return float(np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300))
+
+    err = None
+    if ref64 is not head:
+        c1, c2 = head.scalars()["cycle"], ref64.scalars()["cycle"]
+        assert c1 == c2, (c1, c2)
+        err = {"zr": l1(head.download("zr"), ref64.download("zr")),
+               "ze": l1(head.download("ze"), ref64.download("ze")),
+               "u": l1(np.hypot(*head.download("pu").T), np.hypot(*ref64.download("pu").T)),
+               "cycles": c1, "time": head.scalars()["time"]}
+        ref64.close()
+
     hbm, peak_kind = measured_peaks()
-    ach_dom = ab[names[dom]] / (kms[dom] / 1e3) / 1e9
-    ach_cycle = ab["cycle"] * args.steps / (ms / 1e3) / 1e9
+    dom = int(np.argmax(kms_head[:3]))
+    if args.precision == "mixed":
+        per_launch = {"A": 32 * nump + 44 * numz + 32 * nums, "B": 68 * nump + 16 * nums,
+                      "C": 64 * nump + 12 * nums + 60 * numz}
+    else:
+        per_launch = {k: ab[k] for k in ("A", "B", "C")}
+    ach_dom = per_launch[names[dom]] / (kms_head[dom] / 1e3) / 1e9
+    ach_cycle = ab["cycle"] * args.steps / (ms_head / 1e3) / 1e9
 
     # end to end through the C ABI with pinned host buffers
     fields = ["px", "pu", "zr", "ze", "zm", "zetot", "zwrate", "zvol"]
     host = {}
     for k in fields:
-        arr = h.download(k)
+        arr = head.download(k)
         pin = torch.empty(arr.shape, dtype=torch.float64, pin_memory=True).numpy()
         pin[...] = arr
         host[k] = pin
-    outs = {k: torch.empty(h._shape(k), dtype=torch.float64, pin_memory=True).numpy()
+    outs = {k: torch.empty(head._shape(k), dtype=torch.float64, pin_memory=True).numpy()
             for k in ("zr", "ze", "zp", "px", "pu")}
     barrier_sync()
     t0 = time.perf_counter()
     for k in fields:
-        pb.check(pb.lib.pnt_hydro_upload(h.h, pb.FIELDS[k], host[k].ctypes.data, host[k].nbytes))
+        pb.check(pb.lib.pnt_hydro_upload(head.h, pb.FIELDS[k], host[k].ctypes.data, host[k].nbytes))
     for _ in range(args.steps):
-        h.cycle()
+        head.cycle()
     for k, arr in outs.items():
-        pb.check(pb.lib.pnt_hydro_download(h.h, pb.FIELDS[k], arr.ctypes.data, arr.nbytes))
+        pb.check(pb.lib.pnt_hydro_download(head.h, pb.FIELDS[k], arr.ctypes.data, arr.nbytes))
     barrier_sync()
-    e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_s = float(te.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
     h2d = sum(a.nbytes for a in host.values())
     d2h = sum(a.nbytes for a in outs.values()) + 72 * args.steps
+    head.close()
 
     result = None
     if rank == 0:
+        path = ("mixed precision: FP32 edge/corner geometry and TTS/QCS side forces, FP64 point kinematics, "
+                "volumes, EOS, work and dt; plain QCS" if args.precision == "mixed"
+                else "plain FP64 (bitwise parity path)")
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "warmup": args.warmup, "ms_per_step": ms_head / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
             "config": {"workload": f"{os.path.basename(args.deck)} ({numz} zones, {nums} sides, {nump} points)",
-                       "path": "plain FP64 (bitwise parity path)", "cycles_per_step": 1,
-                       "parallelism": f"replicas x{world}",
-                       "l2": "working set ~1.3 GB per GPU >> 126 MB L2 (no flush needed)"},
-            "roofline": {"bound": "hbm", "kernel": f"pass {names[dom]}", "achieved": ach_dom, "peak": hbm,
-                         "unit": "GB/s", "frac": ach_dom / hbm, "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": ab[names[dom]], "launch_ms": kms[dom],
+                       "path": path, "cycles_per_step": 1, "parallelism": f"replicas x{world}",
+                       "l2": "working set > 1 GB per GPU >> 126 MB L2 (no flush needed)",
+                       "fp64_plain": {"value": value_64, "ms_per_step": ms_64 / args.steps,
+                                      "kernel_ms": dict(zip(names, kms_64))},
+                       "speedup_vs_fp64": value / value_64,
+                       "l1_rel_err_vs_fp64": err},
+            "roofline": {"bound": "hbm", "kernel": f"pass {names[dom]} ({args.precision})", "achieved": ach_dom,
+                         "peak": hbm, "unit": "GB/s", "frac": ach_dom / hbm, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": per_launch[names[dom]], "launch_ms": kms_head[dom],
                          "traffic": None},
             "roofline_cycle": {"achieved": ach_cycle, "peak": hbm, "unit": "GB/s", "frac": ach_cycle / hbm,
-                               "algorithmic_bytes_per_cycle": ab["cycle"]},
-            "kernel_ms": dict(zip(names, kms)),
+                               "algorithmic_bytes_per_cycle": ab["cycle"],
+                               "note": "FP64 schedule bytes B = 164 Np + 100 Ns + 104 Nz for every path"},
+            "kernel_ms": dict(zip(names, kms_head)),
             "e2e": {"value": world * numz * args.steps / e2e_s, "unit": UNIT,
                     "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                     "note": "state uploaded from pinned host memory once per timed run, one pnt_hydro_cycle "
@@ -296,7 +349,6 @@ def main():
             "gpu_launches": 4 * args.steps,
             "clocks": clocks,
         }
-    h.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -55,6 +55,8 @@ struct pnt_hydro {
     // captured CUDA graph of graph_cycles cycles
     cudaGraphExec_t graph = nullptr;
     int graph_cycles = 0;
+    // the cycle of the selected precision
+    cudaError_t (*launch)(const DevArrays&, const HydroConst&, cudaStream_t, cudaEvent_t*) = launch_cycle_fp64;
 
     ~pnt_hydro() {
         DeviceGuard dg(device);
@@ -80,7 +82,7 @@ struct pnt_hydro {
 
     pnt_status launch_cycles(int n) {
         for (int i = 0; i < n; ++i) {
-            const cudaError_t e = launch_cycle_fp64(a, hc, stream);
+            const cudaError_t e = launch(a, hc, stream, nullptr);
             if (e != cudaSuccess) return fail(PNT_ERR_CUDA, "cycle launch: %s", cudaGetErrorString(e));
         }
         return PNT_OK;
@@ -92,7 +94,7 @@ struct pnt_hydro {
         cudaGraph_t g = nullptr;
         CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         for (int i = 0; i < graph_cycles; ++i) {
-            const cudaError_t e = launch_cycle_fp64(a, hc, stream);
+            const cudaError_t e = launch(a, hc, stream, nullptr);
             if (e != cudaSuccess) {
                 cudaStreamEndCapture(stream, &g);
                 if (g) cudaGraphDestroy(g);
@@ -245,6 +247,7 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
     double* smf;
     uint16_t* mask;
     const int64_t nzb = zone_blocks((int32_t)nz);
+    const int64_t nzbc = zone_blocks((int32_t)nz, kZoneThreadsC);
     pnt_status st = PNT_OK;
     if ((st = h->alloc(&zfirst, nz)) || (st = h->alloc(&znump, nz)) || (st = h->alloc(&mapsp1, ns)) ||
         (st = h->alloc(&smf, ns)) || (st = h->alloc(&poff, np + 1)) || (st = h->alloc(&pcorner, ns)) ||
@@ -254,9 +257,14 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
         (st = h->alloc(&a.zwrate, nz)) || (st = h->alloc(&a.zvol, nz)) || (st = h->alloc(&a.zp, nz)) ||
         (st = h->alloc(&a.cmass, ns)) || (st = h->alloc(&a.cforce, ns)) || (st = h->alloc(&a.sftot, ns)) ||
         (st = h->alloc(&a.part_dtnew, nzb)) || (st = h->alloc(&a.part_badA, nzb)) ||
-        (st = h->alloc(&a.part_dvov, nzb)) || (st = h->alloc(&a.part_badC, nzb)) ||
+        (st = h->alloc(&a.part_dvov, nzbc)) || (st = h->alloc(&a.part_badC, nzbc)) ||
         (st = h->alloc(&a.ctl, 1)))
         return st;
+    a.npartA = (int32_t)nzb;
+    a.npartC = (int32_t)nzbc;
+    a.cmass_f = reinterpret_cast<float*>(a.cmass);
+    a.cforce_f = reinterpret_cast<float2*>(a.cforce);
+    a.sftot_f = reinterpret_cast<float2*>(a.sftot);
     a.zfirst = zfirst;
     a.znump = znump;
     a.mapsp1 = mapsp1;
@@ -323,8 +331,6 @@ pnt_status pnt_hydro_create(const pnt_mesh* mesh, const pnt_params* params, int3
     *out = nullptr;
     if (params->precision != PNT_PREC_FP64 && params->precision != PNT_PREC_MIXED)
         return fail(PNT_ERR_INVALID_ARG, "unknown precision %d", params->precision);
-    if (params->precision == PNT_PREC_MIXED)
-        return fail(PNT_ERR_UNSUPPORTED, "precision mixed is not available in this build");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
         cudaGetLastError();
@@ -336,6 +342,7 @@ pnt_status pnt_hydro_create(const pnt_mesh* mesh, const pnt_params* params, int3
     if (!h) return fail(PNT_ERR_NOMEM, "out of memory");
     h->device = device;
     h->params = *params;
+    h->launch = (params->precision == PNT_PREC_MIXED) ? launch_cycle_mixed : launch_cycle_fp64;
     pnt_status st = PNT_OK;
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMallocHost((void**)&h->ctl_host, sizeof(Ctl));
@@ -429,7 +436,7 @@ pnt_status pnt_hydro_time_kernels(pnt_hydro* h, int32_t ncycles, double* kernel_
         if (cudaEventCreate(&e) != cudaSuccess) { st = fail(PNT_ERR_CUDA, "cudaEventCreate failed"); break; }
     }
     for (int32_t i = 0; i < ncycles && !st; ++i) {
-        const cudaError_t e = launch_cycle_fp64(h->a, h->hc, h->stream, &ev[(size_t)i * (kNumPasses + 1)]);
+        const cudaError_t e = h->launch(h->a, h->hc, h->stream, &ev[(size_t)i * (kNumPasses + 1)]);
         if (e != cudaSuccess) st = fail(PNT_ERR_CUDA, "cycle launch: %s", cudaGetErrorString(e));
     }
     if (!st && cudaStreamSynchronize(h->stream) != cudaSuccess) st = fail(PNT_ERR_CUDA, "synchronize failed");

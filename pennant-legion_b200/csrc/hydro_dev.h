@@ -64,7 +64,12 @@ struct DevArrays {
     double* cmass;               // corner mass of side s at point mapsp1[s]
     double2* cforce;             // corner force of side s at point mapsp1[s]
     double2* sftot;              // sfp + sfq of side s (calcWork)
-    // per-block partial reductions
+    // the same buffers in FP32 for the mixed-precision cycle
+    float* cmass_f;
+    float2* cforce_f;
+    float2* sftot_f;
+    // per-block partial reductions (npartA entries for pass A, npartC for C)
+    int32_t npartA, npartC;
     double* part_dtnew;
     int32_t* part_badA;
     double* part_dvov;
@@ -72,11 +77,15 @@ struct DevArrays {
     Ctl* ctl;
 };
 
-constexpr int kZoneThreads = 256;   // 64 zones x 4 side lanes per block
+#ifndef PNT_ZONE_THREADS_C
+#define PNT_ZONE_THREADS_C 128
+#endif
+constexpr int kZoneThreads = 256;   // pass A: 64 zones x 4 side lanes per block
+constexpr int kZoneThreadsC = PNT_ZONE_THREADS_C;   // pass C: 32 zones per block
 constexpr int kPointThreads = 256;
 
-inline int64_t zone_blocks(int32_t numz) {
-    return (4 * (int64_t)numz + kZoneThreads - 1) / kZoneThreads;
+inline int64_t zone_blocks(int32_t numz, int threads = kZoneThreads) {
+    return (4 * (int64_t)numz + threads - 1) / threads;
 }
 
 constexpr int kNumPasses = 4;   // A, B, C, finalize
@@ -86,5 +95,10 @@ constexpr int kNumPasses = 4;   // A, B, C, finalize
 // the last one.
 cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStream_t stream,
                               cudaEvent_t* ev = nullptr);
+// The mixed-precision cycle (hydro_mixed.cu).
+cudaError_t launch_cycle_mixed(const DevArrays& a, const HydroConst& c, cudaStream_t stream,
+                               cudaEvent_t* ev = nullptr);
+// The finalize step shared by both cycles (nA / nC partials of passes A / C).
+void launch_finalize(const DevArrays& a, const HydroConst& c, int nA, int nC, cudaStream_t stream);
 
 }  // namespace pnt

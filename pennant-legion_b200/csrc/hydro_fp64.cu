@@ -23,7 +23,7 @@
 // 1/elen is formed once per side and shared with the neighbouring corner;
 // QCS terms the reference computes and then discards (evol and du unless
 // cdiv < 0, zkur when cdiv > 0) are not computed, which leaves every stored
-// value unchanged.  Pass A is capped at 80 registers (3 blocks per SM): it
+// value unchanged.  Pass A is capped at 64 registers (4 blocks per SM): it
 // is latency bound and gains more from the extra warps than it loses to
 // the few spilled registers.  This file is compiled with -fmad=false
 // and every expression keeps the reference's operation order, including
@@ -110,9 +110,9 @@ __device__ __forceinline__ bool skip_cycle(const Ctl* ctl) {
 
 // Block-wide min (dt) / max (dvov) in the reference fold semantics, and a
 // count.  Writes one partial per block.
-template <bool kMin>
+template <bool kMin, int kThreads>
 __device__ __forceinline__ void block_fold(double v, double* out) {
-    __shared__ double red[kZoneThreads / 32];
+    __shared__ double red[kThreads / 32];
     for (int o = 16; o > 0; o >>= 1) {
         const double w = __shfl_xor_sync(kFull, v, o);
         v = kMin ? dmin(v, w) : ((w > v) ? w : v);
@@ -122,7 +122,7 @@ __device__ __forceinline__ void block_fold(double v, double* out) {
     __syncthreads();
     if (threadIdx.x == 0) {
         double r = red[0];
-        for (int i = 1; i < kZoneThreads / 32; ++i) r = kMin ? dmin(r, red[i]) : ((red[i] > r) ? red[i] : r);
+        for (int i = 1; i < kThreads / 32; ++i) r = kMin ? dmin(r, red[i]) : ((red[i] > r) ? red[i] : r);
         *out = r;
     }
 }
@@ -131,7 +131,10 @@ __device__ __forceinline__ void block_fold(double v, double* out) {
 // Pass A: predictor zone pass
 // ---------------------------------------------------------------------
 template <bool kQuads>
-__global__ void __launch_bounds__(kZoneThreads, 3) pass_a(DevArrays a, HydroConst c) {
+#ifndef PNT_PASS_A_MIN_BLOCKS
+#define PNT_PASS_A_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(kZoneThreads, PNT_PASS_A_MIN_BLOCKS) pass_a(DevArrays a, HydroConst c) {
     const Ctl* ctl = a.ctl;
     if (skip_cycle(ctl)) return;
     const int cur = ctl->cycle & 1;
@@ -313,7 +316,8 @@ __global__ void __launch_bounds__(kZoneThreads, 3) pass_a(DevArrays a, HydroCons
     }
 
     const int nbad = __syncthreads_count(bad);
-    block_fold<true>(zdthyd, a.part_dtnew + blockIdx.x);
+    if (blockIdx.x >= (unsigned)a.npartA) return;   // partials are sized for this grid
+    block_fold<true, kZoneThreads>(zdthyd, a.part_dtnew + blockIdx.x);
     if (threadIdx.x == 0) a.part_badA[blockIdx.x] = nbad;
 }
 
@@ -361,13 +365,13 @@ __global__ void __launch_bounds__(kPointThreads) pass_b(DevArrays a, HydroConst 
 // Pass C: corrector zone pass
 // ---------------------------------------------------------------------
 template <bool kQuads>
-__global__ void __launch_bounds__(kZoneThreads) pass_c(DevArrays a, HydroConst c) {
+__global__ void __launch_bounds__(kZoneThreadsC) pass_c(DevArrays a, HydroConst c) {
     const Ctl* ctl = a.ctl;
     if (skip_cycle(ctl)) return;
     const int cur = ctl->cycle & 1;
     const double dt = ctl->dt;
 
-    const int64_t tid = (int64_t)blockIdx.x * kZoneThreads + threadIdx.x;
+    const int64_t tid = (int64_t)blockIdx.x * kZoneThreadsC + threadIdx.x;
     const int64_t z = tid >> 2;
     const int k = (int)(tid & 3);
     const int lane = threadIdx.x & 31;
@@ -438,7 +442,8 @@ __global__ void __launch_bounds__(kZoneThreads) pass_c(DevArrays a, HydroConst c
         else if (k == 2) a.zwrate[z] = zwrate;
     }
     const int nbad = __syncthreads_count(bad);
-    block_fold<false>(zdvov, a.part_dvov + blockIdx.x);
+    if (blockIdx.x >= (unsigned)a.npartC) return;   // partials are sized for this grid
+    block_fold<false, kZoneThreadsC>(zdvov, a.part_dvov + blockIdx.x);
     if (threadIdx.x == 0) a.part_badC[blockIdx.x] = nbad;
 }
 
@@ -448,16 +453,20 @@ __global__ void __launch_bounds__(kZoneThreads) pass_c(DevArrays a, HydroConst c
 // ---------------------------------------------------------------------
 constexpr int kFinThreads = 1024;
 
-__global__ void __launch_bounds__(kFinThreads) finalize(DevArrays a, HydroConst c, int nblocks) {
+__global__ void __launch_bounds__(kFinThreads) finalize(DevArrays a, HydroConst c, int nblocksA, int nblocksC) {
     Ctl* ctl = a.ctl;
     if (skip_cycle(ctl)) return;
     double dtn = 1.e99, dvm = 1.e-99;
     int badA = 0, badC = 0;
-    for (int i = threadIdx.x; i < nblocks; i += kFinThreads) {
+#pragma unroll 4
+    for (int i = threadIdx.x; i < nblocksA; i += kFinThreads) {
         dtn = dmin(dtn, a.part_dtnew[i]);
+        badA += a.part_badA[i];
+    }
+#pragma unroll 4
+    for (int i = threadIdx.x; i < nblocksC; i += kFinThreads) {
         const double v = a.part_dvov[i];
         dvm = (v > dvm) ? v : dvm;
-        badA += a.part_badA[i];
         badC += a.part_badC[i];
     }
     __shared__ double sdt[kFinThreads / 32], sdv[kFinThreads / 32];
@@ -517,6 +526,7 @@ __global__ void __launch_bounds__(kFinThreads) finalize(DevArrays a, HydroConst 
 
 cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStream_t stream, cudaEvent_t* ev) {
     const int zb = (int)zone_blocks(a.numz);
+    const int zbc = (int)zone_blocks(a.numz, kZoneThreadsC);
     const int pb = (int)((a.nump + kPointThreads - 1) / kPointThreads);
     if (ev) cudaEventRecord(ev[0], stream);
     if (a.quads) pass_a<true><<<zb, kZoneThreads, 0, stream>>>(a, c);
@@ -524,12 +534,16 @@ cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStrea
     if (ev) cudaEventRecord(ev[1], stream);
     pass_b<<<pb, kPointThreads, 0, stream>>>(a, c);
     if (ev) cudaEventRecord(ev[2], stream);
-    if (a.quads) pass_c<true><<<zb, kZoneThreads, 0, stream>>>(a, c);
-    else pass_c<false><<<zb, kZoneThreads, 0, stream>>>(a, c);
+    if (a.quads) pass_c<true><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
+    else pass_c<false><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
     if (ev) cudaEventRecord(ev[3], stream);
-    finalize<<<1, kFinThreads, 0, stream>>>(a, c, zb);
+    finalize<<<1, kFinThreads, 0, stream>>>(a, c, zb, zbc);
     if (ev) cudaEventRecord(ev[4], stream);
     return cudaGetLastError();
+}
+
+void launch_finalize(const DevArrays& a, const HydroConst& c, int nA, int nC, cudaStream_t stream) {
+    finalize<<<1, kFinThreads, 0, stream>>>(a, c, nA, nC);
 }
 
 }  // namespace pnt

@@ -1,0 +1,395 @@
+// hydro_mixed.cu -- the mixed-precision hydro cycle (precision = mixed).
+//
+// Same passes and data flow as the FP64 cycle (hydro_fp64.cu), with the
+// per-side work of the predictor in FP32:
+//
+//   FP64  point positions and velocities (advPosHalf, advPosFull), the
+//         zone centre, side areas and RZ volumes with their zone sums (the
+//         half-step volume change zvolp - zvol0 of PolyGas::calcStateHalf
+//         would cancel in FP32), the zone EOS, calcRho, the corner-mass and
+//         corner-force sums at points, calcWork/calcWorkRate/calcEnergy and
+//         the dt reduction;
+//   FP32  edge lengths, surface vectors, characteristic lengths, the TTS
+//         side force and every QCS corner quantity, formed in coordinates
+//         relative to the zone's first point so that FP32 keeps its
+//         precision on small zones far from the origin.
+//
+// Side results handed to the point and corrector passes are stored in FP32
+// (corner mass 4 B, corner force 8 B, sfp + sfq 8 B per side instead of
+// 40 B).  Compiled with fast math; the accuracy of this path is stated as
+// its L1 error against the FP64 run (tests/test_gpu_mixed.py).
+#include "hydro_dev.h"
+
+#include <cuda_runtime.h>
+
+namespace pnt {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ double2 mk(double x, double y) { return make_double2(x, y); }
+__device__ __forceinline__ double2 add(double2 a, double2 b) { return mk(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 sub(double2 a, double2 b) { return mk(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 smul(double r, double2 v) { return mk(v.x * r, v.y * r); }
+__device__ __forceinline__ double2 neg(double2 a) { return mk(-a.x, -a.y); }
+__device__ __forceinline__ double dot(double2 a, double2 b) { return a.x * b.x + a.y * b.y; }
+__device__ __forceinline__ double cross(double2 a, double2 b) { return a.x * b.y - a.y * b.x; }
+__device__ __forceinline__ double2 project(double2 v, double ux, double uy) {
+    const double d = v.x * ux + v.y * uy;
+    return mk(v.x - ux * d, v.y - uy * d);
+}
+__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }
+
+__device__ __forceinline__ float2 fk(float x, float y) { return make_float2(x, y); }
+__device__ __forceinline__ float2 fadd(float2 a, float2 b) { return fk(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 fsub(float2 a, float2 b) { return fk(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 fmul(float r, float2 v) { return fk(v.x * r, v.y * r); }
+__device__ __forceinline__ float fdot(float2 a, float2 b) { return a.x * b.x + a.y * b.y; }
+__device__ __forceinline__ float fcross(float2 a, float2 b) { return a.x * b.y - a.y * b.x; }
+__device__ __forceinline__ float flen(float2 v) { return sqrtf(v.x * v.x + v.y * v.y); }
+__device__ __forceinline__ float flen2(float2 v) { return v.x * v.x + v.y * v.y; }
+__device__ __forceinline__ float2 f2(double2 v) { return fk((float)v.x, (float)v.y); }
+
+__device__ __forceinline__ double shfl(double v, int src) { return __shfl_sync(kFull, v, src); }
+__device__ __forceinline__ float shflf(float v, int src) { return __shfl_sync(kFull, v, src); }
+__device__ __forceinline__ double2 shfl2(double2 v, int src) {
+    return mk(__shfl_sync(kFull, v.x, src), __shfl_sync(kFull, v.y, src));
+}
+__device__ __forceinline__ float2 shflf2(float2 v, int src) {
+    return fk(__shfl_sync(kFull, v.x, src), __shfl_sync(kFull, v.y, src));
+}
+
+template <typename T>
+__device__ __forceinline__ T zsum4(T v, int g, int n) {
+    T s = __shfl_sync(kFull, v, g);
+    s += __shfl_sync(kFull, v, g + 1);
+    s += __shfl_sync(kFull, v, g + 2);
+    const T d = __shfl_sync(kFull, v, g + 3);
+    if (n == 4) s += d;
+    return s;
+}
+
+__device__ __forceinline__ bool skip_cycle(const Ctl* ctl) {
+    return ctl->done || ctl->cycle >= ctl->stop_at;
+}
+
+template <bool kMin, int kThreads>
+__device__ __forceinline__ void block_fold(double v, double* out) {
+    __shared__ double red[kThreads / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+        const double w = __shfl_xor_sync(kFull, v, o);
+        v = kMin ? dmin(v, w) : ((w > v) ? w : v);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = red[0];
+        for (int i = 1; i < kThreads / 32; ++i) r = kMin ? dmin(r, red[i]) : ((red[i] > r) ? red[i] : r);
+        *out = r;
+    }
+}
+
+// ---------------------------------------------------------------------
+// Pass A, mixed precision
+// ---------------------------------------------------------------------
+template <bool kQuads>
+__global__ void __launch_bounds__(kZoneThreads, 3) pass_a_mixed(DevArrays a, HydroConst c) {
+    const Ctl* ctl = a.ctl;
+    if (skip_cycle(ctl)) return;
+    const int cur = ctl->cycle & 1;
+    const double dt = ctl->dt;
+    const double2* __restrict__ px0 = a.px[cur];
+    const double2* __restrict__ pu0 = a.pu[cur];
+
+    const int64_t tid = (int64_t)blockIdx.x * kZoneThreads + threadIdx.x;
+    const int64_t z = tid >> 2;
+    const int k = (int)(tid & 3);
+    const int lane = threadIdx.x & 31;
+    const int g = lane & ~3;
+    const bool zok = z < a.numz;
+    int n = 4;
+    int64_t s = 4 * z + k;
+    if (!kQuads) {
+        n = zok ? a.znump[z] : 4;
+        s = (zok ? (int64_t)a.zfirst[z] : 0) + k;
+    }
+    const bool act = zok && k < n;
+    const int lp = g + (k == 0 ? n - 1 : k - 1);
+    const int ln = g + (k + 1 >= n ? 0 : k + 1);
+
+    const int32_t p1 = act ? __ldg(a.mapsp1 + s) : 0;
+    const double2 x0 = act ? px0[p1] : mk(0., 0.);
+    const double2 u0 = act ? pu0[p1] : mk(0., 0.);
+    const double mf = act ? __ldg(a.smf + s) : 0.;
+    const double zm = zok ? a.zm[z] : 1.;
+    const double zr = zok ? a.zr[z] : 1.;
+    const double ze = zok ? a.ze[z] : 0.;
+    const double zwrate = zok ? a.zwrate[z] : 0.;
+    const double zvol0 = zok ? a.zvol[z] : 1.;
+
+    // FP64: positions, zone centre, side areas and volumes
+    const double dth = 0.5 * dt;
+    const double2 xp = add(x0, smul(dth, u0));
+    const double2 xp2 = shfl2(xp, ln);
+    const double rn = 1. / (double)n;
+    const double2 zxp = mk(zsum4(xp.x * rn, g, n), zsum4(xp.y * rn, g, n));
+    const double third = 1. / 3.;
+    const double sa = 0.5 * cross(sub(xp2, xp), sub(zxp, xp));
+    const double sv = third * sa * (xp.x + xp2.x + zxp.x);
+    const double zareap = zsum4(sa, g, n);
+    const double zvolp = zsum4(sv, g, n);
+    const bool bad = act && (sv <= 0.);
+
+    // FP64 zone EOS and density (PolyGas.cc:63-109, Hydro.cc:1034-1054),
+    // quotients split over the zone's lanes
+    const double e = dmax(ze, 0.);
+    const double p = c.gm1 * zr * e;
+    const double pre = c.gm1 * e;
+    const double per = c.gm1 * zr;
+    const double rA = ((k == 0) ? per * p : 1.) / ((k == 0) ? zr * zr : zm);
+    const double q = shfl(rA, g);
+    const double minv = shfl(rA, g + 1);
+    const double csqd = dmax(c.ssmin2, pre + q);
+    const double zss = sqrt(csqd);
+    const double dv = (zvolp - zvol0) * minv;
+    const double bulk = zr * csqd;
+    const double denom = 1. + 0.5 * per * dv;
+    const double src = zwrate * dth * minv;
+    const double rB = ((k == 0) ? zm : per * src - zr * bulk * dv) / ((k == 0) ? zvolp : denom);
+    const double zrp = shfl(rB, g);
+    const double zp = p + shfl(rB, g + 1);
+    const double mf3 = shfl(mf, lp);
+    if (act) a.cmass_f[s] = (float)(zrp * zareap * 0.5 * (mf + mf3));
+    if (zok && k == 0) a.zp[z] = zp;
+
+    // FP32 from here, relative to the zone's first point
+    const double2 xref = shfl2(xp, g);
+    const float2 r = f2(sub(xp, xref));
+    const float2 r2 = shflf2(r, ln);
+    const float2 zc = f2(sub(zxp, xref));
+    const float2 uf = f2(u0);
+    const float2 u2f = shflf2(uf, ln);
+    const float2 upf = shflf2(uf, lp);
+    const float rnf = (float)rn;
+    const float2 zuc = fk(zsum4(uf.x * rnf, g, n), zsum4(uf.y * rnf, g, n));
+    const float2 ex = fmul(0.5f, fadd(r, r2));
+    const float2 ssurf = fk(-(ex.y - zc.y), ex.x - zc.x);
+    const float elen = flen(fsub(r2, r));
+    const float saf = (float)sa;
+    const float fac = (n == 3 ? 3.f : 4.f);
+    // zone minimum over the group's 4 lanes; the idle lane of a triangle
+    // contributes +inf
+    float zdl = act ? fac * saf / elen : __int_as_float(0x7f800000);
+    zdl = fminf(zdl, __shfl_xor_sync(kFull, zdl, 1));
+    zdl = fminf(zdl, __shfl_xor_sync(kFull, zdl, 2));
+    const float rinv_el = 1.f / elen;
+
+    const float zssf = (float)zss, zrpf = (float)zrp, zpf = (float)zp;
+    const float2 sfp = fmul(-zpf, ssurf);
+    // TTS (TTS.cc:55-104)
+    const float srho = zrpf * (float)mf * ((float)zareap / saf);
+    float sstmp = fmaxf(zssf, (float)c.tts_ssmin);
+    sstmp = (float)c.alfa * sstmp * sstmp;
+    const float2 sft = fmul(-(sstmp * (srho - zrpf)), ssurf);
+
+    // QCS corner (QCS.cc:116-380), FP32
+    const float2 up0 = uf, xq0 = r;
+    const float2 up1 = fmul(0.5f, fadd(up0, u2f));
+    const float2 xq1 = ex;
+    const float2 up2 = zuc, xq2 = zc;
+    const float2 up3 = fmul(0.5f, fadd(upf, up0));
+    const float2 xq3 = shflf2(ex, lp);
+    const float cvolume = 0.5f * fcross(fsub(xq2, xq0), fsub(xq3, xq1));
+    const float2 v1 = fsub(xq3, xq0), v2 = fsub(xq1, xq0);
+    const float de1 = shflf(elen, lp), de2 = elen;
+    const float rinv_de1 = shflf(rinv_el, lp);
+    const float minelen = fminf(de1, de2);
+    float ccos = (minelen < 1.e-12f) ? 0.f : 4.f * fdot(v1, v2) / (de1 * de2);
+    const float cdiv = (fcross(fsub(up2, up0), fsub(xq3, xq1)) - fcross(fsub(up3, up1), fsub(xq2, xq0))) /
+                       (2.f * cvolume);
+    float crmu = 0.f;
+    if (cdiv < 0.f) {
+        const float2 dxx1 = fmul(0.5f, fsub(fsub(fadd(xq1, xq2), xq0), xq3));
+        const float2 dxx2 = fmul(0.5f, fsub(fsub(fadd(xq2, xq3), xq0), xq1));
+        const float dx1 = flen(dxx1), dx2 = flen(dxx2);
+        const float2 duav = fmul(0.25f, fadd(fadd(fadd(up0, up1), up2), up3));
+        const float test1 = fabsf(fdot(dxx1, duav) * dx2);
+        const float test2 = fabsf(fdot(dxx2, duav) * dx1);
+        const float rr = (test1 > test2) ? dx1 / dx2 : dx2 / dx1;
+        const float evol = fminf(sqrtf(4.f * cvolume * rr), 2.f * minelen);
+        const float du = sqrtf(fmaxf(flen2(fsub(fsub(fadd(up1, up2), up0), up3)),
+                                     flen2(fsub(fsub(fadd(up2, up3), up0), up1))));
+        const float ztmp2 = (float)(c.q2 * 0.25 * c.gammap1) * du;
+        const float ztmp1 = (float)c.q1 * zssf;
+        crmu = (ztmp2 + sqrtf(ztmp2 * ztmp2 + ztmp1 * ztmp1)) * zrpf * evol;
+    }
+    const float2 cqe1 = fmul(crmu * rinv_de1, fsub(up0, upf));
+    const float2 cqe2 = fmul(crmu * rinv_el, fsub(u2f, up0));
+    const float csin2 = 1.f - ccos * ccos;
+    const float cw = (csin2 < 1.e-4f) ? 0.f : cvolume / csin2;
+    ccos = (csin2 < 1.e-4f) ? 0.f : ccos;
+    const float cw2 = shflf(cw, ln), ccos2 = shflf(ccos, ln);
+    const float2 cqe12 = shflf2(cqe1, ln), cqe22 = shflf2(cqe2, ln);
+    const float2 sfq = fmul(rinv_el, fadd(fmul(cw, fadd(cqe2, fmul(ccos, cqe1))),
+                                          fmul(cw2, fadd(cqe12, fmul(ccos2, cqe22)))));
+
+    // QCS::setVelDiff, calcDtNew (FP64 reduction)
+    float dux = fabsf(fdot(fsub(u2f, uf), fsub(r2, r))) * rinv_el;
+    dux = (act && elen > 0.f) ? dux : 0.f;
+    float ztmp = fmaxf(dux, __shfl_xor_sync(kFull, dux, 1));
+    ztmp = fmaxf(ztmp, __shfl_xor_sync(kFull, ztmp, 2));   // idle triangle lanes carry 0
+    const double zdu = c.q1 * zss + 2. * c.q2 * (double)ztmp;
+    const double cdu = dmax(zdu, dmax(zss, 1.e-99));
+    const double zdthyd = zok ? (double)zdl * c.cfl / cdu : 1.e99;
+
+    const float2 sfpq = fadd(sfp, sfq);
+    const float2 ftot = fadd(sfpq, sft);
+    const float2 ftot3 = shflf2(ftot, lp);
+    if (act) {
+        a.cforce_f[s] = fsub(ftot, ftot3);
+        a.sftot_f[s] = sfpq;
+    }
+
+    const int nbad = __syncthreads_count(bad);
+    if (blockIdx.x >= (unsigned)a.npartA) return;   // partials are sized for this grid
+    block_fold<true, kZoneThreads>(zdthyd, a.part_dtnew + blockIdx.x);
+    if (threadIdx.x == 0) a.part_badA[blockIdx.x] = nbad;
+}
+
+// ---------------------------------------------------------------------
+// Pass B, mixed: FP32 corner inputs summed in FP64
+// ---------------------------------------------------------------------
+__global__ void __launch_bounds__(kPointThreads) pass_b_mixed(DevArrays a, HydroConst c) {
+    const Ctl* ctl = a.ctl;
+    if (skip_cycle(ctl)) return;
+    const int64_t p = (int64_t)blockIdx.x * kPointThreads + threadIdx.x;
+    if (p >= a.nump) return;
+    const int cur = ctl->cycle & 1;
+    const double dt = ctl->dt;
+    const double2 x0 = a.px[cur][p];
+    double2 u0 = a.pu[cur][p];
+    const int32_t o0 = a.poff[p], o1 = a.poff[p + 1];
+    double m = 0.;
+    double2 f = mk(0., 0.);
+    for (int32_t i = o0; i < o1; ++i) {
+        const int32_t s = __ldg(a.pcorner + i);
+        m += (double)a.cmass_f[s];
+        const float2 cf = a.cforce_f[s];
+        f = mk(f.x + (double)cf.x, f.y + (double)cf.y);
+    }
+    const unsigned mask = a.bcmask[p];
+    if (mask) {
+        for (int b = 0; b < c.nbc; ++b) {
+            if (mask & (1u << b)) {
+                u0 = project(u0, c.vfix[b][0], c.vfix[b][1]);
+                f = project(f, c.vfix[b][0], c.vfix[b][1]);
+            }
+        }
+    }
+    const double minv = 1. / dmax(m, 1.e-99);
+    const double2 pa = mk(f.x * minv, f.y * minv);
+    const double2 u = add(u0, smul(dt, pa));
+    const double2 x = add(x0, smul(dt * 0.5, add(u0, u)));
+    a.px[cur ^ 1][p] = x;
+    a.pu[cur ^ 1][p] = u;
+}
+
+// ---------------------------------------------------------------------
+// Pass C, mixed: FP64 corrector with the FP32 sfp + sfq input
+// ---------------------------------------------------------------------
+template <bool kQuads>
+__global__ void __launch_bounds__(kZoneThreadsC) pass_c_mixed(DevArrays a, HydroConst c) {
+    const Ctl* ctl = a.ctl;
+    if (skip_cycle(ctl)) return;
+    const int cur = ctl->cycle & 1;
+    const double dt = ctl->dt;
+    const int64_t tid = (int64_t)blockIdx.x * kZoneThreadsC + threadIdx.x;
+    const int64_t z = tid >> 2;
+    const int k = (int)(tid & 3);
+    const int lane = threadIdx.x & 31;
+    const int g = lane & ~3;
+    const bool zok = z < a.numz;
+    int n = 4;
+    int64_t s = 4 * z + k;
+    if (!kQuads) {
+        n = zok ? a.znump[z] : 4;
+        s = (zok ? (int64_t)a.zfirst[z] : 0) + k;
+    }
+    const bool act = zok && k < n;
+    const int ln = g + (k + 1 >= n ? 0 : k + 1);
+
+    const int32_t p1 = act ? __ldg(a.mapsp1 + s) : 0;
+    const double2 x0 = act ? a.px[cur][p1] : mk(0., 0.);
+    const double2 u0 = act ? a.pu[cur][p1] : mk(0., 0.);
+    const double2 x = act ? a.px[cur ^ 1][p1] : mk(0., 0.);
+    const double2 u = act ? a.pu[cur ^ 1][p1] : mk(0., 0.);
+    const unsigned mask = act ? a.bcmask[p1] : 0u;
+    const float2 sff = act ? a.sftot_f[s] : fk(0.f, 0.f);
+    const double2 sft = mk((double)sff.x, (double)sff.y);
+    const double zm = zok ? a.zm[z] : 1.;
+    const double zetot0 = zok ? a.zetot[z] : 0.;
+    const double zvol0 = zok ? a.zvol[z] : 1.;
+    const double zp = zok ? a.zp[z] : 0.;
+
+    const double dth = 0.5 * dt;
+    const double2 xp = add(x0, smul(dth, u0));
+    double2 u0b = u0;
+    if (mask) {
+        for (int b = 0; b < c.nbc; ++b)
+            if (mask & (1u << b)) u0b = project(u0b, c.vfix[b][0], c.vfix[b][1]);
+    }
+    const double2 x2 = shfl2(x, ln);
+    const double2 xp2 = shfl2(xp, ln);
+    const double2 u0b2 = shfl2(u0b, ln);
+    const double2 u2 = shfl2(u, ln);
+    const double rn = 1. / (double)n;
+    const double2 zx = mk(zsum4(x.x * rn, g, n), zsum4(x.y * rn, g, n));
+    const double third = 1. / 3.;
+    const double sa = 0.5 * cross(sub(x2, x), sub(zx, x));
+    const double sv = third * sa * (x.x + x2.x + zx.x);
+    const double zvol = zsum4(sv, g, n);
+    const bool bad = act && (sv <= 0.);
+    const double sd1 = dot(sft, add(u0b, u));
+    const double sd2 = dot(neg(sft), add(u0b2, u2));
+    const double dwork = -dth * (sd1 * xp.x + sd2 * xp2.x);
+    const double zw = zsum4(dwork, g, n);
+    const double zetot = zetot0 + zw;
+    const double zwrate = (zw + zp * (zvol - zvol0)) * ctl->dtinv;
+    const double qv = ((k == 0) ? zm : (k == 1 ? zetot : zvol - zvol0)) /
+                      ((k == 0) ? zvol : (k == 1 ? zm + 1.e-99 : zvol0));
+    const double zdvov = (zok && k == 2) ? fabs(qv) : 1.e-99;
+    __syncwarp();
+    if (zok) {
+        if (k == 0) { a.zvol[z] = zvol; a.zr[z] = qv; }
+        else if (k == 1) { a.zetot[z] = zetot; a.ze[z] = qv; }
+        else if (k == 2) a.zwrate[z] = zwrate;
+    }
+    const int nbad = __syncthreads_count(bad);
+    if (blockIdx.x >= (unsigned)a.npartC) return;   // partials are sized for this grid
+    block_fold<false, kZoneThreadsC>(zdvov, a.part_dvov + blockIdx.x);
+    if (threadIdx.x == 0) a.part_badC[blockIdx.x] = nbad;
+}
+
+}  // namespace
+
+cudaError_t launch_cycle_mixed(const DevArrays& a, const HydroConst& c, cudaStream_t stream, cudaEvent_t* ev) {
+    const int zb = (int)zone_blocks(a.numz);
+    const int zbc = (int)zone_blocks(a.numz, kZoneThreadsC);
+    const int pb = (int)((a.nump + kPointThreads - 1) / kPointThreads);
+    if (ev) cudaEventRecord(ev[0], stream);
+    if (a.quads) pass_a_mixed<true><<<zb, kZoneThreads, 0, stream>>>(a, c);
+    else pass_a_mixed<false><<<zb, kZoneThreads, 0, stream>>>(a, c);
+    if (ev) cudaEventRecord(ev[1], stream);
+    pass_b_mixed<<<pb, kPointThreads, 0, stream>>>(a, c);
+    if (ev) cudaEventRecord(ev[2], stream);
+    if (a.quads) pass_c_mixed<true><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
+    else pass_c_mixed<false><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
+    if (ev) cudaEventRecord(ev[3], stream);
+    launch_finalize(a, c, zb, zbc, stream);
+    if (ev) cudaEventRecord(ev[4], stream);
+    return cudaGetLastError();
+}
+
+}  // namespace pnt
