@@ -11,12 +11,16 @@
 //         the dt reduction;
 //   FP32  edge lengths, surface vectors, characteristic lengths, the TTS
 //         side force and every QCS corner quantity, formed in coordinates
-//         relative to the zone's first point so that FP32 keeps its
-//         precision on small zones far from the origin.
+//         and velocities relative to the zone's first point so that FP32
+//         keeps its precision on small zones far from the origin.  Zones
+//         with a corner sharper than ~30 degrees (the centre of a pie mesh)
+//         form their QCS side force in FP64: there it is a small difference
+//         of terms weighted by 1/sin^2 of the corner angle.
 //
-// Side results handed to the point and corrector passes are stored in FP32
-// (corner mass 4 B, corner force 8 B, sfp + sfq 8 B per side instead of
-// 40 B).  Compiled with fast math; the accuracy of this path is stated as
+// The pressure force sfp is formed in FP64 (its surface vectors cancel
+// around each zone, and calcWork needs that cancellation), and sfp + sfq is
+// handed to calcWork in FP64; the corner mass and corner force handed to the
+// point pass are stored in FP32 (4 + 8 B per side instead of 24 B).  Compiled with fast math; the accuracy of this path is stated as
 // its L1 error against the FP64 run (tests/test_gpu_mixed.py).
 #include "hydro_dev.h"
 
@@ -89,6 +93,54 @@ __device__ __forceinline__ void block_fold(double v, double* out) {
         for (int i = 1; i < kThreads / 32; ++i) r = kMin ? dmin(r, red[i]) : ((red[i] > r) ? red[i] : r);
         *out = r;
     }
+}
+
+// QCS side force of one zone in FP64 (QCS.cc:116-380), for zones with an
+// acute corner: there sfq is a small difference of large terms (cw grows as
+// 1/sin^2 of the corner angle) that FP32 cannot carry.  All lanes of the
+// warp must call it (it shuffles).
+__device__ double2 qcs_sfq_fp64(double2 xp, double2 xp2, double2 zxp, double2 u0, double rn, int g, int n,
+                                int lp, int ln, double zss, double zrp, const HydroConst& c) {
+    const double2 u02 = shfl2(u0, ln), upp = shfl2(u0, lp);
+    const double2 zuc = mk(zsum4(u0.x * rn, g, n), zsum4(u0.y * rn, g, n));
+    const double2 ex = smul(0.5, add(xp, xp2));
+    const double2 xq3 = shfl2(ex, lp);
+    const double2 d = sub(xp2, xp);
+    const double elen = sqrt(dot(d, d));
+    const double de1 = shfl(elen, lp), de2 = elen;
+    const double2 up0 = u0, xq0 = xp, xq1 = ex, up2 = zuc, xq2 = zxp;
+    const double2 up1 = smul(0.5, add(up0, u02));
+    const double2 up3 = smul(0.5, add(upp, up0));
+    const double cvolume = 0.5 * cross(sub(xq2, xq0), sub(xq3, xq1));
+    const double2 v1 = sub(xq3, xq0), v2 = sub(xq1, xq0);
+    const double minelen = dmin(de1, de2);
+    double ccos = (minelen < 1.e-12) ? 0. : 4. * dot(v1, v2) / (de1 * de2);
+    const double cdiv = (cross(sub(up2, up0), sub(xq3, xq1)) - cross(sub(up3, up1), sub(xq2, xq0))) /
+                        (2.0 * cvolume);
+    double crmu = 0.;
+    if (cdiv < 0.0) {
+        const double2 dxx1 = smul(0.5, sub(sub(add(xq1, xq2), xq0), xq3));
+        const double2 dxx2 = smul(0.5, sub(sub(add(xq2, xq3), xq0), xq1));
+        const double dx1 = sqrt(dot(dxx1, dxx1)), dx2 = sqrt(dot(dxx2, dxx2));
+        const double2 duav = smul(0.25, add(add(add(up0, up1), up2), up3));
+        const double test1 = fabs(dot(dxx1, duav) * dx2);
+        const double test2 = fabs(dot(dxx2, duav) * dx1);
+        const double rr = (test1 > test2) ? dx1 / dx2 : dx2 / dx1;
+        const double evol = dmin(sqrt(4.0 * cvolume * rr), 2.0 * minelen);
+        const double2 w1 = sub(sub(add(up1, up2), up0), up3), w2 = sub(sub(add(up2, up3), up0), up1);
+        const double du = sqrt(dmax(dot(w1, w1), dot(w2, w2)));
+        const double ztmp2 = c.q2 * 0.25 * c.gammap1 * du;
+        const double ztmp1 = c.q1 * zss;
+        crmu = (ztmp2 + sqrt(ztmp2 * ztmp2 + ztmp1 * ztmp1)) * zrp * evol;
+    }
+    const double2 cqe1 = smul(crmu / de1, sub(up0, upp));
+    const double2 cqe2 = smul(crmu / de2, sub(u02, up0));
+    const double csin2 = 1.0 - ccos * ccos;
+    const double cw = (csin2 < 1.e-4) ? 0. : cvolume / csin2;
+    ccos = (csin2 < 1.e-4) ? 0. : ccos;
+    const double cw2 = shfl(cw, ln), ccos2 = shfl(ccos, ln);
+    const double2 cqe12 = shfl2(cqe1, ln), cqe22 = shfl2(cqe2, ln);
+    return smul(1. / elen, add(smul(cw, add(cqe2, smul(ccos, cqe1))), smul(cw2, add(cqe12, smul(ccos2, cqe22)))));
 }
 
 // ---------------------------------------------------------------------
@@ -169,7 +221,10 @@ __global__ void __launch_bounds__(kZoneThreads, 3) pass_a_mixed(DevArrays a, Hyd
     const float2 r = f2(sub(xp, xref));
     const float2 r2 = shflf2(r, ln);
     const float2 zc = f2(sub(zxp, xref));
-    const float2 uf = f2(u0);
+    // velocities relative to the zone's first point as well: QCS works on
+    // velocity differences, which absolute FP32 values would round away
+    const double2 uref = shfl2(u0, g);
+    const float2 uf = f2(sub(u0, uref));
     const float2 u2f = shflf2(uf, ln);
     const float2 upf = shflf2(uf, lp);
     const float rnf = (float)rn;
@@ -186,8 +241,13 @@ __global__ void __launch_bounds__(kZoneThreads, 3) pass_a_mixed(DevArrays a, Hyd
     zdl = fminf(zdl, __shfl_xor_sync(kFull, zdl, 2));
     const float rinv_el = 1.f / elen;
 
-    const float zssf = (float)zss, zrpf = (float)zrp, zpf = (float)zp;
-    const float2 sfp = fmul(-zpf, ssurf);
+    const float zssf = (float)zss, zrpf = (float)zrp;
+    // PolyGas::calcForce in FP64: the pressure forces of a zone cancel
+    // around its closed boundary, and calcWork takes the small residual of
+    // their work on moving points; FP32 surface vectors break that
+    // cancellation
+    const double2 ex64 = smul(0.5, add(xp, xp2));
+    const double2 sfp = smul(-zp, mk(-(ex64.y - zxp.y), ex64.x - zxp.x));
     // TTS (TTS.cc:55-104)
     const float srho = zrpf * (float)mf * ((float)zareap / saf);
     float sstmp = fmaxf(zssf, (float)c.tts_ssmin);
@@ -214,7 +274,7 @@ __global__ void __launch_bounds__(kZoneThreads, 3) pass_a_mixed(DevArrays a, Hyd
         const float2 dxx1 = fmul(0.5f, fsub(fsub(fadd(xq1, xq2), xq0), xq3));
         const float2 dxx2 = fmul(0.5f, fsub(fsub(fadd(xq2, xq3), xq0), xq1));
         const float dx1 = flen(dxx1), dx2 = flen(dxx2);
-        const float2 duav = fmul(0.25f, fadd(fadd(fadd(up0, up1), up2), up3));
+        const float2 duav = fadd(fmul(0.25f, fadd(fadd(fadd(up0, up1), up2), up3)), f2(uref));
         const float test1 = fabsf(fdot(dxx1, duav) * dx2);
         const float test2 = fabsf(fdot(dxx2, duav) * dx1);
         const float rr = (test1 > test2) ? dx1 / dx2 : dx2 / dx1;
@@ -227,13 +287,28 @@ __global__ void __launch_bounds__(kZoneThreads, 3) pass_a_mixed(DevArrays a, Hyd
     }
     const float2 cqe1 = fmul(crmu * rinv_de1, fsub(up0, upf));
     const float2 cqe2 = fmul(crmu * rinv_el, fsub(u2f, up0));
-    const float csin2 = 1.f - ccos * ccos;
+    // sin^2 of the corner angle.  The reference forms 1 - ccos^2, which in
+    // FP32 loses the small sines of the acute corners of thin zones (3-degree
+    // corners at the centre of a pie mesh); v1 and v2 run to the edge
+    // midpoints, |v_i| = de_i / 2, so (4 cross / (de1 de2))^2 is the same
+    // quantity without the cancellation.
+    const float ssin = 4.f * fcross(v1, v2) / (de1 * de2);
+    const float csin2 = (minelen < 1.e-12f) ? 1.f : ssin * ssin;
     const float cw = (csin2 < 1.e-4f) ? 0.f : cvolume / csin2;
     ccos = (csin2 < 1.e-4f) ? 0.f : ccos;
     const float cw2 = shflf(cw, ln), ccos2 = shflf(ccos, ln);
     const float2 cqe12 = shflf2(cqe1, ln), cqe22 = shflf2(cqe2, ln);
-    const float2 sfq = fmul(rinv_el, fadd(fmul(cw, fadd(cqe2, fmul(ccos, cqe1))),
-                                          fmul(cw2, fadd(cqe12, fmul(ccos2, cqe22)))));
+    float2 sfq = fmul(rinv_el, fadd(fmul(cw, fadd(cqe2, fmul(ccos, cqe1))),
+                                    fmul(cw2, fadd(cqe12, fmul(ccos2, cqe22)))));
+    // zones with a corner under ~30 degrees take the FP64 form (warp-uniform
+    // branch; never taken on rectangular meshes)
+    int acute = (act && csin2 < 0.25f) ? 1 : 0;
+    acute |= __shfl_xor_sync(kFull, acute, 1);
+    acute |= __shfl_xor_sync(kFull, acute, 2);
+    if (__any_sync(kFull, acute)) {
+        const double2 q = qcs_sfq_fp64(xp, xp2, zxp, u0, rn, g, n, lp, ln, zss, zrp, c);
+        if (acute) sfq = f2(q);
+    }
 
     // QCS::setVelDiff, calcDtNew (FP64 reduction)
     float dux = fabsf(fdot(fsub(u2f, uf), fsub(r2, r))) * rinv_el;
@@ -244,12 +319,12 @@ __global__ void __launch_bounds__(kZoneThreads, 3) pass_a_mixed(DevArrays a, Hyd
     const double cdu = dmax(zdu, dmax(zss, 1.e-99));
     const double zdthyd = zok ? (double)zdl * c.cfl / cdu : 1.e99;
 
-    const float2 sfpq = fadd(sfp, sfq);
-    const float2 ftot = fadd(sfpq, sft);
-    const float2 ftot3 = shflf2(ftot, lp);
+    const double2 sfpq = add(sfp, mk((double)sfq.x, (double)sfq.y));
+    const double2 ftot = add(sfpq, mk((double)sft.x, (double)sft.y));
+    const double2 ftot3 = shfl2(ftot, lp);
     if (act) {
-        a.cforce_f[s] = fsub(ftot, ftot3);
-        a.sftot_f[s] = sfpq;
+        a.cforce_f[s] = f2(sub(ftot, ftot3));
+        a.sftot[s] = sfpq;
     }
 
     const int nbad = __syncthreads_count(bad);
@@ -326,8 +401,7 @@ __global__ void __launch_bounds__(kZoneThreadsC) pass_c_mixed(DevArrays a, Hydro
     const double2 x = act ? a.px[cur ^ 1][p1] : mk(0., 0.);
     const double2 u = act ? a.pu[cur ^ 1][p1] : mk(0., 0.);
     const unsigned mask = act ? a.bcmask[p1] : 0u;
-    const float2 sff = act ? a.sftot_f[s] : fk(0.f, 0.f);
-    const double2 sft = mk((double)sff.x, (double)sff.y);
+    const double2 sft = act ? a.sftot[s] : mk(0., 0.);
     const double zm = zok ? a.zm[z] : 1.;
     const double zetot0 = zok ? a.zetot[z] : 0.;
     const double zvol0 = zok ? a.zvol[z] : 1.;
