@@ -221,6 +221,36 @@ pnt_status pnt_hydro_device_ptr(pnt_hydro* hydro, int32_t field, void** dptr);
 pnt_status pnt_hydro_stream(pnt_hydro* hydro, void** cuda_stream);
 
 /* ------------------------------------------------------------------ */
+/* Batches of independent meshes on one GPU (project extension: the       */
+/* reference advances one mesh per Driver).  Every instance runs the FP64 */
+/* cycle bit-identically to its own pnt_hydro; the batch advances all     */
+/* running instances by one of their own cycles per batch cycle.          */
+/* ------------------------------------------------------------------ */
+typedef struct pnt_batch pnt_batch;
+
+/* n meshes with their own parameters (params[i], precision FP64); the
+ * meshes are copied.  Each instance starts as pnt_hydro_create would. */
+pnt_status pnt_batch_create(const pnt_mesh* const* meshes, const pnt_params* params, int32_t n,
+                            int32_t device, pnt_batch** out);
+void pnt_batch_destroy(pnt_batch* batch);
+/* Work-list shape: zones per tile (multiple of 64) and CTAs per SM of the
+ * persistent zone passes.  Results do not depend on it. */
+pnt_status pnt_batch_set_shape(pnt_batch* batch, int32_t zones_per_tile, int32_t ctas_per_sm);
+pnt_status pnt_batch_get_shape(pnt_batch* batch, int32_t* zones_per_tile, int32_t* ctas_per_sm);
+/* Autotuner: times each candidate shape on `trial_cycles` cycles of this
+ * run (the cycles count: the run advances) and keeps the fastest. */
+pnt_status pnt_batch_tune(pnt_batch* batch, int32_t trial_cycles, int32_t* zones_per_tile,
+                          int32_t* ctas_per_sm, double* ms_per_cycle);
+/* Runs batch cycles until every instance is done or max_cycles (<= 0: no
+ * limit) have been enqueued; *running_left = instances still running. */
+pnt_status pnt_batch_run(pnt_batch* batch, int32_t max_cycles, int32_t* running_left);
+pnt_status pnt_batch_enqueue(pnt_batch* batch, int32_t ncycles);
+pnt_status pnt_batch_time_cycles(pnt_batch* batch, int32_t ncycles, double* elapsed_ms);
+pnt_status pnt_batch_scalars(pnt_batch* batch, int32_t instance, pnt_scalars* out);
+pnt_status pnt_batch_download(pnt_batch* batch, int32_t instance, int32_t field, void* host_dst,
+                              size_t bytes);
+
+/* ------------------------------------------------------------------ */
 /* Per-task operators on caller-owned device arrays                     */
 /* ------------------------------------------------------------------ */
 

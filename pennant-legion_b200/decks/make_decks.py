@@ -54,6 +54,28 @@ def leblanc(nx: int = 2880, ny: int = 288, tstop: float = 6.0, extra: str = "") 
             f"dtreport 100\n{extra}")
 
 
+def sedov_batch(count: int = 256, seed: int = 20240601, nmin: int = 32, nmax: int = 512,
+                tstop: float = 0.5) -> list[dict]:
+    """The batched workload: `count` Sedov instances, side length N drawn
+    log-uniform in [nmin, nmax], deposited energy E0 uniform in [0.1, 1.0],
+    gamma uniform in [1.4, 5/3], each run to `tstop`; numpy's PCG64 seeded
+    with `seed`.  dtinit = min(1e-4, 1e-4 (48/N)^2.5 sqrt(0.25/E0)): the 48^2
+    deck's 1e-4 rescaled by the first step's CFL limit h/c, c ~ sqrt(E0/h^3),
+    so that no instance inverts a zone on its first step.  Returns dicts with
+    keys n, e0, gamma, text."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(nmin), math.log(nmax)))))
+        e0 = float(rng.uniform(0.1, 1.0))
+        gamma = float(rng.uniform(1.4, 5.0 / 3.0))
+        dtinit = min(1e-4, 1e-4 * (48.0 / n) ** 2.5 * math.sqrt(0.25 / e0))
+        out.append({"n": n, "e0": e0, "gamma": gamma,
+                    "text": sedov(n, e0=e0, tstop=tstop, dtinit=dtinit, gamma=gamma)})
+    return out
+
+
 DECKS = {
     "sedov48.pnt": sedov(48),      # CPU-runnable case, FP64, t = 1.0
     "sedov480.pnt": sedov(480),    # FP64 drop-in parity case, t = 1.0

@@ -126,6 +126,16 @@ def _load():
         "pnt_hydro_upload": (i32, [vp, i32, vp, sz]),
         "pnt_hydro_device_ptr": (i32, [vp, i32, pp]),
         "pnt_hydro_stream": (i32, [vp, pp]),
+        "pnt_batch_create": (i32, [C.POINTER(vp), C.POINTER(Params), i32, i32, pp]),
+        "pnt_batch_destroy": (None, [vp]),
+        "pnt_batch_set_shape": (i32, [vp, i32, i32]),
+        "pnt_batch_get_shape": (i32, [vp, C.POINTER(i32), C.POINTER(i32)]),
+        "pnt_batch_tune": (i32, [vp, i32, C.POINTER(i32), C.POINTER(i32), C.POINTER(dbl)]),
+        "pnt_batch_run": (i32, [vp, i32, C.POINTER(i32)]),
+        "pnt_batch_enqueue": (i32, [vp, i32]),
+        "pnt_batch_time_cycles": (i32, [vp, i32, C.POINTER(dbl)]),
+        "pnt_batch_scalars": (i32, [vp, i32, C.POINTER(Scalars)]),
+        "pnt_batch_download": (i32, [vp, i32, i32, vp, sz]),
         "pnt_op_calc_dt": (i32, [vp, vp, vp, vp, vp, C.c_int64, dbl, dbl, dbl, vp, vp]),
         "pnt_op_calc_dt_noalloc": (i32, [vp, vp, vp, vp, vp, C.c_int64, dbl, dbl, dbl, vp, vp]),
         "pnt_hydro_write_xy": (i32, [vp, C.c_char_p]),
@@ -326,6 +336,62 @@ class Hydro:
 
     def write_gold(self, base: str) -> None:
         check(lib.pnt_hydro_write_gold(self.h, _b(base)))
+
+
+class Batch:
+    """Many independent meshes advanced together on one GPU (FP64 cycle)."""
+
+    def __init__(self, meshes, params, device: int = 0):
+        n = len(meshes)
+        harr = (C.c_void_p * n)(*[m.h.value for m in meshes])
+        parr = (Params * n)(*params)
+        h = C.c_void_p()
+        check(lib.pnt_batch_create(harr, parr, n, device, C.byref(h)))
+        self.h = h
+        self.meshes = list(meshes)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.pnt_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_shape(self, zones_per_tile: int, ctas_per_sm: int) -> None:
+        check(lib.pnt_batch_set_shape(self.h, zones_per_tile, ctas_per_sm))
+
+    def shape(self):
+        a, b = C.c_int32(), C.c_int32()
+        check(lib.pnt_batch_get_shape(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def tune(self, trial_cycles: int = 4):
+        a, b, ms = C.c_int32(), C.c_int32(), C.c_double()
+        check(lib.pnt_batch_tune(self.h, trial_cycles, C.byref(a), C.byref(b), C.byref(ms)))
+        return a.value, b.value, ms.value
+
+    def run(self, max_cycles: int = 0) -> int:
+        left = C.c_int32()
+        check(lib.pnt_batch_run(self.h, max_cycles, C.byref(left)))
+        return left.value
+
+    def time_cycles(self, n: int) -> float:
+        ms = C.c_double()
+        check(lib.pnt_batch_time_cycles(self.h, n, C.byref(ms)))
+        return ms.value
+
+    def scalars(self, i: int) -> dict:
+        s = Scalars()
+        check(lib.pnt_batch_scalars(self.h, i, C.byref(s)))
+        return s.as_dict()
+
+    def download(self, i: int, name: str) -> np.ndarray:
+        m = self.meshes[i]
+        shape = (m.nump, 2) if name in _POINT2 else (m.numz,)
+        out = np.empty(shape, dtype=np.float64)
+        check(lib.pnt_batch_download(self.h, i, FIELDS[name], out.ctypes.data, out.nbytes))
+        return out
 
 
 def op_calc_dt(zdl: int, zdu: int, zss: int, zvol: int, zvol0: int, numz: int, cfl: float,
