@@ -112,7 +112,7 @@ void pnt_mesh_destroy(pnt_mesh* mesh);
 /* ------------------------------------------------------------------ */
 #define PNT_MAX_BC 16
 
-enum { PNT_PREC_FP64 = 0, PNT_PREC_MIXED = 1 };
+enum { PNT_PREC_FP64 = 0, PNT_PREC_MIXED = 1, PNT_PREC_LEARNED = 2 };
 
 typedef struct {
     /* Driver */
@@ -139,7 +139,8 @@ typedef struct {
 
 pnt_status pnt_params_default(pnt_params* out);
 /* Reads every key above from the deck (missing keys keep defaults);
- * "precision fp64|mixed" and "graphcycles N" are the project-only keys. */
+ * "precision fp64|mixed|learned" and "graphcycles N" are the project-only
+ * keys. */
 pnt_status pnt_params_from_deck(const pnt_deck* deck, pnt_params* out);
 
 /* ------------------------------------------------------------------ */
@@ -279,6 +280,78 @@ pnt_status pnt_op_calc_dt_noalloc(const double* zdl, const double* zdu, const do
                                   const double* zvol, const double* zvol0, int64_t numz,
                                   double cfl, double cflv, double dtlast, double* out,
                                   void* stream);
+
+/* ------------------------------------------------------------------ */
+/* Learned QCS closure (no counterpart in the reference): a 14-64-64-4   */
+/* network that stands in for the corner forces of QCS::calcForce        */
+/* (QCS.cc:246-327) on compressing corners in the precision-learned      */
+/* cycle (the mixed cycle otherwise).  Corners past the compression      */
+/* threshold, out of the training distribution, or in zones with an      */
+/* acute corner keep the plain QCS; corners in the dead zone (velocity   */
+/* jump <= dead * sound speed) get no viscous force.                     */
+/* ------------------------------------------------------------------ */
+typedef struct pnt_closure pnt_closure;
+
+#define PNT_CLOSURE_PARAMS 5380  /* W1[64][14] b1[64] W2[64][64] b2[64] W3[4][64] b3[4] */
+#define PNT_CLOSURE_NORM 36      /* input mean[14], std[14], output mean[4], std[4] */
+/* corner classes counted by the learned cycle */
+enum {
+    PNT_CLOSURE_ZERO = 0,     /* no compression: no force, as in QCS */
+    PNT_CLOSURE_DEAD = 1,     /* dead zone: no force */
+    PNT_CLOSURE_MLP = 2,      /* the network */
+    PNT_CLOSURE_FALLBACK = 3, /* compression past rho_max: plain QCS */
+    PNT_CLOSURE_OOD = 4,      /* out of distribution: plain QCS */
+    PNT_CLOSURE_ACUTE = 5,    /* zone with an acute corner: plain FP64 QCS */
+    PNT_CLOSURE_ERROR = 6,    /* blocks whose tensor-core wait ran out */
+    PNT_CLOSURE_ZONES = 7,    /* zones evaluated by the closure pass */
+    PNT_CLOSURE_NCLASS = 8
+};
+
+/* Random (Glorot-uniform, seeded) network with identity normalisation. */
+pnt_status pnt_closure_create(int32_t device, uint64_t seed, pnt_closure** out);
+pnt_status pnt_closure_load(const char* path, int32_t device, pnt_closure** out);
+pnt_status pnt_closure_save(const pnt_closure* closure, const char* path);
+void pnt_closure_destroy(pnt_closure* closure);
+/* Host copies of the parameters (PNT_CLOSURE_PARAMS floats), the
+ * normalisation (PNT_CLOSURE_NORM) and the thresholds {dead, rho_max,
+ * ood_kappa}; any pointer may be NULL.  Setting parameters resets Adam. */
+pnt_status pnt_closure_get(const pnt_closure* closure, float* params, float* norm, float* thresholds);
+pnt_status pnt_closure_set(pnt_closure* closure, const float* params, const float* norm,
+                           const float* thresholds);
+/* Training data from the FP64 state at the start of the next cycle of
+ * `hydro` (which must be FP64): every eligible corner, kept with
+ * probability `keep` by a hash of (seed, cycle, side), appended at *count
+ * (in/out) to device arrays feats [capacity][14], targets [capacity][4]
+ * (QCS corner forces in the closure's frame and scale) and sides
+ * [capacity].  Deterministic order. */
+pnt_status pnt_hydro_harvest(pnt_hydro* hydro, double dead, double keep, uint64_t seed, float* feats,
+                             float* targets, int32_t* sides, int64_t capacity, int64_t* count);
+/* Mean and standard deviation of n harvested samples (device arrays). */
+pnt_status pnt_closure_fit_normalization(pnt_closure* closure, const float* feats,
+                                         const float* targets, int64_t n);
+/* Normalised BF16 inputs x [n][16] and FP32 targets t [n][4] (device). */
+pnt_status pnt_closure_prepare(const pnt_closure* closure, const float* feats, const float* targets,
+                               int64_t n, void* x, float* t);
+/* `steps` Adam steps (BF16 tensor-core forward and backward, FP32
+ * accumulation) of mean squared error; step s uses rows (first +
+ * s*rows_per_step + i) mod n, i < rows_per_step.  losses[s] (host, may be
+ * NULL) receives each step's loss. */
+pnt_status pnt_closure_train(pnt_closure* closure, const void* x, const float* t, int64_t n,
+                             int64_t first, int32_t steps, int32_t rows_per_step, float lr,
+                             float* losses);
+/* Loss gradient over all n rows (host grad[PNT_CLOSURE_PARAMS]). */
+pnt_status pnt_closure_gradient(pnt_closure* closure, const void* x, const float* t, int64_t n,
+                                float* grad, float* loss);
+/* The network on n raw input rows (device feats [n][14] -> out [n][4]),
+ * the tcgen05 inference of the learned cycle. */
+pnt_status pnt_closure_forward(const pnt_closure* closure, const float* feats, int64_t n, float* out);
+/* Gives a precision-learned hydro object its copy of the closure.  mode 0:
+ * the network; 1: no force on the network's corners (ablation); 2: plain
+ * QCS on them (isolates the classification). */
+pnt_status pnt_hydro_set_closure(pnt_hydro* hydro, const pnt_closure* closure, int32_t mode);
+/* Corner counts per class (PNT_CLOSURE_NCLASS entries) summed over the
+ * cycles run since the last reset. */
+pnt_status pnt_hydro_closure_counts(pnt_hydro* hydro, uint64_t* counts, int32_t reset);
 
 /* Output writers: WriteXY::write (WriteXY.cc:28-52) and ExportGold::write
  * (ExportGold.cc:31-307) of the current state. */

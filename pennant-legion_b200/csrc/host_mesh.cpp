@@ -519,7 +519,8 @@ pnt_status pnt_params_from_deck(const pnt_deck* deck, pnt_params* p) {
     const std::string prec = get_string(d, "precision", "fp64");
     if (prec == "fp64") p->precision = PNT_PREC_FP64;
     else if (prec == "mixed") p->precision = PNT_PREC_MIXED;
-    else return fail(PNT_ERR_DECK, "precision must be fp64 or mixed");
+    else if (prec == "learned") p->precision = PNT_PREC_LEARNED;
+    else return fail(PNT_ERR_DECK, "precision must be fp64, mixed or learned");
     p->graph_cycles = get_int(d, "graphcycles", 0);
     return PNT_OK;
 }

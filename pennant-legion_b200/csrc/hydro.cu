@@ -1,6 +1,7 @@
 // hydro.cu -- the pnt_hydro object: device state of one mesh on one GPU,
 // Hydro::init, the cycle driver with CUDA-graph replay, field transfer and
 // the output writers.  C ABI in include/pennant_b200.h.
+#include "closure_dev.cuh"
 #include "hydro_dev.h"
 #include "pnt_internal.h"
 
@@ -57,6 +58,9 @@ struct pnt_hydro {
     int graph_cycles = 0;
     // the cycle of the selected precision
     cudaError_t (*launch)(const DevArrays&, const HydroConst&, cudaStream_t, cudaEvent_t*) = launch_cycle_fp64;
+    // learned closure: this object's copy of the parameter image (set by
+    // pnt_hydro_set_closure) and the corner class counters
+    bool learned = false;
 
     ~pnt_hydro() {
         DeviceGuard dg(device);
@@ -80,7 +84,14 @@ struct pnt_hydro {
         return PNT_OK;
     }
 
+    pnt_status check_ready() const {
+        if (learned && !a.closure_img)
+            return fail(PNT_ERR_STATE, "precision learned needs a closure (pnt_hydro_set_closure)");
+        return PNT_OK;
+    }
+
     pnt_status launch_cycles(int n) {
+        if (pnt_status st = check_ready()) return st;
         for (int i = 0; i < n; ++i) {
             const cudaError_t e = launch(a, hc, stream, nullptr);
             if (e != cudaSuccess) return fail(PNT_ERR_CUDA, "cycle launch: %s", cudaGetErrorString(e));
@@ -90,6 +101,7 @@ struct pnt_hydro {
 
     pnt_status ensure_graph() {
         if (graph) return PNT_OK;
+        if (pnt_status st = check_ready()) return st;
         graph_cycles = params.graph_cycles > 0 ? params.graph_cycles : 16;
         cudaGraph_t g = nullptr;
         CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
@@ -329,7 +341,8 @@ extern "C" {
 pnt_status pnt_hydro_create(const pnt_mesh* mesh, const pnt_params* params, int32_t device, pnt_hydro** out) {
     if (!mesh || !params || !out) return fail(PNT_ERR_INVALID_ARG, "null argument");
     *out = nullptr;
-    if (params->precision != PNT_PREC_FP64 && params->precision != PNT_PREC_MIXED)
+    if (params->precision != PNT_PREC_FP64 && params->precision != PNT_PREC_MIXED &&
+        params->precision != PNT_PREC_LEARNED)
         return fail(PNT_ERR_INVALID_ARG, "unknown precision %d", params->precision);
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
@@ -342,7 +355,10 @@ pnt_status pnt_hydro_create(const pnt_mesh* mesh, const pnt_params* params, int3
     if (!h) return fail(PNT_ERR_NOMEM, "out of memory");
     h->device = device;
     h->params = *params;
-    h->launch = (params->precision == PNT_PREC_MIXED) ? launch_cycle_mixed : launch_cycle_fp64;
+    h->launch = (params->precision == PNT_PREC_MIXED)     ? launch_cycle_mixed
+                : (params->precision == PNT_PREC_LEARNED) ? launch_cycle_learned
+                                                          : launch_cycle_fp64;
+    h->learned = params->precision == PNT_PREC_LEARNED;
     pnt_status st = PNT_OK;
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMallocHost((void**)&h->ctl_host, sizeof(Ctl));
@@ -358,6 +374,13 @@ pnt_status pnt_hydro_create(const pnt_mesh* mesh, const pnt_params* params, int3
         h->znump = m.znump;
         h->mapsp1 = m.mapsp1;
         st = init_hydro(h, m, *params);
+        if (!st && h->learned) {
+            unsigned long long* counts = nullptr;
+            st = h->alloc(&counts, kClassCount * 64);
+            if (!st && cudaMemset(counts, 0, kClassCount * 64 * sizeof(unsigned long long)) != cudaSuccess)
+                st = fail(PNT_ERR_CUDA, "counter memset failed");
+            h->a.closure_counts = counts;
+        }
     } catch (const std::bad_alloc&) {
         st = fail(PNT_ERR_NOMEM, "out of host memory");
     }
@@ -630,4 +653,70 @@ pnt_status pnt_hydro_write_gold(pnt_hydro* h, const char* base) {
     return PNT_OK;
 }
 
+pnt_status pnt_hydro_set_closure(pnt_hydro* h, const pnt_closure* c, int32_t mode) {
+    if (!h || !c || mode < 0 || mode > 2) return fail(PNT_ERR_INVALID_ARG, "bad argument");
+    if (!h->learned) return fail(PNT_ERR_STATE, "the hydro object was not created with precision learned");
+    if (pnt::closure_device(c) != h->device) return fail(PNT_ERR_INVALID_ARG, "closure lives on another device");
+    DeviceGuard dg(h->device);
+    if (!h->a.closure_img) {
+        uint8_t* img = nullptr;
+        float* rec = nullptr;
+        int2* hdr = nullptr;
+        int32_t* nrec = nullptr;
+        if (pnt_status st = h->alloc(&img, kImgBytes)) return st;
+        if (pnt_status st = h->alloc(&rec, (size_t)h->numz * 4 * kRecFloats)) return st;
+        if (pnt_status st = h->alloc(&hdr, (size_t)h->numz)) return st;
+        if (pnt_status st = h->alloc(&nrec, 1)) return st;
+        CUDA_TRY(cudaMemset(nrec, 0, sizeof(int32_t)));
+        CUDA_TRY(prepare_learned_kernels());
+        int nsm = 148;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+        h->a.closure_img = img;
+        h->a.closure_rec = rec;
+        h->a.closure_zhdr = hdr;
+        h->a.closure_nrec = nrec;
+        h->a.closure_grid = 2 * nsm;
+    }
+    // the image lives in this object: a copy of the closure's, with the mode
+    uint8_t* img = const_cast<uint8_t*>(h->a.closure_img);
+    const float fmode = (float)mode;
+    CUDA_TRY(cudaMemcpyAsync(img, pnt::closure_image(c), kImgBytes, cudaMemcpyDeviceToDevice, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(img + kImgThr + 12, &fmode, sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (h->graph) {   // the captured cycles hold the old DevArrays
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+    }
+    return PNT_OK;
+}
+
+pnt_status pnt_hydro_closure_counts(pnt_hydro* h, uint64_t* counts, int32_t reset) {
+    if (!h || !counts) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    if (!h->learned) return fail(PNT_ERR_STATE, "the hydro object was not created with precision learned");
+    DeviceGuard dg(h->device);
+    std::vector<unsigned long long> raw(kClassCount * 64);
+    CUDA_TRY(cudaMemcpyAsync(raw.data(), h->a.closure_counts, raw.size() * sizeof(unsigned long long),
+                             cudaMemcpyDeviceToHost, h->stream));
+    if (reset)
+        CUDA_TRY(cudaMemsetAsync(h->a.closure_counts, 0, raw.size() * sizeof(unsigned long long), h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (int q = 0; q < PNT_CLOSURE_NCLASS; ++q) {
+        uint64_t t = 0;
+        for (int b = 0; b < 64; ++b) t += raw[q * 64 + b];
+        counts[q] = t;
+    }
+    return PNT_OK;
+}
+
 }  // extern "C"
+
+namespace pnt {
+bool hydro_access(pnt_hydro* h, HydroAccess* out) {
+    if (!h || !out) return false;
+    out->a = h->a;
+    out->c = h->hc;
+    out->stream = h->stream;
+    out->device = h->device;
+    return true;
+}
+}  // namespace pnt

@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+struct pnt_hydro;
+
 namespace pnt {
 
 constexpr int kMaxBC = 16;
@@ -75,6 +77,16 @@ struct DevArrays {
     double* part_dvov;
     int32_t* part_badC;
     Ctl* ctl;
+    // learned closure (precision = learned): parameter image and the corner
+    // class counters [class][64] (closure_dev.cuh)
+    const uint8_t* closure_img;
+    unsigned long long* closure_counts;
+    // zones whose corners the closure pass evaluates: records [numz][4][24],
+    // headers (first side, sides) [numz], and this cycle's count
+    float* closure_rec;
+    int2* closure_zhdr;
+    int32_t* closure_nrec;
+    int32_t closure_grid;   // CTAs of the persistent closure pass
 };
 
 #ifndef PNT_ZONE_THREADS_C
@@ -98,7 +110,21 @@ cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStrea
 // The mixed-precision cycle (hydro_mixed.cu).
 cudaError_t launch_cycle_mixed(const DevArrays& a, const HydroConst& c, cudaStream_t stream,
                                cudaEvent_t* ev = nullptr);
+// The learned-closure cycle: the mixed cycle with the closure in pass A.
+cudaError_t launch_cycle_learned(const DevArrays& a, const HydroConst& c, cudaStream_t stream,
+                                 cudaEvent_t* ev = nullptr);
+// Raises the learned pass A's dynamic shared-memory limit on the current device.
+cudaError_t prepare_learned_kernels();
 // The finalize step shared by both cycles (nA / nC partials of passes A / C).
 void launch_finalize(const DevArrays& a, const HydroConst& c, int nA, int nC, cudaStream_t stream);
+
+// Device state of a pnt_hydro for the closure harvest (closure.cu).
+struct HydroAccess {
+    DevArrays a;
+    HydroConst c;
+    cudaStream_t stream;
+    int device;
+};
+bool hydro_access(pnt_hydro* h, HydroAccess* out);
 
 }  // namespace pnt

@@ -22,6 +22,7 @@
 // handed to calcWork in FP64; the corner mass and corner force handed to the
 // point pass are stored in FP32 (4 + 8 B per side instead of 24 B).  Compiled with fast math; the accuracy of this path is stated as
 // its L1 error against the FP64 run (tests/test_gpu_mixed.py).
+#include "closure_dev.cuh"
 #include "hydro_dev.h"
 
 #include <cuda_runtime.h>
@@ -146,7 +147,7 @@ __device__ double2 qcs_sfq_fp64(double2 xp, double2 xp2, double2 zxp, double2 u0
 // ---------------------------------------------------------------------
 // Pass A, mixed precision
 // ---------------------------------------------------------------------
-template <bool kQuads>
+template <bool kQuads, bool kLearned>
 __global__ void __launch_bounds__(kZoneThreads, 3) pass_a_mixed(DevArrays a, HydroConst c) {
     const Ctl* ctl = a.ctl;
     if (skip_cycle(ctl)) return;
@@ -269,8 +270,91 @@ __global__ void __launch_bounds__(kZoneThreads, 3) pass_a_mixed(DevArrays a, Hyd
     float ccos = (minelen < 1.e-12f) ? 0.f : 4.f * fdot(v1, v2) / (de1 * de2);
     const float cdiv = (fcross(fsub(up2, up0), fsub(xq3, xq1)) - fcross(fsub(up3, up1), fsub(xq2, xq0))) /
                        (2.f * cvolume);
+    // sin^2 of the corner angle.  The reference forms 1 - ccos^2, which in
+    // FP32 loses the small sines of the acute corners of thin zones (3-degree
+    // corners at the centre of a pie mesh); v1 and v2 run to the edge
+    // midpoints, |v_i| = de_i / 2, so (4 cross / (de1 de2))^2 is the same
+    // quantity without the cancellation.  Zones with a corner under ~30
+    // degrees take the FP64 form (warp-uniform branch; never taken on
+    // rectangular meshes).  The learned cycle needs the flag before the
+    // corner forces, the plain one after them (fewer live registers).
+    float csin2 = 1.f;
+    int acute = 0;
+    auto corner_sin2 = [&]() {
+        const float ssin = 4.f * fcross(v1, v2) / (de1 * de2);
+        csin2 = (minelen < 1.e-12f) ? 1.f : ssin * ssin;
+        acute = (act && csin2 < 0.25f) ? 1 : 0;
+        acute |= __shfl_xor_sync(kFull, acute, 1);
+        acute |= __shfl_xor_sync(kFull, acute, 2);
+    };
+    if constexpr (kLearned) corner_sin2();
+
+    // The learned closure (closure_dev.cuh) replaces the corner forces of
+    // compressing corners outside the dead zone that are neither strongly
+    // compressed nor out of distribution; the others keep the plain QCS.
+    // Those corners get no force here: their zones are recorded and the
+    // closure pass adds the network's force to the zones' sides.
+    bool plain = cdiv < 0.f;
+    int cls = kClassZero;
+    if constexpr (kLearned) {
+        float f[kClIn];
+        float fcx = 0.f, fcy = 0.f, fscale = 0.f;
+        const float* thr = reinterpret_cast<const float*>(a.closure_img + kImgThr);
+        const float dead = __ldg(thr), rho_max = __ldg(thr + 1), kappa = __ldg(thr + 2);
+        const int mode = (int)__ldg(thr + 3);   // 0 network, 1 no force, 2 plain QCS
+        const float2 xpp = shflf2(r, lp);
+        const float2 uav = fadd(fmul(0.25f, fadd(fadd(fadd(up0, up1), up2), up3)), f2(uref));
+        if (act && acute) cls = kClassAcute;
+        else if (act && cdiv < 0.f) {
+            const bool live = closure_features<float>({r.x, r.y}, {xpp.x, xpp.y}, {r2.x, r2.y}, {zc.x, zc.y},
+                                                      {uf.x, uf.y}, {upf.x, upf.y}, {u2f.x, u2f.y}, {zuc.x, zuc.y},
+                                                      {uav.x, uav.y}, zssf, (float)(c.q2 * 0.25 * c.gammap1),
+                                                      (float)c.q1, dead, f, fcx, fcy, fscale);
+            if (!live) cls = kClassDead;
+            else if (f[11] > rho_max) cls = kClassFallback;
+            else {
+                const float* mean = reinterpret_cast<const float*>(a.closure_img + kImgFMean);
+                const float* istd = reinterpret_cast<const float*>(a.closure_img + kImgFIstd);
+                float zmax = 0.f;
+#pragma unroll
+                for (int i = 0; i < kClIn; ++i) zmax = fmaxf(zmax, fabsf((f[i] - __ldg(mean + i)) * __ldg(istd + i)));
+                cls = (zmax > kappa) ? kClassOod : kClassMlp;
+            }
+        }
+        plain = (cls == kClassFallback || cls == kClassOod || (cls == kClassMlp && mode == 2));
+        // record the zones with a corner for the network (one bit per zone:
+        // its first lane), all four corners of each
+        const bool net = cls == kClassMlp && mode == 0;
+        int zflag = net ? 1 : 0;
+        zflag |= __shfl_xor_sync(kFull, zflag, 1);
+        zflag |= __shfl_xor_sync(kFull, zflag, 2);
+        const unsigned zbits = __ballot_sync(kFull, zflag && k == 0);
+        int base = 0;
+        if (lane == 0 && zbits) base = atomicAdd(a.closure_nrec, __popc(zbits));
+        base = __shfl_sync(kFull, base, 0);
+        if (zflag) {
+            const int idx = base + __popc(zbits & ((1u << g) - 1u));
+            float4* rec = reinterpret_cast<float4*>(a.closure_rec + ((int64_t)idx * 4 + k) * kRecFloats);
+            const float nf = net ? 1.f : 0.f;
+            const float sc = net ? zrpf * fscale : 0.f;
+            float v[kRecFloats];
+#pragma unroll
+            for (int i = 0; i < kClIn; ++i) v[i] = net ? f[i] : 0.f;
+            v[kRecCx] = fcx;
+            v[kRecCy] = fcy;
+            v[kRecScale] = sc;
+            v[kRecCw] = (csin2 < 1.e-4f) ? 0.f : cvolume / csin2;
+            v[kRecCcos] = (csin2 < 1.e-4f) ? 0.f : ccos;
+            v[kRecRinv] = rinv_el;
+            v[kRecFlag] = nf;
+            v[21] = v[22] = v[23] = 0.f;
+#pragma unroll
+            for (int i = 0; i < kRecFloats / 4; ++i) rec[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+            if (k == 0) a.closure_zhdr[idx] = make_int2((int)(s - k), n);
+        }
+    }
     float crmu = 0.f;
-    if (cdiv < 0.f) {
+    if (plain) {
         const float2 dxx1 = fmul(0.5f, fsub(fsub(fadd(xq1, xq2), xq0), xq3));
         const float2 dxx2 = fmul(0.5f, fsub(fsub(fadd(xq2, xq3), xq0), xq1));
         const float dx1 = flen(dxx1), dx2 = flen(dxx2);
@@ -287,24 +371,13 @@ __global__ void __launch_bounds__(kZoneThreads, 3) pass_a_mixed(DevArrays a, Hyd
     }
     const float2 cqe1 = fmul(crmu * rinv_de1, fsub(up0, upf));
     const float2 cqe2 = fmul(crmu * rinv_el, fsub(u2f, up0));
-    // sin^2 of the corner angle.  The reference forms 1 - ccos^2, which in
-    // FP32 loses the small sines of the acute corners of thin zones (3-degree
-    // corners at the centre of a pie mesh); v1 and v2 run to the edge
-    // midpoints, |v_i| = de_i / 2, so (4 cross / (de1 de2))^2 is the same
-    // quantity without the cancellation.
-    const float ssin = 4.f * fcross(v1, v2) / (de1 * de2);
-    const float csin2 = (minelen < 1.e-12f) ? 1.f : ssin * ssin;
+    if constexpr (!kLearned) corner_sin2();
     const float cw = (csin2 < 1.e-4f) ? 0.f : cvolume / csin2;
     ccos = (csin2 < 1.e-4f) ? 0.f : ccos;
     const float cw2 = shflf(cw, ln), ccos2 = shflf(ccos, ln);
     const float2 cqe12 = shflf2(cqe1, ln), cqe22 = shflf2(cqe2, ln);
     float2 sfq = fmul(rinv_el, fadd(fmul(cw, fadd(cqe2, fmul(ccos, cqe1))),
                                     fmul(cw2, fadd(cqe12, fmul(ccos2, cqe22)))));
-    // zones with a corner under ~30 degrees take the FP64 form (warp-uniform
-    // branch; never taken on rectangular meshes)
-    int acute = (act && csin2 < 0.25f) ? 1 : 0;
-    acute |= __shfl_xor_sync(kFull, acute, 1);
-    acute |= __shfl_xor_sync(kFull, acute, 2);
     if (__any_sync(kFull, acute)) {
         const double2 q = qcs_sfq_fp64(xp, xp2, zxp, u0, rn, g, n, lp, ln, zss, zrp, c);
         if (acute) sfq = f2(q);
@@ -327,7 +400,23 @@ __global__ void __launch_bounds__(kZoneThreads, 3) pass_a_mixed(DevArrays a, Hyd
         a.sftot[s] = sfpq;
     }
 
+    __shared__ unsigned wcount[kLearned ? kZoneThreads / 32 : 1][kClassErr];
+    if constexpr (kLearned) {
+        // corner class counts per warp, summed per block below
+        for (int q = 0; q < kClassErr; ++q) {
+            const unsigned nq = __popc(__ballot_sync(kFull, act && cls == q));
+            if (lane == 0) wcount[threadIdx.x >> 5][q] = nq;
+        }
+    }
+
     const int nbad = __syncthreads_count(bad);
+    if constexpr (kLearned) {
+        if (threadIdx.x < kClassErr) {
+            unsigned t = 0;
+            for (int w = 0; w < kZoneThreads / 32; ++w) t += wcount[w][threadIdx.x];
+            if (t) atomicAdd(a.closure_counts + threadIdx.x * 64 + (blockIdx.x & 63), (unsigned long long)t);
+        }
+    }
     if (blockIdx.x >= (unsigned)a.npartA) return;   // partials are sized for this grid
     block_fold<true, kZoneThreads>(zdthyd, a.part_dtnew + blockIdx.x);
     if (threadIdx.x == 0) a.part_badA[blockIdx.x] = nbad;
@@ -338,6 +427,8 @@ __global__ void __launch_bounds__(kZoneThreads, 3) pass_a_mixed(DevArrays a, Hyd
 // ---------------------------------------------------------------------
 __global__ void __launch_bounds__(kPointThreads) pass_b_mixed(DevArrays a, HydroConst c) {
     const Ctl* ctl = a.ctl;
+    // the closure pass has consumed this cycle's zone records
+    if (a.closure_nrec && blockIdx.x == 0 && threadIdx.x == 0) *a.closure_nrec = 0;
     if (skip_cycle(ctl)) return;
     const int64_t p = (int64_t)blockIdx.x * kPointThreads + threadIdx.x;
     if (p >= a.nump) return;
@@ -369,6 +460,70 @@ __global__ void __launch_bounds__(kPointThreads) pass_b_mixed(DevArrays a, Hydro
     const double2 x = add(x0, smul(dt * 0.5, add(u0, u)));
     a.px[cur ^ 1][p] = x;
     a.pu[cur ^ 1][p] = u;
+}
+
+// ---------------------------------------------------------------------
+// Closure pass (learned cycle): the network on the corners of the zones
+// pass A recorded, 64 zones (256 corners) per tcgen05 batch, persistent.
+// A corner's QCS forces cqe1, cqe2 enter QCS::setForce (QCS.cc:331-380)
+// linearly: its side s gets d1 = cw (cqe2 + ccos cqe1) / elen[s] and the
+// previous side gets d2 = cw (cqe1 + ccos cqe2) / elen[s3].  The corner
+// force of side s, ftot[s] - ftot[s3] (Hydro.cc:1159-1193), and sfp + sfq
+// of side s then change by
+//   dcforce[s] = d1(s) - d2(s) - d1(s3) + d2(s4),  dsftot[s] = d1(s) + d2(s4),
+// which only touch the recorded zone's own sides: no two records write the
+// same side, so the update is deterministic without atomics.
+// ---------------------------------------------------------------------
+__global__ void __launch_bounds__(kMlpRows, 2) closure_pass(DevArrays a) {
+    if (skip_cycle(a.ctl)) return;
+    const int nrec = *a.closure_nrec;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && nrec)
+        atomicAdd(a.closure_counts + kClassZones * 64, (unsigned long long)nrec);
+    if ((int64_t)blockIdx.x * 64 >= nrec) return;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    MlpState st;
+    closure_mlp_setup(smem, a.closure_img, st);
+    const int k = threadIdx.x & 3, lane = threadIdx.x & 31, g = lane & ~3;
+    for (int tile = blockIdx.x; (int64_t)tile * 64 < nrec; tile += gridDim.x) {
+        const int zi = tile * 64 + (threadIdx.x >> 2);
+        const bool zok = zi < nrec;
+        float v[kRecFloats];
+        const float4* rec = reinterpret_cast<const float4*>(a.closure_rec + ((int64_t)zi * 4 + k) * kRecFloats);
+#pragma unroll
+        for (int i = 0; i < kRecFloats / 4; ++i) {
+            const float4 q = zok ? rec[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+            v[4 * i] = q.x;
+            v[4 * i + 1] = q.y;
+            v[4 * i + 2] = q.z;
+            v[4 * i + 3] = q.w;
+        }
+        const int2 hdr = zok ? a.closure_zhdr[zi] : make_int2(0, 4);
+        float y[4];
+        closure_mlp_rows(smem, st, v, y);
+        const bool net = v[kRecFlag] != 0.f;
+        const float cx = v[kRecCx], cy = v[kRecCy], sc = v[kRecScale];
+        const float2 q1 = net ? fk((cx * y[0] - cy * y[1]) * sc, (cy * y[0] + cx * y[1]) * sc) : fk(0.f, 0.f);
+        const float2 q2 = net ? fk((cx * y[2] - cy * y[3]) * sc, (cy * y[2] + cx * y[3]) * sc) : fk(0.f, 0.f);
+        const float cw = v[kRecCw], ccos = v[kRecCcos], rinv = v[kRecRinv];
+        const int n = hdr.y;
+        const int lp = g + (k == 0 ? n - 1 : k - 1);
+        const int ln = g + (k + 1 >= n ? 0 : k + 1);
+        const float rinv_prev = shflf(rinv, lp);
+        const float2 d1 = fmul(cw * rinv, fadd(q2, fmul(ccos, q1)));
+        const float2 d2 = fmul(cw * rinv_prev, fadd(q1, fmul(ccos, q2)));
+        const float2 d1p = shflf2(d1, lp);
+        const float2 d2n = shflf2(d2, ln);
+        if (zok && k < n) {
+            const int64_t sd = (int64_t)hdr.x + k;
+            const float2 cf = a.cforce_f[sd];
+            a.cforce_f[sd] = fadd(cf, fadd(fsub(d1, d2), fsub(d2n, d1p)));
+            const double2 sf = a.sftot[sd];
+            const float2 ds = fadd(d1, d2n);
+            a.sftot[sd] = mk(sf.x + (double)ds.x, sf.y + (double)ds.y);
+        }
+    }
+    const bool ok = closure_mlp_teardown(st);
+    if (!ok && threadIdx.x == 0) atomicAdd(a.closure_counts + kClassErr * 64, 1ull);
 }
 
 // ---------------------------------------------------------------------
@@ -448,13 +603,22 @@ __global__ void __launch_bounds__(kZoneThreadsC) pass_c_mixed(DevArrays a, Hydro
 
 }  // namespace
 
-cudaError_t launch_cycle_mixed(const DevArrays& a, const HydroConst& c, cudaStream_t stream, cudaEvent_t* ev) {
+namespace {
+
+cudaError_t launch_cycle_mixed_impl(const DevArrays& a, const HydroConst& c, cudaStream_t stream, cudaEvent_t* ev,
+                                    bool learned) {
     const int zb = (int)zone_blocks(a.numz);
     const int zbc = (int)zone_blocks(a.numz, kZoneThreadsC);
     const int pb = (int)((a.nump + kPointThreads - 1) / kPointThreads);
     if (ev) cudaEventRecord(ev[0], stream);
-    if (a.quads) pass_a_mixed<true><<<zb, kZoneThreads, 0, stream>>>(a, c);
-    else pass_a_mixed<false><<<zb, kZoneThreads, 0, stream>>>(a, c);
+    if (learned) {
+        if (a.quads) pass_a_mixed<true, true><<<zb, kZoneThreads, 0, stream>>>(a, c);
+        else pass_a_mixed<false, true><<<zb, kZoneThreads, 0, stream>>>(a, c);
+        closure_pass<<<a.closure_grid, kMlpRows, kMlpSmemBytes, stream>>>(a);
+    } else {
+        if (a.quads) pass_a_mixed<true, false><<<zb, kZoneThreads, 0, stream>>>(a, c);
+        else pass_a_mixed<false, false><<<zb, kZoneThreads, 0, stream>>>(a, c);
+    }
     if (ev) cudaEventRecord(ev[1], stream);
     pass_b_mixed<<<pb, kPointThreads, 0, stream>>>(a, c);
     if (ev) cudaEventRecord(ev[2], stream);
@@ -464,6 +628,20 @@ cudaError_t launch_cycle_mixed(const DevArrays& a, const HydroConst& c, cudaStre
     launch_finalize(a, c, zb, zbc, stream);
     if (ev) cudaEventRecord(ev[4], stream);
     return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_cycle_mixed(const DevArrays& a, const HydroConst& c, cudaStream_t stream, cudaEvent_t* ev) {
+    return launch_cycle_mixed_impl(a, c, stream, ev, false);
+}
+
+cudaError_t launch_cycle_learned(const DevArrays& a, const HydroConst& c, cudaStream_t stream, cudaEvent_t* ev) {
+    return launch_cycle_mixed_impl(a, c, stream, ev, true);
+}
+
+cudaError_t prepare_learned_kernels() {
+    return cudaFuncSetAttribute(closure_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, kMlpSmemBytes);
 }
 
 }  // namespace pnt

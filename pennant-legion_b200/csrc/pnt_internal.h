@@ -47,6 +47,10 @@ pnt_status generate_mesh(const Deck& d, Mesh& m);
 // Validates connectivity, builds zfirst/CSR and the initial geometry.
 pnt_status finish_mesh(Mesh& m);
 
+// The closure's device parameter image and device (closure.cu).
+const uint8_t* closure_image(const pnt_closure* c);
+int closure_device(const pnt_closure* c);
+
 }  // namespace pnt
 
 struct pnt_deck {

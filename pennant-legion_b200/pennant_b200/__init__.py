@@ -30,7 +30,13 @@ PNT_ERR_STATE = 9
 
 PREC_FP64 = 0
 PREC_MIXED = 1
+PREC_LEARNED = 2
 MAX_BC = 16
+
+CLOSURE_PARAMS = 5380
+CLOSURE_NORM = 36
+CLOSURE_IN = 14
+CLOSURE_CLASSES = ("zero", "dead", "mlp", "fallback", "ood", "acute", "error", "zones")
 
 FIELDS = {"px": 0, "pu": 1, "zr": 2, "ze": 3, "zp": 4, "zm": 5, "zetot": 6,
           "zvol": 7, "zwrate": 8, "smf": 9}
@@ -138,6 +144,20 @@ def _load():
         "pnt_batch_download": (i32, [vp, i32, i32, vp, sz]),
         "pnt_op_calc_dt": (i32, [vp, vp, vp, vp, vp, C.c_int64, dbl, dbl, dbl, vp, vp]),
         "pnt_op_calc_dt_noalloc": (i32, [vp, vp, vp, vp, vp, C.c_int64, dbl, dbl, dbl, vp, vp]),
+        "pnt_closure_create": (i32, [i32, C.c_uint64, pp]),
+        "pnt_closure_load": (i32, [C.c_char_p, i32, pp]),
+        "pnt_closure_save": (i32, [vp, C.c_char_p]),
+        "pnt_closure_destroy": (None, [vp]),
+        "pnt_closure_get": (i32, [vp, vp, vp, vp]),
+        "pnt_closure_set": (i32, [vp, vp, vp, vp]),
+        "pnt_hydro_harvest": (i32, [vp, dbl, dbl, C.c_uint64, vp, vp, vp, C.c_int64, C.POINTER(C.c_int64)]),
+        "pnt_closure_fit_normalization": (i32, [vp, vp, vp, C.c_int64]),
+        "pnt_closure_prepare": (i32, [vp, vp, vp, C.c_int64, vp, vp]),
+        "pnt_closure_train": (i32, [vp, vp, vp, C.c_int64, C.c_int64, i32, i32, C.c_float, vp]),
+        "pnt_closure_gradient": (i32, [vp, vp, vp, C.c_int64, vp, C.POINTER(C.c_float)]),
+        "pnt_closure_forward": (i32, [vp, vp, C.c_int64, vp]),
+        "pnt_hydro_set_closure": (i32, [vp, vp, i32]),
+        "pnt_hydro_closure_counts": (i32, [vp, C.POINTER(C.c_uint64), i32]),
         "pnt_hydro_write_xy": (i32, [vp, C.c_char_p]),
         "pnt_hydro_write_gold": (i32, [vp, C.c_char_p]),
     }
@@ -331,6 +351,23 @@ class Hydro:
         check(lib.pnt_hydro_stream(self.h, C.byref(p)))
         return p.value or 0
 
+    def set_closure(self, closure: "Closure", mode: int = 0) -> None:
+        """Learned cycle: 0 the network, 1 no force on its corners, 2 plain QCS there."""
+        check(lib.pnt_hydro_set_closure(self.h, closure.h, mode))
+        self.closure = closure
+
+    def closure_counts(self, reset: bool = False) -> dict:
+        out = (C.c_uint64 * len(CLOSURE_CLASSES))()
+        check(lib.pnt_hydro_closure_counts(self.h, out, 1 if reset else 0))
+        return dict(zip(CLOSURE_CLASSES, [int(v) for v in out]))
+
+    def harvest(self, dead: float, keep: float, seed: int, feats: int, targets: int, sides: int,
+                capacity: int, count: int) -> int:
+        """Appends closure training samples (device addresses) at `count`; returns the new count."""
+        n = C.c_int64(count)
+        check(lib.pnt_hydro_harvest(self.h, dead, keep, seed, feats, targets, sides, capacity, C.byref(n)))
+        return n.value
+
     def write_xy(self, path: str) -> None:
         check(lib.pnt_hydro_write_xy(self.h, _b(path)))
 
@@ -392,6 +429,61 @@ class Batch:
         out = np.empty(shape, dtype=np.float64)
         check(lib.pnt_batch_download(self.h, i, FIELDS[name], out.ctypes.data, out.nbytes))
         return out
+
+
+class Closure:
+    """The learned QCS closure: 14-64-64-4 network, its normalisation and thresholds."""
+
+    def __init__(self, seed: int = 0, device: int = 0, path: str | None = None):
+        h = C.c_void_p()
+        if path is not None:
+            check(lib.pnt_closure_load(_b(path), device, C.byref(h)))
+        else:
+            check(lib.pnt_closure_create(device, seed, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.pnt_closure_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def save(self, path: str) -> None:
+        check(lib.pnt_closure_save(self.h, _b(path)))
+
+    def get(self):
+        p = np.empty(CLOSURE_PARAMS, np.float32)
+        nm = np.empty(CLOSURE_NORM, np.float32)
+        th = np.empty(3, np.float32)
+        check(lib.pnt_closure_get(self.h, p.ctypes.data, nm.ctypes.data, th.ctypes.data))
+        return p, nm, th
+
+    def set(self, params=None, norm=None, thresholds=None) -> None:
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (params, norm, thresholds)]
+        ptrs = [None if a is None else a.ctypes.data for a in arrs]
+        check(lib.pnt_closure_set(self.h, *ptrs))
+
+    def fit_normalization(self, feats: int, targets: int, n: int) -> None:
+        check(lib.pnt_closure_fit_normalization(self.h, feats, targets, n))
+
+    def prepare(self, feats: int, targets: int, n: int, x: int, t: int) -> None:
+        check(lib.pnt_closure_prepare(self.h, feats, targets, n, x, t))
+
+    def train(self, x: int, t: int, n: int, first: int, steps: int, rows_per_step: int, lr: float) -> np.ndarray:
+        losses = np.zeros(max(steps, 1), np.float32)
+        check(lib.pnt_closure_train(self.h, x, t, n, first, steps, rows_per_step, lr, losses.ctypes.data))
+        return losses[:steps]
+
+    def gradient(self, x: int, t: int, n: int):
+        g = np.empty(CLOSURE_PARAMS, np.float32)
+        loss = C.c_float()
+        check(lib.pnt_closure_gradient(self.h, x, t, n, g.ctypes.data, C.byref(loss)))
+        return g, loss.value
+
+    def forward(self, feats: int, n: int, out: int) -> None:
+        check(lib.pnt_closure_forward(self.h, feats, n, out))
 
 
 def op_calc_dt(zdl: int, zdu: int, zss: int, zvol: int, zvol0: int, numz: int, cfl: float,

@@ -1,0 +1,209 @@
+"""The learned QCS closure on the GPU (needs a GPU): the harvest against the
+CPU oracle's QCS, the tcgen05 inference and the BF16 tensor-core training
+gradient against the CPU restatement of the network, training, and the
+learned cycle's accuracy with its ablations."""
+import os
+import sys
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import DECKS, golden
+from oracle import Oracle
+import closure_oracle as co
+import pennant_b200 as pb
+
+sys.path.insert(0, DECKS)
+from make_decks import sedov  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda:0"
+WEIGHTS = os.path.join(os.path.dirname(DECKS), "closure", "qcs_mlp.bin")
+QA, QB = 1.0 * 0.25 * (5.0 / 3.0 + 1.0), 0.1   # sedov decks: q2 = 1, q1 = 0.1, qgamma = 5/3
+
+
+def harvest_all(h, nums, dead=1e-6, keep=1.0, seed=1):
+    f = torch.empty((nums, 14), dtype=torch.float32, device=DEV)
+    t = torch.empty((nums, 4), dtype=torch.float32, device=DEV)
+    s = torch.empty((nums,), dtype=torch.int32, device=DEV)
+    n = h.harvest(dead, keep, seed, f.data_ptr(), t.data_ptr(), s.data_ptr(), nums, 0)
+    return f[:n].cpu().numpy(), t[:n].cpu().numpy(), s[:n].cpu().numpy()
+
+
+@pytest.mark.parametrize("text,cycles", [
+    (sedov(24, tstop=1.0), 40),
+    (open(golden("nohsmall.pnt")).read().replace("cstop   10", "cstop   100"), 30),
+])
+def test_harvest_matches_oracle_qcs(text, cycles):
+    d = pb.Deck(text=text)
+    m = pb.Mesh(deck=d)
+    h = pb.Hydro(m, d.params())
+    h.run(max_cycles=cycles)
+    f, t, s = harvest_all(h, m.nums)
+    assert len(s) > 20
+    # deterministic, and a keep < 1 harvest is a subset in the same order
+    f2, t2, s2 = harvest_all(h, m.nums)
+    assert np.array_equal(s, s2) and np.array_equal(f, f2) and np.array_equal(t, t2)
+    _, _, s3 = harvest_all(h, m.nums, keep=0.3, seed=9)
+    assert 0 < len(s3) < len(s) and np.all(np.isin(s3, s)) and np.all(np.diff(s3) > 0)
+
+    o = Oracle(text=text)
+    o.run(cycles + 1)
+    qa = 1.0 * 0.25 * (5.0 / 3.0 + 1.0) if "sedov" not in text else QA
+    fo, to, elig = co.corner_features(o, 1e-6, qa, QB)
+    es = np.nonzero(elig)[0]
+    # the eligible sets agree (up to corners with cdiv at roundoff level)
+    common = np.intersect1d(s, es)
+    assert len(common) >= 0.999 * max(len(s), len(es)), (len(s), len(es), len(common))
+    gi = np.searchsorted(s, common)
+    df = np.abs(f[gi] - fo[common])
+    assert df.max() < 1e-5, df.max()
+    scale = np.abs(to[common]).max()
+    dt = np.abs(t[gi] - to[common]) / scale
+    assert dt.max() < 1e-5, dt.max()
+
+
+def random_closure(seed):
+    rng = np.random.default_rng(seed)
+    c = pb.Closure(seed=seed)
+    p, _, _ = c.get()
+    norm = np.concatenate([rng.normal(size=14), rng.uniform(0.5, 2.0, 14),
+                           rng.normal(size=4), rng.uniform(0.5, 2.0, 4)]).astype(np.float32)
+    p = p + rng.normal(scale=0.05, size=p.shape).astype(np.float32)   # non-zero biases too
+    c.set(p, norm, np.array([1e-6, 0.5, 6.0], np.float32))
+    return c, p, norm, rng
+
+
+@pytest.mark.parametrize("n", [256, 1000, 1])
+def test_tcgen05_forward_matches_oracle(n):
+    c, p, norm, rng = random_closure(11)
+    feats = (rng.normal(size=(n, 14)) * norm[14:28] + norm[:14]).astype(np.float32)
+    ft = torch.from_numpy(feats).to(DEV)
+    out = torch.full((n, 4), float("nan"), dtype=torch.float32, device=DEV)
+    c.forward(ft.data_ptr(), n, out.data_ptr())
+    y = out.cpu().numpy()
+    x = co.normalise(feats, norm)
+    yn, _ = co.forward(p, x, bf16_round=True)
+    yo = yn * norm[32:36] + norm[28:32]
+    err = np.abs(y - yo)
+    print(f"n={n} max abs err {err.max():.3e}, mean {err.mean():.3e}, output scale {np.abs(yo).max():.3e}")
+    assert np.all(np.isfinite(y))
+    # BF16 activations: the GPU's tanh.approx GELU flips a few BF16 roundings
+    assert err.max() <= 2e-2 * np.abs(yo).max()
+    assert err.mean() <= 2e-3 * np.abs(yo).max()
+
+
+@pytest.mark.parametrize("n", [128, 300, 1024])
+def test_training_gradient_matches_oracle(n):
+    c, p, norm, rng = random_closure(5)
+    feats = (rng.normal(size=(n, 14)) * norm[14:28] + norm[:14]).astype(np.float32)
+    targs = rng.normal(size=(n, 4)).astype(np.float32) * norm[32:36] + norm[28:32]
+    ft, tt = torch.from_numpy(feats).to(DEV), torch.from_numpy(targs.astype(np.float32)).to(DEV)
+    x = torch.empty((n, 16), dtype=torch.bfloat16, device=DEV)
+    t = torch.empty((n, 4), dtype=torch.float32, device=DEV)
+    c.prepare(ft.data_ptr(), tt.data_ptr(), n, x.data_ptr(), t.data_ptr())
+    xn = x.float().cpu().numpy()
+    assert np.all(xn[:, 14:] == 0)
+    assert np.array_equal(xn[:, :14], co.bf16(co.normalise(feats, norm)))
+    tn = t.cpu().numpy()
+    g, loss = c.gradient(x.data_ptr(), t.data_ptr(), n)
+    lo, go = co.loss_grad(p, xn[:, :14], tn, bf16_round=True)
+    assert abs(loss - lo) <= 1e-4 * lo, (loss, lo)
+    for name, a, b in (("W1", co.W1, co.B1), ("b1", co.B1, co.W2), ("W2", co.W2, co.B2), ("b2", co.B2, co.W3),
+                       ("W3", co.W3, co.B3), ("b3", co.B3, co.N_PARAMS)):
+        rel = np.linalg.norm(g[a:b] - go[a:b]) / np.linalg.norm(go[a:b])
+        print(f"n={n} {name}: relative gradient error {rel:.2e}")
+        assert rel < 2e-3, (name, rel)
+
+
+def test_training_lowers_loss_and_save_load():
+    text = sedov(40, tstop=1.0)
+    d = pb.Deck(text=text)
+    m = pb.Mesh(deck=d)
+    h = pb.Hydro(m, d.params())
+    cap = 200000
+    f = torch.empty((cap, 14), dtype=torch.float32, device=DEV)
+    t = torch.empty((cap, 4), dtype=torch.float32, device=DEV)
+    s = torch.empty((cap,), dtype=torch.int32, device=DEV)
+    n = 0
+    for _ in range(30):
+        n = h.harvest(1e-6, 1.0, 3, f.data_ptr(), t.data_ptr(), s.data_ptr(), cap, n)
+        h.run(max_cycles=10)
+    assert n > 5000
+    c = pb.Closure(seed=1)
+    c.fit_normalization(f.data_ptr(), t.data_ptr(), n)
+    x = torch.empty((n, 16), dtype=torch.bfloat16, device=DEV)
+    tn = torch.empty((n, 4), dtype=torch.float32, device=DEV)
+    c.prepare(f.data_ptr(), t.data_ptr(), n, x.data_ptr(), tn.data_ptr())
+    _, l0 = c.gradient(x.data_ptr(), tn.data_ptr(), n)
+    losses = c.train(x.data_ptr(), tn.data_ptr(), n, 0, 300, 4096, 3e-3)
+    _, l1 = c.gradient(x.data_ptr(), tn.data_ptr(), n)
+    print(f"{n} samples: loss {l0:.4e} -> {l1:.4e}")
+    assert np.all(np.isfinite(losses)) and l1 < 0.1 * l0
+    # the same training again gives the same network (deterministic kernels)
+    c2 = pb.Closure(seed=1)
+    c2.fit_normalization(f.data_ptr(), t.data_ptr(), n)
+    c2.train(x.data_ptr(), tn.data_ptr(), n, 0, 300, 4096, 3e-3)
+    assert np.array_equal(c.get()[0], c2.get()[0])
+    path = os.path.join(os.environ.get("TMPDIR", "/tmp"), "pnt_closure_test.bin")
+    c.save(path)
+    c3 = pb.Closure(path=path)
+    for a, b in zip(c.get(), c3.get()):
+        assert np.array_equal(a, b)
+    os.remove(path)
+
+
+def test_learned_cycle_needs_a_closure():
+    d = pb.Deck(text=sedov(16, tstop=0.01))
+    d.set("precision", "learned")
+    h = pb.Hydro(pb.Mesh(deck=d), d.params())
+    with pytest.raises(pb.PntError) as e:
+        h.run()
+    assert e.value.status == pb.PNT_ERR_STATE
+    d2 = pb.Deck(text=sedov(16, tstop=0.01))
+    h2 = pb.Hydro(pb.Mesh(deck=d2), d2.params())
+    with pytest.raises(pb.PntError):
+        h2.set_closure(pb.Closure(seed=0))
+
+
+def run_prec(text, precision, closure=None, mode=0):
+    d = pb.Deck(text=text)
+    d.set("precision", precision)
+    h = pb.Hydro(pb.Mesh(deck=d), d.params())
+    if closure is not None:
+        h.set_closure(closure, mode)
+    s = h.run()
+    out = {k: h.download(k) for k in ("zr", "ze", "pu")}
+    counts = h.closure_counts() if closure is not None else None
+    h.close()
+    return s, out, counts
+
+
+def l1(a, b):
+    return float(np.abs(a - b).sum() / np.abs(b).sum())
+
+
+@pytest.mark.skipif(not os.path.exists(WEIGHTS), reason="trained closure file not built")
+def test_learned_cycle_accuracy_and_ablation():
+    """Sedov 48^2 to t = 1: the learned cycle against the FP64 cycle, and
+    what the network gains over the same cycle without it (no viscous force
+    on the network's corners).  Mode 2 (plain QCS on those corners)
+    measures the dead zone and FP32 alone."""
+    text = open(os.path.join(DECKS, "sedov48.pnt")).read()
+    clo = pb.Closure(path=WEIGHTS)
+    s64, f64, _ = run_prec(text, "fp64")
+    res = {}
+    for mode, name in ((0, "network"), (1, "no force"), (2, "plain QCS")):
+        s, f, cnt = run_prec(text, "learned", clo, mode)
+        assert s["status"] == 0 and cnt["error"] == 0
+        res[name] = (l1(f["zr"], f64["zr"]), l1(f["ze"], f64["ze"]), cnt)
+    for name, (er, ee, cnt) in res.items():
+        tot = sum(v for k, v in cnt.items() if k not in ("error", "zones"))
+        frac = {k: v / tot for k, v in cnt.items() if k != "error"}
+        print(f"{name}: L1 rho {er:.3e} e {ee:.3e}; classes {frac}")
+    er_net = res["network"][0]
+    assert res["network"][2]["mlp"] > 0
+    assert er_net <= 1e-3
+    assert res["no force"][0] > 2 * er_net   # the network carries the force it replaces
