@@ -2,18 +2,27 @@
 """Benchmark of the hydro cycle: zone-cycles/s on the 1920^2 Sedov deck.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--precision learned|mixed|fp64] [--full-run]
 
 A step is one hydro cycle (Hydro::doCycle plus the Driver's dt update) over
-the whole mesh.  `value` is device-timed throughput with the state resident
-in HBM (CUDA events on the library's stream around K graph-replayed cycles,
-barrier + synchronize on both sides, max over ranks).  With N > 1 (torchrun,
-one rank per GPU) each rank runs an independent replica: the single-mesh
-path has no multi-GPU decomposition in this build, so scaling is weak.
+the whole mesh.  Every path is timed from the same state: the plain FP64
+cycle run to cycle --start-cycles (30000, t ~ 0.06: a developed blast whose
+shock spans the mesh; the first cycles of the deck have almost no
+compressing corners and would flatter the learned closure) and copied into
+each path's object.  `value` is device-timed throughput with the state
+resident in HBM (CUDA events on the library's stream around K
+graph-replayed cycles, barrier + synchronize on both sides, max over
+ranks).  With N > 1 (torchrun, one rank per GPU) each rank runs an
+independent replica (the single-mesh path has no multi-GPU decomposition):
+scaling is weak.
 
-The headline path is the mixed-precision cycle (FP32 side forces, FP64
-kinematics/volumes/work/dt; `--precision fp64` selects the plain cycle); the
-plain FP64 cycle is timed beside it on the same deck and the headline path's
-relative L1 errors against it are reported.
+The headline path is the learned cycle: the mixed-precision cycle (FP32
+side geometry, TTS and QCS forces; FP64 point kinematics, volumes, EOS,
+work and dt) with the learned closure in place of QCS on its corners.  The
+plain FP64 cycle and the mixed cycle with the plain QCS are timed beside it,
+and the headline path's relative L1 errors against the FP64 cycle are
+reported after the timed window and over whole runs to t = 1 (480^2 by
+default; 1920^2 as well with --full-run).
 
 `e2e` runs the same K cycles through the C ABI from host buffers: state
 uploaded from pinned host memory, one pnt_hydro_cycle call per step (each
@@ -22,7 +31,8 @@ returns that step's dt/time to the host), final fields downloaded.
 `--impl reference` times the reference's CPU path on this machine's host
 cores: the oracle (a restatement of the reference's *OMPTask loops; the
 reference itself needs the Legion runtime and cannot be built here) with
-all host threads, one cycle of the same deck per step.
+all host threads, one cycle of the same deck per step from its initial
+state (the plain QCS does the same work per cycle whatever the state).
 """
 import argparse
 import json
@@ -37,10 +47,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "pennant-legion_b200")
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 sys.path.insert(0, PKG)
+sys.path.insert(0, os.path.join(PKG, "decks"))
 
 METRIC = "zone-cycles/s on 1920² Sedov, learned+FP32 vs plain FP64 GPU at ≤1e-3 L1 err"
 UNIT = "zone-cycles/s"
 DEFAULT_DECK = os.path.join(PKG, "decks", "sedov1920.pnt")
+DEFAULT_CLOSURE = os.path.join(PKG, "closure", "qcs_mlp.bin")
+MLP_FLOP_PER_ROW = 2 * (16 * 64 + 64 * 64 + 64 * 16)   # tensor-core MMA shapes, padded
 
 
 def algorithmic_bytes(nump, nums, numz):
@@ -188,8 +201,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--deck", default=DEFAULT_DECK)
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+    ap.add_argument("--precision", default="learned", choices=["learned", "mixed", "fp64"],
                     help="path of the headline value; the plain FP64 cycle is always timed beside it")
+    ap.add_argument("--closure", default=DEFAULT_CLOSURE)
+    ap.add_argument("--start-cycles", type=int, default=30000)
+    ap.add_argument("--full-run", action="store_true", help="also run 1920^2 to t = 1 with each path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()
@@ -206,20 +222,27 @@ def main():
     import torch
     import torch.distributed as dist
     import pennant_b200 as pb
+    from make_decks import sedov
 
     torch.cuda.set_device(local_rank)
     if world > 1:
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local_rank))
 
     mesh = pb.Mesh(deck=pb.Deck(path=args.deck))
     nump, numz, nums = mesh.nump, mesh.numz, mesh.nums
     ab = algorithmic_bytes(nump, nums, numz)
+    closure = pb.Closure(path=args.closure, device=local_rank) if args.precision == "learned" else None
 
-    def make(precision):
-        d = pb.Deck(path=args.deck)
+    def make(precision, text=None, **keys):
+        d = pb.Deck(text=text) if text is not None else pb.Deck(path=args.deck)
         d.set("precision", precision)
-        return pb.Hydro(mesh, d.params(), device=local_rank)
+        for k, v in keys.items():
+            d.set(k, v)
+        h = pb.Hydro(mesh if text is None else pb.Mesh(deck=d), d.params(), device=local_rank)
+        if precision == "learned":
+            h.set_closure(closure)
+        return h
 
     def barrier_sync():
         torch.cuda.synchronize()
@@ -233,10 +256,24 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    def l1(a, b):
+        return float(np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300))
+
+    def errors(h, ref):
+        return {"zr": l1(h.download("zr"), ref.download("zr")), "ze": l1(h.download("ze"), ref.download("ze")),
+                "u": l1(np.hypot(*h.download("pu").T), np.hypot(*ref.download("pu").T)),
+                "cycles": h.scalars()["cycle"], "cycles_fp64": ref.scalars()["cycle"], "time": h.scalars()["time"]}
+
+    def fractions(c):
+        tot = sum(v for k, v in c.items() if k not in ("error", "zones"))
+        return {k: v / max(tot, 1) for k, v in c.items() if k not in ("error", "zones")}
+
     gpu_index = os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)).split(",")[local_rank if world > 1 else 0]
 
-    def timed(h, sample_clocks):
+    def timed(h, learned, sample_clocks):
         h.time_cycles(args.warmup)      # graph capture + W cycles
+        if learned:
+            h.closure_counts(reset=True)
         barrier_sync()
         clocks = None
         if sample_clocks:
@@ -250,47 +287,86 @@ def main():
             ms = h.time_cycles(args.steps)
             barrier_sync()
         s = h.scalars()
-        if s["status"] or s["cycle"] < args.warmup + args.steps:
+        if s["status"] or s["done"]:
             raise SystemExit(f"run stopped early: {s}")
         return max_over_ranks(ms), clocks
 
-    names = ["A", "B", "C", "finalize"]
-    head = make(args.precision)
-    ms_head, clocks = timed(head, True)
-    kms_head = head.time_kernels(10)
-    if args.precision == "fp64":
-        ref64, ms_64, kms_64 = head, ms_head, kms_head
-    else:
-        ref64 = make("fp64")
-        ms_64, _ = timed(ref64, False)
-        kms_64 = ref64.time_kernels(10)
-    value = world * numz * args.steps / (ms_head / 1e3)
-    value_64 = world * numz * args.steps / (ms_64 / 1e3)
+    # the common start state: the FP64 cycle to cycle --start-cycles
+    t0 = time.perf_counter()
+    base = make("fp64", cstop=args.start_cycles)
+    s0 = base.run()
+    start = {"cycle": s0["cycle"], "time": s0["time"], "setup_s": time.perf_counter() - t0,
+             "note": "plain FP64 run from the deck's initial state, copied into every timed path"}
 
-    # accuracy of the headline path against the FP64 cycle after the same
-    # number of cycles (the FP64 cycle is bit-identical to the CPU oracle)
-    def l1(a, b):
-        return float(np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300))
+    order = [args.precision] + [p for p in ("fp64", "mixed") if p != args.precision]
+    heads, res = {}, {}
+    for p in order:
+        h = make(p)
+        h.copy_state_from(base)
+        heads[p] = h
+        ms, clocks = timed(h, p == "learned", p == args.precision)
+        cnt = h.closure_counts(reset=True) if p == "learned" else None
+        kms = h.time_kernels(10)
+        res[p] = {"ms": ms, "clocks": clocks, "kernel_ms": kms, "counts": cnt,
+                  "value": world * numz * args.steps / (ms / 1e3)}
+    base.close()
+    head = heads[args.precision]
+    window_err = {p: errors(heads[p], heads["fp64"]) for p in order if p != "fp64"}
+    for p in order:
+        if p != args.precision:
+            heads[p].close()
 
-    err = None
-    if ref64 is not head:
-        c1, c2 = head.scalars()["cycle"], ref64.scalars()["cycle"]
-        assert c1 == c2, (c1, c2)
-        err = {"zr": l1(head.download("zr"), ref64.download("zr")),
-               "ze": l1(head.download("ze"), ref64.download("ze")),
-               "u": l1(np.hypot(*head.download("pu").T), np.hypot(*ref64.download("pu").T)),
-               "cycles": c1, "time": head.scalars()["time"]}
-        ref64.close()
+    # whole runs to t = 1 against the FP64 cycle: 480^2 always, 1920^2 with --full-run
+    def full_run(n):
+        text = sedov(n, tstop=1.0)
+        ref = make("fp64", text=text)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        ref.run()
+        out = {"fp64": {"wall_s": time.perf_counter() - t1, "cycles": ref.scalars()["cycle"]}}
+        for p in order:
+            if p == "fp64":
+                continue
+            h = make(p, text=text)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            h.run()
+            out[p] = {"wall_s": time.perf_counter() - t1, "l1_rel_err_vs_fp64": errors(h, ref)}
+            if p == "learned":
+                out[p]["corner_fractions"] = fractions(h.closure_counts())
+            h.close()
+        ref.close()
+        return out
+
+    full = {"480": full_run(480)}
+    if args.full_run:
+        full["1920"] = full_run(1920)
 
     hbm, peak_kind = measured_peaks()
+    names = ["A", "B", "C", "finalize", "closure"]
+    kms_head = res[args.precision]["kernel_ms"]
     dom = int(np.argmax(kms_head[:3]))
-    if args.precision == "mixed":
+    if args.precision in ("mixed", "learned"):
         per_launch = {"A": 32 * nump + 44 * numz + 32 * nums, "B": 68 * nump + 16 * nums,
                       "C": 64 * nump + 12 * nums + 60 * numz}
     else:
         per_launch = {k: ab[k] for k in ("A", "B", "C")}
     ach_dom = per_launch[names[dom]] / (kms_head[dom] / 1e3) / 1e9
+    ms_head = res[args.precision]["ms"]
     ach_cycle = ab["cycle"] * args.steps / (ms_head / 1e3) / 1e9
+
+    closure_info = None
+    if args.precision == "learned":
+        cnt = res["learned"]["counts"]
+        zones_per_cycle = cnt["zones"] / args.steps
+        cl_ms = kms_head[4]
+        closure_info = {
+            "corner_fractions": fractions(cnt),
+            "fallback_fraction_of_compressing": (cnt["fallback"] + cnt["ood"] + cnt["acute"]) /
+            max(cnt["mlp"] + cnt["fallback"] + cnt["ood"] + cnt["acute"], 1),
+            "zones_per_cycle": zones_per_cycle, "closure_pass_ms": cl_ms,
+            "tensor_tflops": (4 * zones_per_cycle * MLP_FLOP_PER_ROW) / (cl_ms / 1e3) / 1e12 if cl_ms > 0 else None,
+            "wait_timeouts": cnt["error"], "weights": os.path.relpath(args.closure, ROOT)}
 
     # end to end through the C ABI with pinned host buffers
     fields = ["px", "pu", "zr", "ze", "zm", "zetot", "zwrate", "zvol"]
@@ -318,21 +394,31 @@ def main():
 
     result = None
     if rank == 0:
-        path = ("mixed precision: FP32 edge/corner geometry and TTS/QCS side forces, FP64 point kinematics, "
-                "volumes, EOS, work and dt; plain QCS" if args.precision == "mixed"
-                else "plain FP64 (bitwise parity path)")
+        paths = {
+            "learned": "learned closure + mixed precision: the 14-64-64-4 BF16 network (tcgen05) in place of QCS "
+                       "on compressing corners within its range, plain QCS elsewhere; FP32 side geometry and "
+                       "TTS/QCS forces, FP64 point kinematics, volumes, EOS, work and dt",
+            "mixed": "mixed precision: FP32 edge/corner geometry and TTS/QCS side forces, FP64 point kinematics, "
+                     "volumes, EOS, work and dt; plain QCS",
+            "fp64": "plain FP64 (bitwise parity path)"}
+        launches = 5 if args.precision == "learned" else 4
+        others = {p: {"value": res[p]["value"], "ms_per_step": res[p]["ms"] / args.steps,
+                      "kernel_ms": dict(zip(names, res[p]["kernel_ms"]))} for p in order if p != args.precision}
         result = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_head / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+            "metric": METRIC, "value": res[args.precision]["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_head / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"learned": "bf16+f32+f64", "mixed": "f32+f64", "fp64": "f64"}[args.precision],
+            "data": "synthetic",
             "config": {"workload": f"{os.path.basename(args.deck)} ({numz} zones, {nums} sides, {nump} points)",
-                       "path": path, "cycles_per_step": 1, "parallelism": f"replicas x{world}",
+                       "path": paths[args.precision], "cycles_per_step": 1, "parallelism": f"replicas x{world}",
+                       "start_state": start,
                        "l2": "working set > 1 GB per GPU >> 126 MB L2 (no flush needed)",
-                       "fp64_plain": {"value": value_64, "ms_per_step": ms_64 / args.steps,
-                                      "kernel_ms": dict(zip(names, kms_64))},
-                       "speedup_vs_fp64": value / value_64,
-                       "l1_rel_err_vs_fp64": err},
+                       "others": others,
+                       "speedup_vs_fp64": res[args.precision]["value"] / res["fp64"]["value"],
+                       "l1_rel_err_vs_fp64_window": window_err,
+                       "full_runs_to_t1": full,
+                       "closure": closure_info},
             "roofline": {"bound": "hbm", "kernel": f"pass {names[dom]} ({args.precision})", "achieved": ach_dom,
                          "peak": hbm, "unit": "GB/s", "frac": ach_dom / hbm, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": per_launch[names[dom]], "launch_ms": kms_head[dom],
@@ -346,8 +432,8 @@ def main():
                     "note": "state uploaded from pinned host memory once per timed run, one pnt_hydro_cycle "
                             "call per step (returns the step's dt/time), final fields downloaded; "
                             "bytes per step are run totals / steps"},
-            "gpu_launches": 4 * args.steps,
-            "clocks": clocks,
+            "gpu_launches": launches * args.steps,
+            "clocks": res[args.precision]["clocks"],
         }
     if world > 1:
         dist.barrier()

@@ -191,9 +191,15 @@ pnt_status pnt_hydro_get_scalars(pnt_hydro* hydro, pnt_scalars* out);
  * Driver.cc:117-168): runs `ncycles` cycles launching each pass separately
  * with CUDA events around it and writes the mean milliseconds of pass i to
  * kernel_ms[i] for i < nkernels (0 pass A zone predictor, 1 pass B point
- * update, 2 pass C zone corrector, 3 finalize). */
+ * update, 2 pass C zone corrector, 3 finalize, 4 the learned cycle's closure
+ * pass, 0 for the other cycles). */
 pnt_status pnt_hydro_time_kernels(pnt_hydro* hydro, int32_t ncycles, double* kernel_ms,
                                   int32_t nkernels);
+/* Copies the run state (point positions and velocities, zone fields, time,
+ * dt, cycle) of `src` into `dst`: two objects of the same mesh on the same
+ * device, whatever their precision (a restart of dst from src's state; no
+ * counterpart in the reference). */
+pnt_status pnt_hydro_copy_state(pnt_hydro* dst, const pnt_hydro* src);
 /* Enqueues `ncycles` cycles (graph replay) between two CUDA events on the
  * object's stream, waits, and returns the elapsed device milliseconds. */
 pnt_status pnt_hydro_time_cycles(pnt_hydro* hydro, int32_t ncycles, double* elapsed_ms);

@@ -453,22 +453,25 @@ pnt_status pnt_hydro_enqueue(pnt_hydro* h, int32_t ncycles) {
 pnt_status pnt_hydro_time_kernels(pnt_hydro* h, int32_t ncycles, double* kernel_ms, int32_t nkernels) {
     if (!h || !kernel_ms || ncycles <= 0 || nkernels <= 0) return fail(PNT_ERR_INVALID_ARG, "bad argument");
     DeviceGuard dg(h->device);
-    std::vector<cudaEvent_t> ev((size_t)ncycles * (kNumPasses + 1), nullptr);
+    std::vector<cudaEvent_t> ev((size_t)ncycles * kNumEvents, nullptr);
     pnt_status st = PNT_OK;
     for (auto& e : ev) {
         if (cudaEventCreate(&e) != cudaSuccess) { st = fail(PNT_ERR_CUDA, "cudaEventCreate failed"); break; }
     }
     for (int32_t i = 0; i < ncycles && !st; ++i) {
-        const cudaError_t e = h->launch(h->a, h->hc, h->stream, &ev[(size_t)i * (kNumPasses + 1)]);
+        const cudaError_t e = h->launch(h->a, h->hc, h->stream, &ev[(size_t)i * kNumEvents]);
         if (e != cudaSuccess) st = fail(PNT_ERR_CUDA, "cycle launch: %s", cudaGetErrorString(e));
     }
     if (!st && cudaStreamSynchronize(h->stream) != cudaSuccess) st = fail(PNT_ERR_CUDA, "synchronize failed");
     if (!st) {
         for (int k = 0; k < nkernels; ++k) kernel_ms[k] = 0.;
+        // kernel k runs between events from[k] and from[k] + 1
+        static const int from[kNumKernels] = {0, 2, 3, 4, 1};
         for (int32_t i = 0; i < ncycles; ++i) {
-            for (int k = 0; k < kNumPasses && k < nkernels; ++k) {
+            for (int k = 0; k < kNumKernels && k < nkernels; ++k) {
                 float ms = 0.f;
-                cudaEventElapsedTime(&ms, ev[(size_t)i * (kNumPasses + 1) + k], ev[(size_t)i * (kNumPasses + 1) + k + 1]);
+                const cudaEvent_t* e = &ev[(size_t)i * kNumEvents];
+                cudaEventElapsedTime(&ms, e[from[k]], e[from[k] + 1]);
                 kernel_ms[k] += ms / ncycles;
             }
         }
@@ -705,6 +708,33 @@ pnt_status pnt_hydro_closure_counts(pnt_hydro* h, uint64_t* counts, int32_t rese
         for (int b = 0; b < 64; ++b) t += raw[q * 64 + b];
         counts[q] = t;
     }
+    return PNT_OK;
+}
+
+pnt_status pnt_hydro_copy_state(pnt_hydro* dst, const pnt_hydro* src) {
+    if (!dst || !src) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    if (dst->device != src->device || dst->nump != src->nump || dst->numz != src->numz || dst->nums != src->nums)
+        return fail(PNT_ERR_INVALID_ARG, "objects differ in mesh or device");
+    if (dst == src) return PNT_OK;
+    DeviceGuard dg(dst->device);
+    pnt_hydro* s = const_cast<pnt_hydro*>(src);
+    if (pnt_status st = s->fetch_ctl()) return st;
+    const size_t np = (size_t)src->nump * sizeof(double2), nz = (size_t)src->numz * sizeof(double);
+    CUDA_TRY(cudaStreamSynchronize(dst->stream));
+    for (int b = 0; b < 2; ++b) {
+        CUDA_TRY(cudaMemcpyAsync(dst->a.px[b], src->a.px[b], np, cudaMemcpyDeviceToDevice, dst->stream));
+        CUDA_TRY(cudaMemcpyAsync(dst->a.pu[b], src->a.pu[b], np, cudaMemcpyDeviceToDevice, dst->stream));
+    }
+    double* zd[] = {dst->a.zm, dst->a.zr, dst->a.ze, dst->a.zetot, dst->a.zwrate, dst->a.zvol, dst->a.zp};
+    const double* zs[] = {src->a.zm, src->a.zr, src->a.ze, src->a.zetot, src->a.zwrate, src->a.zvol, src->a.zp};
+    for (int i = 0; i < 7; ++i) CUDA_TRY(cudaMemcpyAsync(zd[i], zs[i], nz, cudaMemcpyDeviceToDevice, dst->stream));
+    // run state: the source's, with done judged again by dst's deck
+    Ctl c = *src->ctl_host;
+    c.stop_at = INT_MAX;
+    c.done = (c.status != 0 || c.cycle >= dst->params.cstop || !(c.time < dst->params.tstop)) ? 1 : 0;
+    *dst->ctl_host = c;
+    CUDA_TRY(cudaMemcpyAsync(dst->a.ctl, dst->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, dst->stream));
+    CUDA_TRY(cudaStreamSynchronize(dst->stream));
     return PNT_OK;
 }
 

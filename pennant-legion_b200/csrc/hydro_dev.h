@@ -100,11 +100,13 @@ inline int64_t zone_blocks(int32_t numz, int threads = kZoneThreads) {
     return (4 * (int64_t)numz + threads - 1) / threads;
 }
 
-constexpr int kNumPasses = 4;   // A, B, C, finalize
+// Events a cycle records when timed: before pass A, after A, after the
+// closure pass (right after A when there is none), after B, C, finalize.
+constexpr int kNumEvents = 6;
+constexpr int kNumKernels = 5;   // A, B, C, finalize, closure pass
 
 // One hydro cycle (passes A, B, C and the finalize step) on `stream`.  With
-// `ev` non-null, ev[i] is recorded before pass i and ev[kNumPasses] after
-// the last one.
+// `ev` non-null, the kNumEvents events above are recorded.
 cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStream_t stream,
                               cudaEvent_t* ev = nullptr);
 // The mixed-precision cycle (hydro_mixed.cu).

@@ -130,13 +130,14 @@ cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStrea
     if (a.quads) pass_a<true><<<zb, kZoneThreads, 0, stream>>>(a, c);
     else pass_a<false><<<zb, kZoneThreads, 0, stream>>>(a, c);
     if (ev) cudaEventRecord(ev[1], stream);
+    if (ev) cudaEventRecord(ev[2], stream);   // no closure pass
     pass_b<<<pb, kPointThreads, 0, stream>>>(a, c);
-    if (ev) cudaEventRecord(ev[2], stream);
+    if (ev) cudaEventRecord(ev[3], stream);
     if (a.quads) pass_c<true><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
     else pass_c<false><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
-    if (ev) cudaEventRecord(ev[3], stream);
-    finalize<<<1, kFinThreads, 0, stream>>>(a, c, zb, zbc);
     if (ev) cudaEventRecord(ev[4], stream);
+    finalize<<<1, kFinThreads, 0, stream>>>(a, c, zb, zbc);
+    if (ev) cudaEventRecord(ev[5], stream);
     return cudaGetLastError();
 }
 

@@ -614,19 +614,21 @@ cudaError_t launch_cycle_mixed_impl(const DevArrays& a, const HydroConst& c, cud
     if (learned) {
         if (a.quads) pass_a_mixed<true, true><<<zb, kZoneThreads, 0, stream>>>(a, c);
         else pass_a_mixed<false, true><<<zb, kZoneThreads, 0, stream>>>(a, c);
+        if (ev) cudaEventRecord(ev[1], stream);
         closure_pass<<<a.closure_grid, kMlpRows, kMlpSmemBytes, stream>>>(a);
     } else {
         if (a.quads) pass_a_mixed<true, false><<<zb, kZoneThreads, 0, stream>>>(a, c);
         else pass_a_mixed<false, false><<<zb, kZoneThreads, 0, stream>>>(a, c);
+        if (ev) cudaEventRecord(ev[1], stream);
     }
-    if (ev) cudaEventRecord(ev[1], stream);
-    pass_b_mixed<<<pb, kPointThreads, 0, stream>>>(a, c);
     if (ev) cudaEventRecord(ev[2], stream);
+    pass_b_mixed<<<pb, kPointThreads, 0, stream>>>(a, c);
+    if (ev) cudaEventRecord(ev[3], stream);
     if (a.quads) pass_c_mixed<true><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
     else pass_c_mixed<false><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
-    if (ev) cudaEventRecord(ev[3], stream);
-    launch_finalize(a, c, zb, zbc, stream);
     if (ev) cudaEventRecord(ev[4], stream);
+    launch_finalize(a, c, zb, zbc, stream);
+    if (ev) cudaEventRecord(ev[5], stream);
     return cudaGetLastError();
 }
 

@@ -127,6 +127,7 @@ def _load():
         "pnt_hydro_synchronize": (i32, [vp]),
         "pnt_hydro_time_kernels": (i32, [vp, i32, C.POINTER(C.c_double), i32]),
         "pnt_hydro_time_cycles": (i32, [vp, i32, C.POINTER(C.c_double)]),
+        "pnt_hydro_copy_state": (i32, [vp, vp]),
         "pnt_hydro_get_scalars": (i32, [vp, C.POINTER(Scalars)]),
         "pnt_hydro_download": (i32, [vp, i32, vp, sz]),
         "pnt_hydro_upload": (i32, [vp, i32, vp, sz]),
@@ -306,10 +307,14 @@ class Hydro:
         check(lib.pnt_hydro_enqueue(self.h, ncycles))
 
     def time_kernels(self, ncycles: int) -> list:
-        """Mean ms of passes A, B, C, finalize over `ncycles` (these cycles advance the run)."""
-        out = (C.c_double * 4)()
-        check(lib.pnt_hydro_time_kernels(self.h, ncycles, out, 4))
+        """Mean ms of passes A, B, C, finalize and the closure pass over `ncycles`
+        (these cycles advance the run)."""
+        out = (C.c_double * 5)()
+        check(lib.pnt_hydro_time_kernels(self.h, ncycles, out, 5))
         return list(out)
+
+    def copy_state_from(self, src: "Hydro") -> None:
+        check(lib.pnt_hydro_copy_state(self.h, src.h))
 
     def time_cycles(self, ncycles: int) -> float:
         """Device milliseconds of `ncycles` graph-replayed cycles (CUDA events on the stream)."""
