@@ -54,6 +54,12 @@ UNIT = "zone-cycles/s"
 DEFAULT_DECK = os.path.join(PKG, "decks", "sedov1920.pnt")
 DEFAULT_CLOSURE = os.path.join(PKG, "closure", "qcs_mlp.bin")
 MLP_FLOP_PER_ROW = 2 * (16 * 64 + 64 * 64 + 64 * 16)   # tensor-core MMA shapes, padded
+# DRAM bytes (read + write) of one pass A launch per zone, from the ncu
+# capture of profiles/pass_a_closure_sedov1024.md (1,048,576 zones; the
+# bench scales them by its zone count)
+PASS_A_TRAFFIC_PER_ZONE = {"learned": (127.181e6 + 99.845e6) / 1048576,
+                           "mixed": (125.929e6 + 88.921e6) / 1048576,
+                           "fp64": (126.054e6 + 148.091e6) / 1048576}
 
 
 def algorithmic_bytes(nump, nums, numz):
@@ -194,6 +200,131 @@ def run_reference(args, rank, world):
     return 0
 
 
+def l1_rel(a, b):
+    import numpy as np
+    return float(np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300))
+
+
+def run_leblanc(args, pb, np, torch):
+    """The Leblanc-type tube (2880 x 288 over [0,9] x [0,0.9], rho 1 / e 0.1 for
+    x < 3, rho 1e-3 / e 1e-7 beyond) to t = 6 with the FP64, mixed and learned
+    cycles: whole-run zone-cycles/s (wall clock around pnt_hydro_run, which
+    replays graphs and polls the done flag) and the L1 errors of rho, e, |u|
+    against the FP64 run."""
+    from make_decks import leblanc
+    text = leblanc()
+    closure = pb.Closure(path=args.closure)
+    out = {"metric": "whole-run zone-cycles/s and L1 errors vs FP64", "workload": "leblanc2880x288 to t=6",
+           "unit": "zone-cycles/s", "data": "synthetic"}
+    ref = None
+    for p in ("fp64", "mixed", "learned"):
+        d = pb.Deck(text=text)
+        d.set("precision", p)
+        m = pb.Mesh(deck=d)
+        h = pb.Hydro(m, d.params())
+        if p == "learned":
+            h.set_closure(closure)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s = h.run()
+        wall = time.perf_counter() - t0
+        r = {"cycles": s["cycle"], "time": s["time"], "wall_s": wall, "value": m.numz * s["cycle"] / wall}
+        f = {k: h.download(k) for k in ("zr", "ze", "pu")}
+        if p == "fp64":
+            ref = f
+        else:
+            r["l1_rel_err_vs_fp64"] = {"rho": l1_rel(f["zr"], ref["zr"]), "e": l1_rel(f["ze"], ref["ze"]),
+                                       "u": l1_rel(np.hypot(*f["pu"].T), np.hypot(*ref["pu"].T))}
+        if p == "learned":
+            c = h.closure_counts()
+            tot = sum(v for k, v in c.items() if k not in ("error", "zones"))
+            r["corner_fractions"] = {k: v / max(tot, 1) for k, v in c.items() if k not in ("error", "zones")}
+        out[p] = r
+        h.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_batch(args, pb, np, torch):
+    """The seeded 256-instance Sedov batch (decks/make_decks.py sedov_batch:
+    N log-uniform in [32, 512], E0 in [0.1, 1], gamma in [1.4, 5/3], t = 0.5)
+    in one pnt_batch (autotuned tile shape, persistent launches, CUDA graph),
+    against the same instances run one after another as single-mesh objects
+    (graph replay each).  Both timings are wall clock around the runs with
+    the objects already created; a sample of instances is compared bit for
+    bit."""
+    from make_decks import sedov_batch
+    insts = sedov_batch(256)
+    decks = [pb.Deck(text=i["text"]) for i in insts]
+    meshes = [pb.Mesh(deck=d) for d in decks]
+    params = [d.params() for d in decks]
+    tuner = pb.Batch(meshes, params)
+    zpt, cps, ms_tune = tuner.tune(4)
+    tuner.close()
+    b = pb.Batch(meshes, params)
+    b.set_shape(zpt, cps)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    left = b.run()
+    t_batch = time.perf_counter() - t0
+    sc = [b.scalars(i) for i in range(len(insts))]
+    zc = sum(m.numz * s["cycle"] for m, s in zip(meshes, sc))
+    hs = [pb.Hydro(m, p) for m, p in zip(meshes, params)]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for h in hs:
+        h.run()
+    t_seq = time.perf_counter() - t0
+    mismatch = 0
+    for i in range(0, len(insts), 16):
+        for k in ("zr", "ze", "px", "pu"):
+            mismatch += int(hs[i].download(k).tobytes() != b.download(i, k).tobytes())
+    out = {"metric": "zone-cycles/s, 256-instance Sedov batch to t=0.5", "unit": "zone-cycles/s",
+           "value": zc / t_batch, "data": "synthetic", "dtype": "f64",
+           "config": {"instances": len(insts), "zones": sum(m.numz for m in meshes), "zone_cycles": zc,
+                      "cycles_min": min(s["cycle"] for s in sc), "cycles_max": max(s["cycle"] for s in sc),
+                      "tile_zones": zpt, "ctas_per_sm": cps, "tuned_ms_per_cycle": ms_tune,
+                      "left_running": left},
+           "batch_wall_s": t_batch, "sequential_wall_s": t_seq, "sequential_value": zc / t_seq,
+           "speedup_vs_sequential": t_seq / t_batch, "sampled_instances_bitwise_mismatches": mismatch,
+           "status_nonzero": sum(1 for s in sc if s["status"])}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_probe(args, pb, sedov, torch):
+    """A developed state (the FP64 cycle to --start-cycles on Sedov N^2) and one
+    single-launch cycle of each path from it inside the NVTX range 'prof',
+    after one unmarked cycle: the small case the pass A profiles capture."""
+    text = sedov(args.probe)
+    closure = pb.Closure(path=args.closure)
+
+    def make(p, **keys):
+        d = pb.Deck(text=text)
+        d.set("precision", p)
+        for k, v in keys.items():
+            d.set(k, v)
+        h = pb.Hydro(pb.Mesh(deck=d), d.params())
+        if p == "learned":
+            h.set_closure(closure)
+        return h
+
+    base = make("fp64", cstop=args.start_cycles)
+    base.run()
+    out = {"probe": args.probe, "start_cycle": base.scalars()["cycle"], "time": base.scalars()["time"]}
+    for p in ("mixed", "learned", "fp64"):
+        h = make(p)
+        h.copy_state_from(base)
+        h.cycle()
+        torch.cuda.nvtx.range_push("prof")
+        h.cycle()
+        torch.cuda.nvtx.range_pop()
+        out[p] = h.scalars()["cycle"]
+        h.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -206,6 +337,15 @@ def main():
     ap.add_argument("--closure", default=DEFAULT_CLOSURE)
     ap.add_argument("--start-cycles", type=int, default=30000)
     ap.add_argument("--full-run", action="store_true", help="also run 1920^2 to t = 1 with each path")
+    ap.add_argument("--no-full-480", action="store_true",
+                    help="skip the 480^2 whole runs (short profiling runs)")
+    ap.add_argument("--workload", default="sedov1920", choices=["sedov1920", "leblanc", "batch"],
+                    help="sedov1920: the headline line; leblanc: the 2880x288 Leblanc-type tube to t = 6 "
+                         "with each path (accuracy of the mixed cycle); batch: the seeded 256-instance "
+                         "Sedov batch to t = 0.5, batched against one instance at a time")
+    ap.add_argument("--probe", type=int, default=0, metavar="N",
+                    help="profiling probe instead of the benchmark: Sedov N^2, the FP64 cycle to "
+                         "--start-cycles, then one single-launch cycle of each path inside NVTX range 'prof'")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()
@@ -225,6 +365,12 @@ def main():
     from make_decks import sedov
 
     torch.cuda.set_device(local_rank)
+    if args.probe:
+        return run_probe(args, pb, sedov, torch)
+    if args.workload == "leblanc":
+        return run_leblanc(args, pb, np, torch)
+    if args.workload == "batch":
+        return run_batch(args, pb, np, torch)
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local_rank))
@@ -270,21 +416,26 @@ def main():
 
     gpu_index = os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)).split(",")[local_rank if world > 1 else 0]
 
-    def timed(h, learned, sample_clocks):
+    def timed(h, learned, sample_clocks, name):
         h.time_cycles(args.warmup)      # graph capture + W cycles
         if learned:
             h.closure_counts(reset=True)
         barrier_sync()
         clocks = None
+        # NVTX range "timed_<path>": lets a profiler select the timed kernels
         if sample_clocks:
             with ClockSampler(gpu_index) as clk:
                 barrier_sync()
+                torch.cuda.nvtx.range_push(f"timed_{name}")
                 ms = h.time_cycles(args.steps)
+                torch.cuda.nvtx.range_pop()
                 barrier_sync()
             clocks = clk.summary()
         else:
             barrier_sync()
+            torch.cuda.nvtx.range_push(f"timed_{name}")
             ms = h.time_cycles(args.steps)
+            torch.cuda.nvtx.range_pop()
             barrier_sync()
         s = h.scalars()
         if s["status"] or s["done"]:
@@ -304,7 +455,7 @@ def main():
         h = make(p)
         h.copy_state_from(base)
         heads[p] = h
-        ms, clocks = timed(h, p == "learned", p == args.precision)
+        ms, clocks = timed(h, p == "learned", p == args.precision, p)
         cnt = h.closure_counts(reset=True) if p == "learned" else None
         kms = h.time_kernels(10)
         res[p] = {"ms": ms, "clocks": clocks, "kernel_ms": kms, "counts": cnt,
@@ -338,7 +489,7 @@ def main():
         ref.close()
         return out
 
-    full = {"480": full_run(480)}
+    full = {} if args.no_full_480 else {"480": full_run(480)}
     if args.full_run:
         full["1920"] = full_run(1920)
 
@@ -422,7 +573,9 @@ def main():
             "roofline": {"bound": "hbm", "kernel": f"pass {names[dom]} ({args.precision})", "achieved": ach_dom,
                          "peak": hbm, "unit": "GB/s", "frac": ach_dom / hbm, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": per_launch[names[dom]], "launch_ms": kms_head[dom],
-                         "traffic": None},
+                         "traffic": PASS_A_TRAFFIC_PER_ZONE[args.precision] * numz if names[dom] == "A" else None,
+                         "traffic_note": "ncu DRAM read+write of one pass A launch at 1024^2 (cycle 16000), "
+                                         "scaled by the zone count"},
             "roofline_cycle": {"achieved": ach_cycle, "peak": hbm, "unit": "GB/s", "frac": ach_cycle / hbm,
                                "algorithmic_bytes_per_cycle": ab["cycle"],
                                "note": "FP64 schedule bytes B = 164 Np + 100 Ns + 104 Nz for every path"},

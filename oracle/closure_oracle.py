@@ -148,8 +148,9 @@ def corner_features(o, dead: float, qa: float, qb: float):
     e1, e2 = xpp - xp, xpn - xp
     iL = 2.0 / (np.hypot(*e1.T) + np.hypot(*e2.T))
     d1, d2, dc = up - upp, upn - up, uz - up
-    D = np.sqrt(np.maximum(np.maximum((d1 ** 2).sum(1), (d2 ** 2).sum(1)), (dc ** 2).sum(1)))
-    live = D > dead * css
+    m2 = np.maximum(np.maximum((d1 ** 2).sum(1), (d2 ** 2).sum(1)), (dc ** 2).sum(1))
+    D = np.sqrt(m2)
+    live = m2 > (dead * css) ** 2
     Ds = np.where(live, D, 1.0)
     Q = qa * Ds + qb * css
     scale = Ds * Q

@@ -106,13 +106,8 @@ template <typename T>
 __device__ __forceinline__ bool closure_features(ClV<T> xp, ClV<T> xpp, ClV<T> xpn, ClV<T> xz, ClV<T> up, ClV<T> upp,
                                                  ClV<T> upn, ClV<T> uz, ClV<T> uav, T css, T qa, T qb, T dead,
                                                  float* f, T& cx, T& cy, T& scale) {
-    const T dx = xz.x - xp.x, dy = xz.y - xp.y;
-    const T il = T(1) / cl_sqrt(dx * dx + dy * dy);
-    cx = dx * il;
-    cy = dy * il;
-    const T e1x = xpp.x - xp.x, e1y = xpp.y - xp.y;
-    const T e2x = xpn.x - xp.x, e2y = xpn.y - xp.y;
-    const T iL = T(2) / (cl_sqrt(e1x * e1x + e1y * e1y) + cl_sqrt(e2x * e2x + e2y * e2y));
+    // the dead-zone test first, on squares: most compressing corners ahead
+    // of a shock carry round-off velocities and stop here
     const T d1x = up.x - upp.x, d1y = up.y - upp.y;
     const T d2x = upn.x - up.x, d2y = upn.y - up.y;
     const T dcx = uz.x - up.x, dcy = uz.y - up.y;
@@ -120,8 +115,16 @@ __device__ __forceinline__ bool closure_features(ClV<T> xp, ClV<T> xpp, ClV<T> x
     const T n2 = d2x * d2x + d2y * d2y, nc = dcx * dcx + dcy * dcy;
     m2 = (n2 > m2) ? n2 : m2;
     m2 = (nc > m2) ? nc : m2;
+    const T lim = dead * css;
+    if (!(m2 > lim * lim)) return false;
     const T D = cl_sqrt(m2);
-    if (!(D > dead * css)) return false;
+    const T dx = xz.x - xp.x, dy = xz.y - xp.y;
+    const T il = T(1) / cl_sqrt(dx * dx + dy * dy);
+    cx = dx * il;
+    cy = dy * il;
+    const T e1x = xpp.x - xp.x, e1y = xpp.y - xp.y;
+    const T e2x = xpn.x - xp.x, e2y = xpn.y - xp.y;
+    const T iL = T(2) / (cl_sqrt(e1x * e1x + e1y * e1y) + cl_sqrt(e2x * e2x + e2y * e2y));
     const T Q = qa * D + qb * css;
     scale = D * Q;
     const T iD = T(1) / D;

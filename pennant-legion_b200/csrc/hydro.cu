@@ -678,7 +678,7 @@ pnt_status pnt_hydro_set_closure(pnt_hydro* h, const pnt_closure* c, int32_t mod
         h->a.closure_rec = rec;
         h->a.closure_zhdr = hdr;
         h->a.closure_nrec = nrec;
-        h->a.closure_grid = 2 * nsm;
+        h->a.closure_grid = 3 * nsm;   // 3 x 128 TMEM columns and 3 x 54 KB shared memory per SM
     }
     // the image lives in this object: a copy of the closure's, with the mode
     uint8_t* img = const_cast<uint8_t*>(h->a.closure_img);

@@ -147,8 +147,12 @@ __device__ double2 qcs_sfq_fp64(double2 xp, double2 xp2, double2 zxp, double2 u0
 // ---------------------------------------------------------------------
 // Pass A, mixed precision
 // ---------------------------------------------------------------------
+#ifndef PNT_LEARNED_A_MIN_BLOCKS
+#define PNT_LEARNED_A_MIN_BLOCKS 3
+#endif
 template <bool kQuads, bool kLearned>
-__global__ void __launch_bounds__(kZoneThreads, 3) pass_a_mixed(DevArrays a, HydroConst c) {
+__global__ void __launch_bounds__(kZoneThreads, kLearned ? PNT_LEARNED_A_MIN_BLOCKS : 3)
+    pass_a_mixed(DevArrays a, HydroConst c) {
     const Ctl* ctl = a.ctl;
     if (skip_cycle(ctl)) return;
     const int cur = ctl->cycle & 1;
@@ -474,7 +478,7 @@ __global__ void __launch_bounds__(kPointThreads) pass_b_mixed(DevArrays a, Hydro
 // which only touch the recorded zone's own sides: no two records write the
 // same side, so the update is deterministic without atomics.
 // ---------------------------------------------------------------------
-__global__ void __launch_bounds__(kMlpRows, 2) closure_pass(DevArrays a) {
+__global__ void __launch_bounds__(kMlpRows, 3) closure_pass(DevArrays a) {
     if (skip_cycle(a.ctl)) return;
     const int nrec = *a.closure_nrec;
     if (blockIdx.x == 0 && threadIdx.x == 0 && nrec)
