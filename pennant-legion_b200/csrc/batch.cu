@@ -189,6 +189,7 @@ struct pnt_batch {
     void* parts = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_cycles = 8;
+    int32_t live = 0;                            // instances in the current work lists
 
     ~pnt_batch() {
         int prev = -1;
@@ -220,13 +221,18 @@ struct pnt_batch {
         return PNT_OK;
     }
 
-    // Work lists for a tile shape; partial arrays sized to the zone tiles.
+    // Work lists for a tile shape over the instances still running (ctl_host
+    // must be current); partial arrays sized to the zone tiles.  Finished
+    // instances get no tiles, so the persistent passes do not walk them.
     pnt_status build_tiles(const Shape& sh) {
         std::vector<Tile> zt, pt;
         std::vector<int32_t> tb(ninst + 1, 0);
         const int ppt = kBatchThreads * 4;   // points per point tile
+        int32_t nlive = 0;
         for (int i = 0; i < ninst; ++i) {
             tb[i] = (int32_t)zt.size();
+            if (ctl_host[i].done) continue;
+            ++nlive;
             for (int64_t z = 0; z < nz[i]; z += sh.zones_per_tile)
                 zt.push_back({i, (int32_t)(zoff[i] + z), (int32_t)(zoff[i] + std::min<int64_t>(nz[i], z + sh.zones_per_tile)),
                               quads[i]});
@@ -234,6 +240,7 @@ struct pnt_batch {
                 pt.push_back({i, (int32_t)(poff[i] + p), (int32_t)(poff[i] + std::min<int64_t>(np[i], p + ppt)), quads[i]});
         }
         tb[ninst] = (int32_t)zt.size();
+        live = nlive;
         if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
         CUDA_TRY(cudaStreamSynchronize(stream));
         if (ztiles) cudaFree(ztiles);
@@ -242,12 +249,12 @@ struct pnt_batch {
         if (parts) cudaFree(parts);
         ztiles = nullptr; ptiles = nullptr; inst_tbeg = nullptr; parts = nullptr;
         const size_t nzt = zt.size();
-        CUDA_TRY(cudaMalloc(&ztiles, nzt * sizeof(Tile)));
-        CUDA_TRY(cudaMalloc(&ptiles, pt.size() * sizeof(Tile)));
+        CUDA_TRY(cudaMalloc(&ztiles, std::max<size_t>(nzt, 1) * sizeof(Tile)));
+        CUDA_TRY(cudaMalloc(&ptiles, std::max<size_t>(pt.size(), 1) * sizeof(Tile)));
         CUDA_TRY(cudaMalloc(&inst_tbeg, tb.size() * sizeof(int32_t)));
-        CUDA_TRY(cudaMalloc(&parts, nzt * (2 * sizeof(double) + 2 * sizeof(int32_t))));
-        CUDA_TRY(cudaMemcpy(ztiles, zt.data(), nzt * sizeof(Tile), cudaMemcpyHostToDevice));
-        CUDA_TRY(cudaMemcpy(ptiles, pt.data(), pt.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMalloc(&parts, std::max<size_t>(nzt, 1) * (2 * sizeof(double) + 2 * sizeof(int32_t))));
+        if (nzt) CUDA_TRY(cudaMemcpy(ztiles, zt.data(), nzt * sizeof(Tile), cudaMemcpyHostToDevice));
+        if (!pt.empty()) CUDA_TRY(cudaMemcpy(ptiles, pt.data(), pt.size() * sizeof(Tile), cudaMemcpyHostToDevice));
         CUDA_TRY(cudaMemcpy(inst_tbeg, tb.data(), tb.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
         b.ztiles = ztiles;
         b.ptiles = ptiles;
@@ -554,6 +561,8 @@ pnt_status pnt_batch_set_shape(pnt_batch* bt, int32_t zones_per_tile, int32_t ct
         return fail(PNT_ERR_INVALID_ARG, "tile must be a positive multiple of %d zones, 1-8 CTAs per SM",
                     kZonesPerIter);
     DeviceGuard dg(bt->device);
+    pnt_status st = bt->fetch_ctls();
+    if (st) return st;
     return bt->build_tiles(Shape{zones_per_tile, ctas_per_sm});
 }
 
@@ -600,6 +609,7 @@ pnt_status pnt_batch_tune(pnt_batch* bt, int32_t trial_cycles, int32_t* zones_pe
     static const int kCtas[] = {2, 3, 4};
     Shape best{256, 3};
     double best_ms = 1e300;
+    if (pnt_status st = bt->fetch_ctls()) return st;
     for (int tz : kTiles) {
         for (int cs : kCtas) {
             pnt_status st = bt->build_tiles(Shape{tz, cs});
@@ -613,7 +623,8 @@ pnt_status pnt_batch_tune(pnt_batch* bt, int32_t trial_cycles, int32_t* zones_pe
             }
         }
     }
-    pnt_status st = bt->build_tiles(best);
+    pnt_status st = bt->fetch_ctls();
+    if (!st) st = bt->build_tiles(best);
     if (st) return st;
     if (zones_per_tile) *zones_per_tile = best.zones_per_tile;
     if (ctas_per_sm) *ctas_per_sm = best.ctas_per_sm;
@@ -628,6 +639,9 @@ pnt_status pnt_batch_run(pnt_batch* bt, int32_t max_cycles, int32_t* running_lef
     int running = 0;
     pnt_status st = bt->running(&running);
     while (!st && running > 0 && (max_cycles <= 0 || done_cycles < max_cycles)) {
+        // drop finished instances from the work lists
+        if (running < bt->live && (st = bt->fetch_ctls()) == PNT_OK) st = bt->build_tiles(bt->shape);
+        if (st) break;
         const int chunk = max_cycles > 0 ? (int)std::min<int64_t>(64, max_cycles - done_cycles) : 64;
         if ((st = bt->enqueue(chunk))) break;
         done_cycles += chunk;
