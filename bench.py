@@ -513,8 +513,9 @@ def main():
         cl_ms = kms_head[4]
         closure_info = {
             "corner_fractions": fractions(cnt),
-            "fallback_fraction_of_compressing": (cnt["fallback"] + cnt["ood"] + cnt["acute"]) /
-            max(cnt["mlp"] + cnt["fallback"] + cnt["ood"] + cnt["acute"], 1),
+            # plain-QCS share of the compressing corners the network could take
+            # (zones with an acute corner keep the FP64 QCS whatever the compression)
+            "fallback_fraction": (cnt["fallback"] + cnt["ood"]) / max(cnt["mlp"] + cnt["fallback"] + cnt["ood"], 1),
             "zones_per_cycle": zones_per_cycle, "closure_pass_ms": cl_ms,
             "tensor_tflops": (4 * zones_per_cycle * MLP_FLOP_PER_ROW) / (cl_ms / 1e3) / 1e12 if cl_ms > 0 else None,
             "wait_timeouts": cnt["error"], "weights": os.path.relpath(args.closure, ROOT)}
