@@ -73,12 +73,15 @@ constexpr int kImgBytes = 13056;
 __host__ __device__ constexpr int canon_off(int r, int k, int rows) { return (k >> 3) * rows * 16 + r * 16 + (k & 7) * 2; }
 
 // Deferred corners of the learned cycle: pass A records every zone that has
-// a corner for the network (64 zones = 256 rows per inference batch).  Per
-// corner 24 floats: inputs [0,14), frame cx cy, force scale zrp*D*(aD+bc),
-// cw, ccos (QCS::setForce's corner weights, QCS.cc:331-380), 1/elen of the
-// corner's side, class flag (1 = network), pad.  Per zone: first side, sides.
+// a compressing corner outside the dead zone (64 zones = 256 rows per
+// inference batch) with the raw FP32 data of each corner, relative to the
+// zone's first point: position, previous and next points, zone centre,
+// velocities of the point, previous and next points and the zone centre,
+// the mean corner velocity (absolute), the zone's sound speed and density,
+// and a flag (1 = deferred corner).  Per zone: first side, sides.
 constexpr int kRecFloats = 24;
-enum { kRecCx = 14, kRecCy = 15, kRecScale = 16, kRecCw = 17, kRecCcos = 18, kRecRinv = 19, kRecFlag = 20 };
+enum { kRecX = 0, kRecXp = 2, kRecXn = 4, kRecXz = 6, kRecU = 8, kRecUp = 10, kRecUn = 12, kRecUz = 14,
+       kRecUav = 16, kRecSs = 18, kRecRho = 19, kRecFlag = 20 };
 
 // Shared memory of the 256-row inference block.
 constexpr int kMlpRows = 256;

@@ -148,10 +148,13 @@ __device__ double2 qcs_sfq_fp64(double2 xp, double2 xp2, double2 zxp, double2 u0
 // Pass A, mixed precision
 // ---------------------------------------------------------------------
 #ifndef PNT_LEARNED_A_MIN_BLOCKS
-#define PNT_LEARNED_A_MIN_BLOCKS 3
+#define PNT_LEARNED_A_MIN_BLOCKS 4
+#endif
+#ifndef PNT_MIXED_A_MIN_BLOCKS
+#define PNT_MIXED_A_MIN_BLOCKS 4
 #endif
 template <bool kQuads, bool kLearned>
-__global__ void __launch_bounds__(kZoneThreads, kLearned ? PNT_LEARNED_A_MIN_BLOCKS : 3)
+__global__ void __launch_bounds__(kZoneThreads, kLearned ? PNT_LEARNED_A_MIN_BLOCKS : PNT_MIXED_A_MIN_BLOCKS)
     pass_a_mixed(DevArrays a, HydroConst c) {
     const Ctl* ctl = a.ctl;
     if (skip_cycle(ctl)) return;
@@ -293,45 +296,27 @@ __global__ void __launch_bounds__(kZoneThreads, kLearned ? PNT_LEARNED_A_MIN_BLO
     };
     if constexpr (kLearned) corner_sin2();
 
-    // The learned closure (closure_dev.cuh) replaces the corner forces of
-    // compressing corners outside the dead zone that are neither strongly
-    // compressed nor out of distribution; the others keep the plain QCS.
-    // Those corners get no force here: their zones are recorded and the
-    // closure pass adds the network's force to the zones' sides.
+    // The learned cycle (closure_dev.cuh) forms no QCS corner force here:
+    // compressing corners outside the dead zone are deferred (their zones
+    // recorded with the corners' raw data) to the closure pass, which runs
+    // the network or, past its range, the plain QCS; the rest carry none.
+    // Zones with an acute corner keep the FP64 QCS below.
     bool plain = cdiv < 0.f;
     int cls = kClassZero;
     if constexpr (kLearned) {
-        float f[kClIn];
-        float fcx = 0.f, fcy = 0.f, fscale = 0.f;
-        const float* thr = reinterpret_cast<const float*>(a.closure_img + kImgThr);
-        const float dead = __ldg(thr), rho_max = __ldg(thr + 1), kappa = __ldg(thr + 2);
-        const int mode = (int)__ldg(thr + 3);   // 0 network, 1 no force, 2 plain QCS
-        const float2 xpp = shflf2(r, lp);
-        const float2 uav = fadd(fmul(0.25f, fadd(fadd(fadd(up0, up1), up2), up3)), f2(uref));
+        plain = false;
+        const float dead = __ldg(reinterpret_cast<const float*>(a.closure_img + kImgThr));
+        // dead-zone test on squares (closure_features' first step)
+        const float2 d1 = fsub(uf, upf), d2 = fsub(u2f, uf), dc = fsub(zuc, uf);
+        const float m2 = fmaxf(fmaxf(flen2(d1), flen2(d2)), flen2(dc));
+        const float lim = dead * zssf;
         if (act && acute) cls = kClassAcute;
-        else if (act && cdiv < 0.f) {
-            const bool live = closure_features<float>({r.x, r.y}, {xpp.x, xpp.y}, {r2.x, r2.y}, {zc.x, zc.y},
-                                                      {uf.x, uf.y}, {upf.x, upf.y}, {u2f.x, u2f.y}, {zuc.x, zuc.y},
-                                                      {uav.x, uav.y}, zssf, (float)(c.q2 * 0.25 * c.gammap1),
-                                                      (float)c.q1, dead, f, fcx, fcy, fscale);
-            if (!live) cls = kClassDead;
-            else if (f[11] > rho_max) cls = kClassFallback;
-            else {
-                const float* mean = reinterpret_cast<const float*>(a.closure_img + kImgFMean);
-                const float* istd = reinterpret_cast<const float*>(a.closure_img + kImgFIstd);
-                float zmax = 0.f;
-#pragma unroll
-                for (int i = 0; i < kClIn; ++i) zmax = fmaxf(zmax, fabsf((f[i] - __ldg(mean + i)) * __ldg(istd + i)));
-                cls = (zmax > kappa) ? kClassOod : kClassMlp;
-            }
-        }
-        plain = (cls == kClassFallback || cls == kClassOod || (cls == kClassMlp && mode == 2));
-        // record the zones with a corner for the network (one bit per zone:
-        // its first lane), all four corners of each
-        const bool net = cls == kClassMlp && mode == 0;
-        int zflag = net ? 1 : 0;
+        else if (act && cdiv < 0.f) cls = (m2 > lim * lim) ? kClassMlp : kClassDead;   // kClassMlp: deferred
+        const bool defer = cls == kClassMlp;
+        int zflag = defer ? 1 : 0;
         zflag |= __shfl_xor_sync(kFull, zflag, 1);
         zflag |= __shfl_xor_sync(kFull, zflag, 2);
+        const float2 xpp = shflf2(r, lp);
         const unsigned zbits = __ballot_sync(kFull, zflag && k == 0);
         int base = 0;
         if (lane == 0 && zbits) base = atomicAdd(a.closure_nrec, __popc(zbits));
@@ -339,21 +324,13 @@ __global__ void __launch_bounds__(kZoneThreads, kLearned ? PNT_LEARNED_A_MIN_BLO
         if (zflag) {
             const int idx = base + __popc(zbits & ((1u << g) - 1u));
             float4* rec = reinterpret_cast<float4*>(a.closure_rec + ((int64_t)idx * 4 + k) * kRecFloats);
-            const float nf = net ? 1.f : 0.f;
-            const float sc = net ? zrpf * fscale : 0.f;
-            float v[kRecFloats];
-#pragma unroll
-            for (int i = 0; i < kClIn; ++i) v[i] = net ? f[i] : 0.f;
-            v[kRecCx] = fcx;
-            v[kRecCy] = fcy;
-            v[kRecScale] = sc;
-            v[kRecCw] = (csin2 < 1.e-4f) ? 0.f : cvolume / csin2;
-            v[kRecCcos] = (csin2 < 1.e-4f) ? 0.f : ccos;
-            v[kRecRinv] = rinv_el;
-            v[kRecFlag] = nf;
-            v[21] = v[22] = v[23] = 0.f;
-#pragma unroll
-            for (int i = 0; i < kRecFloats / 4; ++i) rec[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+            const float2 uav = fadd(fmul(0.25f, fadd(fadd(fadd(up0, up1), up2), up3)), f2(uref));
+            rec[0] = make_float4(r.x, r.y, xpp.x, xpp.y);
+            rec[1] = make_float4(r2.x, r2.y, zc.x, zc.y);
+            rec[2] = make_float4(uf.x, uf.y, upf.x, upf.y);
+            rec[3] = make_float4(u2f.x, u2f.y, zuc.x, zuc.y);
+            rec[4] = make_float4(uav.x, uav.y, zssf, zrpf);
+            rec[5] = make_float4(defer ? 1.f : 0.f, 0.f, 0.f, 0.f);
             if (k == 0) a.closure_zhdr[idx] = make_int2((int)(s - k), n);
         }
     }
@@ -404,21 +381,23 @@ __global__ void __launch_bounds__(kZoneThreads, kLearned ? PNT_LEARNED_A_MIN_BLO
         a.sftot[s] = sfpq;
     }
 
-    __shared__ unsigned wcount[kLearned ? kZoneThreads / 32 : 1][kClassErr];
+    // pass A counts the corners without compression, in the dead zone and in
+    // acute zones; the closure pass counts the deferred ones by class
+    constexpr int kCounted[3] = {kClassZero, kClassDead, kClassAcute};
+    __shared__ unsigned wcount[kLearned ? kZoneThreads / 32 : 1][3];
     if constexpr (kLearned) {
-        // corner class counts per warp, summed per block below
-        for (int q = 0; q < kClassErr; ++q) {
-            const unsigned nq = __popc(__ballot_sync(kFull, act && cls == q));
+        for (int q = 0; q < 3; ++q) {
+            const unsigned nq = __popc(__ballot_sync(kFull, act && cls == kCounted[q]));
             if (lane == 0) wcount[threadIdx.x >> 5][q] = nq;
         }
     }
 
     const int nbad = __syncthreads_count(bad);
     if constexpr (kLearned) {
-        if (threadIdx.x < kClassErr) {
+        if (threadIdx.x < 3) {
             unsigned t = 0;
             for (int w = 0; w < kZoneThreads / 32; ++w) t += wcount[w][threadIdx.x];
-            if (t) atomicAdd(a.closure_counts + threadIdx.x * 64 + (blockIdx.x & 63), (unsigned long long)t);
+            if (t) atomicAdd(a.closure_counts + kCounted[threadIdx.x] * 64 + (blockIdx.x & 63), (unsigned long long)t);
         }
     }
     if (blockIdx.x >= (unsigned)a.npartA) return;   // partials are sized for this grid
@@ -467,26 +446,38 @@ __global__ void __launch_bounds__(kPointThreads) pass_b_mixed(DevArrays a, Hydro
 }
 
 // ---------------------------------------------------------------------
-// Closure pass (learned cycle): the network on the corners of the zones
-// pass A recorded, 64 zones (256 corners) per tcgen05 batch, persistent.
-// A corner's QCS forces cqe1, cqe2 enter QCS::setForce (QCS.cc:331-380)
-// linearly: its side s gets d1 = cw (cqe2 + ccos cqe1) / elen[s] and the
-// previous side gets d2 = cw (cqe1 + ccos cqe2) / elen[s3].  The corner
-// force of side s, ftot[s] - ftot[s3] (Hydro.cc:1159-1193), and sfp + sfq
-// of side s then change by
+// Closure pass (learned cycle): the deferred corners of the zones pass A
+// recorded, 64 zones (256 corners) per batch, persistent.  Each deferred
+// corner is classified (compression past rho_max or inputs out of
+// distribution: plain QCS, QCS.cc:116-327 in FP32 as in the mixed pass A;
+// otherwise the network, tcgen05, closure_dev.cuh); a tile without network
+// corners skips the network.  A corner's QCS forces cqe1, cqe2 enter
+// QCS::setForce (QCS.cc:331-380) linearly: its side s gets
+// d1 = cw (cqe2 + ccos cqe1) / elen[s] and the previous side
+// d2 = cw (cqe1 + ccos cqe2) / elen[s3].  The corner force of side s,
+// ftot[s] - ftot[s3] (Hydro.cc:1159-1193), and sfp + sfq of side s then
+// change by
 //   dcforce[s] = d1(s) - d2(s) - d1(s3) + d2(s4),  dsftot[s] = d1(s) + d2(s4),
 // which only touch the recorded zone's own sides: no two records write the
 // same side, so the update is deterministic without atomics.
 // ---------------------------------------------------------------------
-__global__ void __launch_bounds__(kMlpRows, 3) closure_pass(DevArrays a) {
+__global__ void __launch_bounds__(kMlpRows, 3) closure_pass(DevArrays a, HydroConst c) {
     if (skip_cycle(a.ctl)) return;
     const int nrec = *a.closure_nrec;
     if (blockIdx.x == 0 && threadIdx.x == 0 && nrec)
         atomicAdd(a.closure_counts + kClassZones * 64, (unsigned long long)nrec);
     if ((int64_t)blockIdx.x * 64 >= nrec) return;
     extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ unsigned ccount[3];   // network, fallback, out of distribution
+    if (threadIdx.x < 3) ccount[threadIdx.x] = 0u;
     MlpState st;
-    closure_mlp_setup(smem, a.closure_img, st);
+    closure_mlp_setup(smem, a.closure_img, st);   // its barrier publishes ccount's zeros
+    const float* thr = reinterpret_cast<const float*>(smem + kImgThr);
+    const float rho_max = thr[1], kappa = thr[2];
+    const int mode = (int)thr[3];   // 0 network, 1 no force, 2 plain QCS
+    const float* mean = reinterpret_cast<const float*>(smem + kImgFMean);
+    const float* istd = reinterpret_cast<const float*>(smem + kImgFIstd);
+    const float qa = (float)(c.q2 * 0.25 * c.gammap1), qb = (float)c.q1;
     const int k = threadIdx.x & 3, lane = threadIdx.x & 31, g = lane & ~3;
     for (int tile = blockIdx.x; (int64_t)tile * 64 < nrec; tile += gridDim.x) {
         const int zi = tile * 64 + (threadIdx.x >> 2);
@@ -502,19 +493,86 @@ __global__ void __launch_bounds__(kMlpRows, 3) closure_pass(DevArrays a) {
             v[4 * i + 3] = q.w;
         }
         const int2 hdr = zok ? a.closure_zhdr[zi] : make_int2(0, 4);
-        float y[4];
-        closure_mlp_rows(smem, st, v, y);
-        const bool net = v[kRecFlag] != 0.f;
-        const float cx = v[kRecCx], cy = v[kRecCy], sc = v[kRecScale];
-        const float2 q1 = net ? fk((cx * y[0] - cy * y[1]) * sc, (cy * y[0] + cx * y[1]) * sc) : fk(0.f, 0.f);
-        const float2 q2 = net ? fk((cx * y[2] - cy * y[3]) * sc, (cy * y[2] + cx * y[3]) * sc) : fk(0.f, 0.f);
-        const float cw = v[kRecCw], ccos = v[kRecCcos], rinv = v[kRecRinv];
+        const float2 x = fk(v[kRecX], v[kRecX + 1]), xpv = fk(v[kRecXp], v[kRecXp + 1]);
+        const float2 xn = fk(v[kRecXn], v[kRecXn + 1]), xz = fk(v[kRecXz], v[kRecXz + 1]);
+        const float2 u = fk(v[kRecU], v[kRecU + 1]), upv = fk(v[kRecUp], v[kRecUp + 1]);
+        const float2 un = fk(v[kRecUn], v[kRecUn + 1]), uz = fk(v[kRecUz], v[kRecUz + 1]);
+        const float2 uav = fk(v[kRecUav], v[kRecUav + 1]);
+        const float css = v[kRecSs], rho = v[kRecRho];
+        // classify the deferred corners
+        int cls = -1;
+        float f[kClIn];
+        float cx = 0.f, cy = 0.f, scale = 0.f;
+        if (v[kRecFlag] != 0.f &&
+            closure_features<float>({x.x, x.y}, {xpv.x, xpv.y}, {xn.x, xn.y}, {xz.x, xz.y}, {u.x, u.y},
+                                    {upv.x, upv.y}, {un.x, un.y}, {uz.x, uz.y}, {uav.x, uav.y}, css, qa, qb, 0.f,
+                                    f, cx, cy, scale)) {
+            if (f[11] > rho_max) cls = kClassFallback;
+            else {
+                float zmax = 0.f;
+#pragma unroll
+                for (int i = 0; i < kClIn; ++i) zmax = fmaxf(zmax, fabsf((f[i] - mean[i]) * istd[i]));
+                cls = (zmax > kappa) ? kClassOod : kClassMlp;
+            }
+        }
+        const bool net = cls == kClassMlp && mode == 0;
+        const bool plain = cls == kClassFallback || cls == kClassOod || (cls == kClassMlp && mode == 2);
+        {
+            const unsigned nm = __popc(__ballot_sync(kFull, cls == kClassMlp));
+            const unsigned nf = __popc(__ballot_sync(kFull, cls == kClassFallback));
+            const unsigned no = __popc(__ballot_sync(kFull, cls == kClassOod));
+            if (lane == 0) {
+                if (nm) atomicAdd(&ccount[0], nm);
+                if (nf) atomicAdd(&ccount[1], nf);
+                if (no) atomicAdd(&ccount[2], no);
+            }
+        }
+        if (!net) {
+#pragma unroll
+            for (int i = 0; i < kClIn; ++i) f[i] = 0.f;
+        }
+        float y[4] = {0.f, 0.f, 0.f, 0.f};
+        if (__syncthreads_or(net)) closure_mlp_rows(smem, st, f, y);
+        // corner geometry (QCS::setCornerDiv / setForce, FP32 as in pass A)
+        const float2 ex = fmul(0.5f, fadd(x, xn));
+        const float2 xq3 = fmul(0.5f, fadd(xpv, x));
+        const float cvolume = 0.5f * fcross(fsub(xz, x), fsub(xq3, ex));
+        const float2 v1 = fsub(xq3, x), v2 = fsub(ex, x);
+        const float de1 = flen(fsub(x, xpv)), de2 = flen(fsub(xn, x));
+        const float rinv_de1 = 1.f / de1, rinv_el = 1.f / de2;
+        const float minelen = fminf(de1, de2);
+        float ccos = (minelen < 1.e-12f) ? 0.f : 4.f * fdot(v1, v2) / (de1 * de2);
+        float2 q1 = fk(0.f, 0.f), q2 = fk(0.f, 0.f);
+        if (net) {
+            const float sc = rho * scale;
+            q1 = fk((cx * y[0] - cy * y[1]) * sc, (cy * y[0] + cx * y[1]) * sc);
+            q2 = fk((cx * y[2] - cy * y[3]) * sc, (cy * y[2] + cx * y[3]) * sc);
+        } else if (plain) {
+            const float2 up1 = fmul(0.5f, fadd(u, un)), up3 = fmul(0.5f, fadd(upv, u));
+            const float2 dxx1 = fmul(0.5f, fsub(fsub(fadd(ex, xz), x), xq3));
+            const float2 dxx2 = fmul(0.5f, fsub(fsub(fadd(xz, xq3), x), ex));
+            const float dx1 = flen(dxx1), dx2 = flen(dxx2);
+            const float test1 = fabsf(fdot(dxx1, uav) * dx2);
+            const float test2 = fabsf(fdot(dxx2, uav) * dx1);
+            const float rr = (test1 > test2) ? dx1 / dx2 : dx2 / dx1;
+            const float evol = fminf(sqrtf(4.f * cvolume * rr), 2.f * minelen);
+            const float du = sqrtf(fmaxf(flen2(fsub(fsub(fadd(up1, uz), u), up3)),
+                                         flen2(fsub(fsub(fadd(uz, up3), u), up1))));
+            const float ztmp2 = qa * du;
+            const float ztmp1 = qb * css;
+            const float crmu = (ztmp2 + sqrtf(ztmp2 * ztmp2 + ztmp1 * ztmp1)) * rho * evol;
+            q1 = fmul(crmu * rinv_de1, fsub(u, upv));
+            q2 = fmul(crmu * rinv_el, fsub(un, u));
+        }
+        const float ssin = 4.f * fcross(v1, v2) / (de1 * de2);
+        const float csin2 = (minelen < 1.e-12f) ? 1.f : ssin * ssin;
+        const float cw = (csin2 < 1.e-4f) ? 0.f : cvolume / csin2;
+        ccos = (csin2 < 1.e-4f) ? 0.f : ccos;
         const int n = hdr.y;
         const int lp = g + (k == 0 ? n - 1 : k - 1);
         const int ln = g + (k + 1 >= n ? 0 : k + 1);
-        const float rinv_prev = shflf(rinv, lp);
-        const float2 d1 = fmul(cw * rinv, fadd(q2, fmul(ccos, q1)));
-        const float2 d2 = fmul(cw * rinv_prev, fadd(q1, fmul(ccos, q2)));
+        const float2 d1 = fmul(cw * rinv_el, fadd(q2, fmul(ccos, q1)));
+        const float2 d2 = fmul(cw * rinv_de1, fadd(q1, fmul(ccos, q2)));
         const float2 d1p = shflf2(d1, lp);
         const float2 d2n = shflf2(d2, ln);
         if (zok && k < n) {
@@ -527,7 +585,11 @@ __global__ void __launch_bounds__(kMlpRows, 3) closure_pass(DevArrays a) {
         }
     }
     const bool ok = closure_mlp_teardown(st);
-    if (!ok && threadIdx.x == 0) atomicAdd(a.closure_counts + kClassErr * 64, 1ull);
+    if (threadIdx.x == 0 && !ok) atomicAdd(a.closure_counts + kClassErr * 64, 1ull);
+    if (threadIdx.x < 3 && ccount[threadIdx.x]) {
+        const int q = threadIdx.x == 0 ? kClassMlp : (threadIdx.x == 1 ? kClassFallback : kClassOod);
+        atomicAdd(a.closure_counts + q * 64 + (blockIdx.x & 63), (unsigned long long)ccount[threadIdx.x]);
+    }
 }
 
 // ---------------------------------------------------------------------
@@ -619,7 +681,7 @@ cudaError_t launch_cycle_mixed_impl(const DevArrays& a, const HydroConst& c, cud
         if (a.quads) pass_a_mixed<true, true><<<zb, kZoneThreads, 0, stream>>>(a, c);
         else pass_a_mixed<false, true><<<zb, kZoneThreads, 0, stream>>>(a, c);
         if (ev) cudaEventRecord(ev[1], stream);
-        closure_pass<<<a.closure_grid, kMlpRows, kMlpSmemBytes, stream>>>(a);
+        closure_pass<<<a.closure_grid, kMlpRows, kMlpSmemBytes, stream>>>(a, c);
     } else {
         if (a.quads) pass_a_mixed<true, false><<<zb, kZoneThreads, 0, stream>>>(a, c);
         else pass_a_mixed<false, false><<<zb, kZoneThreads, 0, stream>>>(a, c);
