@@ -15,20 +15,22 @@
 //   finalize  calcDt, checkBadSides, time/cycle update and the next
 //           cycle's calcGlobalDt (Driver.cc:213-245), all on the device
 //
-// Zone passes map four lanes to a zone (one lane per side/corner, zones
-// with 3 sides leave one lane idle).  Zone-local side data moves between
-// lanes with warp shuffles; zone sums are formed by every lane in the
-// reference's serial side order.  Quotients the reference forms once per
-// zone are split over the zone's lanes, one division each, and shared;
-// 1/elen is formed once per side and shared with the neighbouring corner;
-// QCS terms the reference computes and then discards (evol and du unless
-// cdiv < 0, zkur when cdiv > 0) are not computed, which leaves every stored
-// value unchanged.  Pass A is capped at 64 registers (4 blocks per SM): it
-// is latency bound and gains more from the extra warps than it loses to
-// the few spilled registers.  The arithmetic lives in hydro_fp64_body.cuh
-// (shared with the batched kernels); this file is compiled with
-// -fmad=false, so the results match a serial CPU run of the reference bit
-// for bit.
+// Pass A runs one thread per zone (pass_a_zone_thread): the zone's sides
+// in the reference's side order, each zone-level quantity (centre, sums,
+// EOS) formed once, 4-way independent corner work for latency hiding, no
+// shuffles; 168 registers, 3 blocks of 128 per SM (13% faster than the
+// four-lanes-per-zone form pass_a_zone at a developed 1024^2 Sedov state;
+// it is bound by the ~50 correctly rounded FP64 divisions and square roots
+// of a zone).  Pass C and the batched kernels keep four lanes per zone: one
+// lane per side/corner, zone-local side data moved by warp shuffles, zone
+// sums formed by every lane in the serial side order, zone quotients split
+// over the lanes.  1/elen is formed
+// once per side and shared with the neighbouring corner; QCS terms the
+// reference computes and then discards (evol and du unless cdiv < 0, zkur
+// when cdiv > 0) are not computed, which leaves every stored value
+// unchanged.  The arithmetic lives in hydro_fp64_body.cuh (shared with the
+// batched kernels); this file is compiled with -fmad=false, so the results
+// match a serial CPU run of the reference bit for bit.
 #include "hydro_fp64_body.cuh"
 
 namespace pnt {
@@ -36,23 +38,33 @@ namespace {
 
 using namespace fp64;
 
-#ifndef PNT_PASS_A_MIN_BLOCKS
-#define PNT_PASS_A_MIN_BLOCKS 4
+#ifndef PNT_PASS_A_ZT_MIN_BLOCKS
+#define PNT_PASS_A_ZT_MIN_BLOCKS 3
 #endif
+constexpr int kZoneThreadsZT = 128;   // one zone per thread
 
 template <bool kQuads>
-__global__ void __launch_bounds__(kZoneThreads, PNT_PASS_A_MIN_BLOCKS) pass_a(DevArrays a, HydroConst c) {
+__global__ void __launch_bounds__(kZoneThreadsZT, PNT_PASS_A_ZT_MIN_BLOCKS) pass_a_zt(DevArrays a, HydroConst c) {
     const Ctl* ctl = a.ctl;
     if (skip_cycle(ctl)) return;
-    const int64_t tid = (int64_t)blockIdx.x * kZoneThreads + threadIdx.x;
-    const int64_t z = tid >> 2;
-    double zdthyd;
-    bool bad;
-    pass_a_zone<kQuads>(a, c, ctl->cycle & 1, ctl->dt, z, (int)(tid & 3), threadIdx.x & 31, z < a.numz, zdthyd,
-                        bad);
+    const int64_t z = (int64_t)blockIdx.x * kZoneThreadsZT + threadIdx.x;
+    double zdthyd = 1.e99;
+    bool bad = false;
+    if (z < a.numz) {
+        const int cur = ctl->cycle & 1;
+        const double dt = ctl->dt;
+        if (kQuads) {
+            pass_a_zone_thread<4>(a, c, cur, dt, z, 4 * z, zdthyd, bad);
+        } else {
+            const int n = a.znump[z];
+            const int64_t s0 = a.zfirst[z];
+            if (n == 4) pass_a_zone_thread<4>(a, c, cur, dt, z, s0, zdthyd, bad);
+            else pass_a_zone_thread<3>(a, c, cur, dt, z, s0, zdthyd, bad);
+        }
+    }
     const int nbad = __syncthreads_count(bad);
     if (blockIdx.x >= (unsigned)a.npartA) return;   // partials are sized for this grid
-    block_fold<true, kZoneThreads>(zdthyd, a.part_dtnew + blockIdx.x);
+    block_fold<true, kZoneThreadsZT>(zdthyd, a.part_dtnew + blockIdx.x);
     if (threadIdx.x == 0) a.part_badA[blockIdx.x] = nbad;
 }
 
@@ -127,8 +139,9 @@ cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStrea
     const int zbc = (int)zone_blocks(a.numz, kZoneThreadsC);
     const int pb = (int)((a.nump + kPointThreads - 1) / kPointThreads);
     if (ev) cudaEventRecord(ev[0], stream);
-    if (a.quads) pass_a<true><<<zb, kZoneThreads, 0, stream>>>(a, c);
-    else pass_a<false><<<zb, kZoneThreads, 0, stream>>>(a, c);
+    const int zba = (int)((a.numz + kZoneThreadsZT - 1) / kZoneThreadsZT);
+    if (a.quads) pass_a_zt<true><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
+    else pass_a_zt<false><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
     if (ev) cudaEventRecord(ev[1], stream);
     if (ev) cudaEventRecord(ev[2], stream);   // no closure pass
     pass_b<<<pb, kPointThreads, 0, stream>>>(a, c);
@@ -136,7 +149,7 @@ cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStrea
     if (a.quads) pass_c<true><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
     else pass_c<false><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
     if (ev) cudaEventRecord(ev[4], stream);
-    finalize<<<1, kFinThreads, 0, stream>>>(a, c, zb, zbc);
+    finalize<<<1, kFinThreads, 0, stream>>>(a, c, zba, zbc);
     if (ev) cudaEventRecord(ev[5], stream);
     return cudaGetLastError();
 }

@@ -289,6 +289,185 @@ __device__ __forceinline__ void pass_a_zone(const DevArrays& a, const HydroConst
 }
 
 // ---------------------------------------------------------------------
+// Pass A, one thread per zone of N sides (N = 3 or 4, static so the side
+// arrays stay in registers): the arithmetic of pass_a_zone, side by side in
+// the zone's side order, so zone sums keep the reference's serial order and
+// every zone-level quantity is formed once.
+// ---------------------------------------------------------------------
+template <int N>
+__device__ __forceinline__ void pass_a_zone_thread(const DevArrays& a, const HydroConst& c, int cur, double dt,
+                                                   int64_t z, int64_t s0, double& zdthyd, bool& bad) {
+    const double2* __restrict__ px0 = a.px[cur];
+    const double2* __restrict__ pu0 = a.pu[cur];
+    double2 xp[N], u0[N];
+    double mf[N];
+    const double dth = 0.5 * dt;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const int32_t p = __ldg(a.mapsp1 + s0 + k);
+        const double2 x0 = px0[p];
+        u0[k] = pu0[p];
+        mf[k] = __ldg(a.smf + s0 + k);
+        xp[k] = add(x0, smul(dth, u0[k]));   // advPosHalf (Hydro.cc:986-1006)
+    }
+    const double zm = a.zm[z], zr = a.zr[z], ze = a.ze[z], zwrate = a.zwrate[z], zvol0 = a.zvol[z];
+    const double rn = 1. / (double)N;
+    // calcCtrs (Mesh.cc:797-837)
+    double zx = __dadd_rn(0.0, xp[0].x * rn), zy = __dadd_rn(0.0, xp[0].y * rn);
+#pragma unroll
+    for (int k = 1; k < N; ++k) {
+        zx = zx + xp[k].x * rn;
+        zy = zy + xp[k].y * rn;
+    }
+    const double2 zxp = mk(zx, zy);
+    // calcVols (Mesh.cc:928-989), calcEdgeLen (:1151-1179), calcCharLen (:1216-1244)
+    const double third = 1. / 3.;
+    const double fac = (N == 3 ? 3. : 4.);
+    double sa[N], elen[N], rinv[N];
+    double zareap = 0., zvolp = 0., zdl = 1.e99;
+    bad = false;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const int nk = (k + 1 == N) ? 0 : k + 1;
+        sa[k] = 0.5 * cross(sub(xp[nk], xp[k]), sub(zxp, xp[k]));
+        const double sv = third * sa[k] * (xp[k].x + xp[nk].x + zxp.x);
+        zareap = (k == 0) ? __dadd_rn(0.0, sa[k]) : zareap + sa[k];
+        zvolp = (k == 0) ? __dadd_rn(0.0, sv) : zvolp + sv;
+        bad = bad || (sv <= 0.);
+        elen[k] = length(sub(xp[nk], xp[k]));
+        rinv[k] = 1. / elen[k];
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) zdl = dmin(zdl, fac * sa[k] / elen[k]);
+    // PolyGas::calcStateHalf (PolyGas.cc:63-109) with calcRho
+    const double e = dmax(ze, 0.);
+    const double p = c.gm1 * zr * e;
+    const double pre = c.gm1 * e;
+    const double per = c.gm1 * zr;
+    const double q = (per * p) / (zr * zr);
+    const double minv = 1. / zm;
+    const double csqd = dmax(c.ssmin2, pre + q);
+    const double zss = sqrt(csqd);
+    const double dv = (zvolp - zvol0) * minv;
+    const double bulk = zr * csqd;
+    const double denom = 1. + 0.5 * per * dv;
+    const double src = zwrate * dth * minv;
+    const double zrp = zm / zvolp;
+    const double zp = p + (per * src - zr * bulk * dv) / denom;
+    a.zp[z] = zp;
+    // calcCrnrMass (Hydro.cc:1083-1117)
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const int pk = (k == 0) ? N - 1 : k - 1;
+        a.cmass[s0 + k] = zrp * zareap * 0.5 * (mf[k] + mf[pk]);
+    }
+    // QCS::setCornerDiv / setQCnForce (QCS.cc:116-327), corner k at point k
+    double zux = __dadd_rn(0.0, u0[0].x * rn), zuy = __dadd_rn(0.0, u0[0].y * rn);
+#pragma unroll
+    for (int k = 1; k < N; ++k) {
+        zux = zux + u0[k].x * rn;
+        zuy = zuy + u0[k].y * rn;
+    }
+    const double2 zuc = mk(zux, zuy);
+    double2 ex[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) ex[k] = smul(0.5, add(xp[k], xp[(k + 1 == N) ? 0 : k + 1]));
+    double cw[N], cc[N];
+    double2 cqe1[N], cqe2[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const int pk = (k == 0) ? N - 1 : k - 1;
+        const int nk = (k + 1 == N) ? 0 : k + 1;
+        const double2 up0 = u0[k], xq0 = xp[k];
+        const double2 upp = u0[pk];
+        const double2 up1 = smul(0.5, add(up0, u0[nk]));
+        const double2 xq1 = ex[k];
+        const double2 up2 = zuc, xq2 = zxp;
+        const double2 up3 = smul(0.5, add(upp, up0));
+        const double2 xq3 = ex[pk];
+        const double cvolume = 0.5 * cross(sub(xq2, xq0), sub(xq3, xq1));
+        const double2 v1 = sub(xq3, xq0);
+        const double2 v2 = sub(xq1, xq0);
+        const double de1 = elen[pk], de2 = elen[k];
+        const double minelen = dmin(de1, de2);
+        double ccos = ((minelen < 1.e-12) ? 0. : 4. * dot(v1, v2) / (de1 * de2));
+        const double cdiv = (cross(sub(up2, up0), sub(xq3, xq1)) - cross(sub(up3, up1), sub(xq2, xq0))) /
+                            (2.0 * cvolume);
+        double evol = 0., du = 0.;
+        if (cdiv < 0.0) {
+            const double2 dxx1 = smul(0.5, sub(sub(add(xq1, xq2), xq0), xq3));
+            const double2 dxx2 = smul(0.5, sub(sub(add(xq2, xq3), xq0), xq1));
+            const double dx1 = length(dxx1);
+            const double dx2 = length(dxx2);
+            const double2 duav = smul(0.25, add(add(add(up0, up1), up2), up3));
+            const double test1 = fabs(dot(dxx1, duav) * dx2);
+            const double test2 = fabs(dot(dxx2, duav) * dx1);
+            const double num = (test1 > test2 ? dx1 : dx2);
+            const double den = (test1 > test2 ? dx2 : dx1);
+            const double r = num / den;
+            evol = sqrt(4.0 * cvolume * r);
+            evol = dmin(evol, 2.0 * minelen);
+            const double dv1 = length2(sub(sub(add(up1, up2), up0), up3));
+            const double dv2 = length2(sub(sub(add(up2, up3), up0), up1));
+            du = sqrt(dmax(dv1, dv2));
+        }
+        double crmu = 0.;
+        if (!(cdiv > 0.0)) {
+            const double ztmp2 = c.q2 * 0.25 * c.gammap1 * du;
+            const double ztmp1 = c.q1 * zss;
+            const double zkur = ztmp2 + sqrt(ztmp2 * ztmp2 + ztmp1 * ztmp1);
+            crmu = zkur * zrp * evol;
+        }
+        const double2 t1 = smul(crmu, sub(up0, upp));
+        cqe1[k] = mk(t1.x * rinv[pk], t1.y * rinv[pk]);   // / elen[s]
+        const double2 t2 = smul(crmu, sub(u0[nk], up0));
+        cqe2[k] = mk(t2.x * rinv[k], t2.y * rinv[k]);     // / elen[s2]
+        // QCS::setForce (QCS.cc:331-380) corner weights
+        const double csin2 = 1.0 - ccos * ccos;
+        cw[k] = ((csin2 < 1.e-4) ? 0. : cvolume / csin2);
+        cc[k] = ((csin2 < 1.e-4) ? 0. : ccos);
+    }
+    // side forces: PolyGas::calcForce (PolyGas.cc:164-184), TTS::calcForce
+    // (TTS.cc:55-104), QCS sfq, and the side part of sumCrnrForce
+    // (Hydro.cc:1159-1193)
+    double sstmp = dmax(zss, c.tts_ssmin);
+    sstmp = c.alfa * sstmp * sstmp;
+    double2 ftot[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const int nk = (k + 1 == N) ? 0 : k + 1;
+        const double2 ssurf = rotateCCW(sub(ex[k], zxp));
+        const double2 sfp = smul(-zp, ssurf);
+        const double vfacinv = zareap / sa[k];
+        const double srho = zrp * mf[k] * vfacinv;
+        const double sdp = sstmp * (srho - zrp);
+        const double2 sft = smul(-sdp, ssurf);
+        const double2 fs = add(smul(cw[k], add(cqe2[k], smul(cc[k], cqe1[k]))),
+                               smul(cw[nk], add(cqe1[nk], smul(cc[nk], cqe2[nk]))));
+        const double2 sfq = mk(fs.x * rinv[k], fs.y * rinv[k]);
+        const double2 sfpq = add(sfp, sfq);
+        ftot[k] = add(sfpq, sft);
+        a.sftot[s0 + k] = sfpq;
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) a.cforce[s0 + k] = sub(ftot[k], ftot[(k == 0) ? N - 1 : k - 1]);
+    // QCS::setVelDiff (QCS.cc:384-448) and calcDtNew (Hydro.cc:1591-1619)
+    double ztmp = 0.;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const int nk = (k + 1 == N) ? 0 : k + 1;
+        const double2 dxs = sub(xp[nk], xp[k]);
+        const double2 dus = sub(u0[nk], u0[k]);
+        double dux = dot(dus, dxs);
+        dux = (elen[k] > 0. ? fabs(dux) / elen[k] : 0.);
+        ztmp = dmax(ztmp, dux);
+    }
+    const double zdu = c.q1 * zss + 2. * c.q2 * ztmp;
+    const double cdu = dmax(zdu, dmax(zss, 1.e-99));
+    zdthyd = zdl * c.cfl / cdu;
+}
+
+// ---------------------------------------------------------------------
 // Pass B, one point
 // ---------------------------------------------------------------------
 __device__ __forceinline__ void pass_b_point(const DevArrays& a, const HydroConst& c, int cur, double dt,

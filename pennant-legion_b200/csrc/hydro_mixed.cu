@@ -20,8 +20,13 @@
 // The pressure force sfp is formed in FP64 (its surface vectors cancel
 // around each zone, and calcWork needs that cancellation), and sfp + sfq is
 // handed to calcWork in FP64; the corner mass and corner force handed to the
-// point pass are stored in FP32 (4 + 8 B per side instead of 24 B).  Compiled with fast math; the accuracy of this path is stated as
-// its L1 error against the FP64 run (tests/test_gpu_mixed.py).
+// point pass are stored in FP32 (4 + 8 B per side instead of 24 B).  Pass A
+// runs one thread per zone (128 registers, 4 blocks of 128 per SM): with the
+// divisions and square roots in FP32 it is 40% faster than four lanes per
+// zone.  The learned cycle (precision learned) is this cycle with the QCS
+// corner forces of compressing corners moved to the closure pass.
+// Compiled with fast math; the accuracy of this path is stated as its L1
+// error against the FP64 run (tests/test_gpu_mixed.py).
 #include "closure_dev.cuh"
 #include "hydro_dev.h"
 
@@ -96,312 +101,366 @@ __device__ __forceinline__ void block_fold(double v, double* out) {
     }
 }
 
+// ---------------------------------------------------------------------
+// Pass A, mixed precision, one thread per zone of N sides (N = 3 or 4): the
+// arithmetic of pass_a_mixed side by side in the zone's side order.
+// ---------------------------------------------------------------------
 // QCS side force of one zone in FP64 (QCS.cc:116-380), for zones with an
 // acute corner: there sfq is a small difference of large terms (cw grows as
-// 1/sin^2 of the corner angle) that FP32 cannot carry.  All lanes of the
-// warp must call it (it shuffles).
-__device__ double2 qcs_sfq_fp64(double2 xp, double2 xp2, double2 zxp, double2 u0, double rn, int g, int n,
-                                int lp, int ln, double zss, double zrp, const HydroConst& c) {
-    const double2 u02 = shfl2(u0, ln), upp = shfl2(u0, lp);
-    const double2 zuc = mk(zsum4(u0.x * rn, g, n), zsum4(u0.y * rn, g, n));
-    const double2 ex = smul(0.5, add(xp, xp2));
-    const double2 xq3 = shfl2(ex, lp);
-    const double2 d = sub(xp2, xp);
-    const double elen = sqrt(dot(d, d));
-    const double de1 = shfl(elen, lp), de2 = elen;
-    const double2 up0 = u0, xq0 = xp, xq1 = ex, up2 = zuc, xq2 = zxp;
-    const double2 up1 = smul(0.5, add(up0, u02));
-    const double2 up3 = smul(0.5, add(upp, up0));
-    const double cvolume = 0.5 * cross(sub(xq2, xq0), sub(xq3, xq1));
-    const double2 v1 = sub(xq3, xq0), v2 = sub(xq1, xq0);
-    const double minelen = dmin(de1, de2);
-    double ccos = (minelen < 1.e-12) ? 0. : 4. * dot(v1, v2) / (de1 * de2);
-    const double cdiv = (cross(sub(up2, up0), sub(xq3, xq1)) - cross(sub(up3, up1), sub(xq2, xq0))) /
-                        (2.0 * cvolume);
-    double crmu = 0.;
-    if (cdiv < 0.0) {
-        const double2 dxx1 = smul(0.5, sub(sub(add(xq1, xq2), xq0), xq3));
-        const double2 dxx2 = smul(0.5, sub(sub(add(xq2, xq3), xq0), xq1));
-        const double dx1 = sqrt(dot(dxx1, dxx1)), dx2 = sqrt(dot(dxx2, dxx2));
-        const double2 duav = smul(0.25, add(add(add(up0, up1), up2), up3));
-        const double test1 = fabs(dot(dxx1, duav) * dx2);
-        const double test2 = fabs(dot(dxx2, duav) * dx1);
-        const double rr = (test1 > test2) ? dx1 / dx2 : dx2 / dx1;
-        const double evol = dmin(sqrt(4.0 * cvolume * rr), 2.0 * minelen);
-        const double2 w1 = sub(sub(add(up1, up2), up0), up3), w2 = sub(sub(add(up2, up3), up0), up1);
-        const double du = sqrt(dmax(dot(w1, w1), dot(w2, w2)));
-        const double ztmp2 = c.q2 * 0.25 * c.gammap1 * du;
-        const double ztmp1 = c.q1 * zss;
-        crmu = (ztmp2 + sqrt(ztmp2 * ztmp2 + ztmp1 * ztmp1)) * zrp * evol;
+// 1/sin^2 of the corner angle) that FP32 cannot carry.
+template <int N>
+__device__ __forceinline__ void qcs_sfq_fp64_zone(const DevArrays& a, const HydroConst& c, int cur, int64_t s0,
+                                                  const double2* xp, double2 zxp, double zss, double zrp,
+                                                  double2* sfq) {
+    double2 u0[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) u0[k] = a.pu[cur][__ldg(a.mapsp1 + s0 + k)];
+    const double rn = 1. / (double)N;
+    double zx = u0[0].x * rn, zy = u0[0].y * rn;
+#pragma unroll
+    for (int k = 1; k < N; ++k) {
+        zx += u0[k].x * rn;
+        zy += u0[k].y * rn;
     }
-    const double2 cqe1 = smul(crmu / de1, sub(up0, upp));
-    const double2 cqe2 = smul(crmu / de2, sub(u02, up0));
-    const double csin2 = 1.0 - ccos * ccos;
-    const double cw = (csin2 < 1.e-4) ? 0. : cvolume / csin2;
-    ccos = (csin2 < 1.e-4) ? 0. : ccos;
-    const double cw2 = shfl(cw, ln), ccos2 = shfl(ccos, ln);
-    const double2 cqe12 = shfl2(cqe1, ln), cqe22 = shfl2(cqe2, ln);
-    return smul(1. / elen, add(smul(cw, add(cqe2, smul(ccos, cqe1))), smul(cw2, add(cqe12, smul(ccos2, cqe22)))));
+    const double2 zuc = mk(zx, zy);
+    double2 ex[N], cqe1[N], cqe2[N];
+    double elen[N], cw[N], cc[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const int nk = (k + 1 == N) ? 0 : k + 1;
+        ex[k] = smul(0.5, add(xp[k], xp[nk]));
+        const double2 d = sub(xp[nk], xp[k]);
+        elen[k] = sqrt(dot(d, d));
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const int pk = (k == 0) ? N - 1 : k - 1;
+        const int nk = (k + 1 == N) ? 0 : k + 1;
+        const double2 up0 = u0[k], xq0 = xp[k], xq1 = ex[k], up2 = zuc, xq2 = zxp, upp = u0[pk], xq3 = ex[pk];
+        const double2 up1 = smul(0.5, add(up0, u0[nk]));
+        const double2 up3 = smul(0.5, add(upp, up0));
+        const double de1 = elen[pk], de2 = elen[k];
+        const double cvolume = 0.5 * cross(sub(xq2, xq0), sub(xq3, xq1));
+        const double2 v1 = sub(xq3, xq0), v2 = sub(xq1, xq0);
+        const double minelen = dmin(de1, de2);
+        double ccos = (minelen < 1.e-12) ? 0. : 4. * dot(v1, v2) / (de1 * de2);
+        const double cdiv = (cross(sub(up2, up0), sub(xq3, xq1)) - cross(sub(up3, up1), sub(xq2, xq0))) /
+                            (2.0 * cvolume);
+        double crmu = 0.;
+        if (cdiv < 0.0) {
+            const double2 dxx1 = smul(0.5, sub(sub(add(xq1, xq2), xq0), xq3));
+            const double2 dxx2 = smul(0.5, sub(sub(add(xq2, xq3), xq0), xq1));
+            const double dx1 = sqrt(dot(dxx1, dxx1)), dx2 = sqrt(dot(dxx2, dxx2));
+            const double2 duav = smul(0.25, add(add(add(up0, up1), up2), up3));
+            const double test1 = fabs(dot(dxx1, duav) * dx2);
+            const double test2 = fabs(dot(dxx2, duav) * dx1);
+            const double rr = (test1 > test2) ? dx1 / dx2 : dx2 / dx1;
+            const double evol = dmin(sqrt(4.0 * cvolume * rr), 2.0 * minelen);
+            const double2 w1 = sub(sub(add(up1, up2), up0), up3), w2 = sub(sub(add(up2, up3), up0), up1);
+            const double du = sqrt(dmax(dot(w1, w1), dot(w2, w2)));
+            const double ztmp2 = c.q2 * 0.25 * c.gammap1 * du;
+            const double ztmp1 = c.q1 * zss;
+            crmu = (ztmp2 + sqrt(ztmp2 * ztmp2 + ztmp1 * ztmp1)) * zrp * evol;
+        }
+        cqe1[k] = smul(crmu / de1, sub(up0, upp));
+        cqe2[k] = smul(crmu / de2, sub(u0[nk], up0));
+        const double csin2 = 1.0 - ccos * ccos;
+        cw[k] = (csin2 < 1.e-4) ? 0. : cvolume / csin2;
+        cc[k] = (csin2 < 1.e-4) ? 0. : ccos;
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const int nk = (k + 1 == N) ? 0 : k + 1;
+        sfq[k] = smul(1. / elen[k], add(smul(cw[k], add(cqe2[k], smul(cc[k], cqe1[k]))),
+                                        smul(cw[nk], add(cqe1[nk], smul(cc[nk], cqe2[nk])))));
+    }
 }
 
-// ---------------------------------------------------------------------
-// Pass A, mixed precision
-// ---------------------------------------------------------------------
-#ifndef PNT_LEARNED_A_MIN_BLOCKS
-#define PNT_LEARNED_A_MIN_BLOCKS 4
-#endif
-#ifndef PNT_MIXED_A_MIN_BLOCKS
-#define PNT_MIXED_A_MIN_BLOCKS 4
-#endif
-template <bool kQuads, bool kLearned>
-__global__ void __launch_bounds__(kZoneThreads, kLearned ? PNT_LEARNED_A_MIN_BLOCKS : PNT_MIXED_A_MIN_BLOCKS)
-    pass_a_mixed(DevArrays a, HydroConst c) {
-    const Ctl* ctl = a.ctl;
-    if (skip_cycle(ctl)) return;
-    const int cur = ctl->cycle & 1;
-    const double dt = ctl->dt;
+// cnt[3]: this zone's corners without compression, in the dead zone, in an
+// acute zone (learned cycle).
+template <int N, bool kLearned>
+__device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const HydroConst& c, int cur, double dt,
+                                                  int64_t z, int64_t s0, double& zdthyd, bool& bad, int* cnt) {
     const double2* __restrict__ px0 = a.px[cur];
     const double2* __restrict__ pu0 = a.pu[cur];
-
-    const int64_t tid = (int64_t)blockIdx.x * kZoneThreads + threadIdx.x;
-    const int64_t z = tid >> 2;
-    const int k = (int)(tid & 3);
-    const int lane = threadIdx.x & 31;
-    const int g = lane & ~3;
-    const bool zok = z < a.numz;
-    int n = 4;
-    int64_t s = 4 * z + k;
-    if (!kQuads) {
-        n = zok ? a.znump[z] : 4;
-        s = (zok ? (int64_t)a.zfirst[z] : 0) + k;
-    }
-    const bool act = zok && k < n;
-    const int lp = g + (k == 0 ? n - 1 : k - 1);
-    const int ln = g + (k + 1 >= n ? 0 : k + 1);
-
-    const int32_t p1 = act ? __ldg(a.mapsp1 + s) : 0;
-    const double2 x0 = act ? px0[p1] : mk(0., 0.);
-    const double2 u0 = act ? pu0[p1] : mk(0., 0.);
-    const double mf = act ? __ldg(a.smf + s) : 0.;
-    const double zm = zok ? a.zm[z] : 1.;
-    const double zr = zok ? a.zr[z] : 1.;
-    const double ze = zok ? a.ze[z] : 0.;
-    const double zwrate = zok ? a.zwrate[z] : 0.;
-    const double zvol0 = zok ? a.zvol[z] : 1.;
-
-    // FP64: positions, zone centre, side areas and volumes
+    double2 xp[N];
+    float2 uf[N];
+    double mf[N];
     const double dth = 0.5 * dt;
-    const double2 xp = add(x0, smul(dth, u0));
-    const double2 xp2 = shfl2(xp, ln);
-    const double rn = 1. / (double)n;
-    const double2 zxp = mk(zsum4(xp.x * rn, g, n), zsum4(xp.y * rn, g, n));
+    double2 uref;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const int32_t p = __ldg(a.mapsp1 + s0 + k);
+        const double2 u0 = pu0[p];
+        xp[k] = add(px0[p], smul(dth, u0));
+        if (k == 0) uref = u0;
+        // velocities relative to the zone's first point: QCS works on
+        // velocity differences, which absolute FP32 values would round away
+        uf[k] = f2(sub(u0, uref));
+        mf[k] = __ldg(a.smf + s0 + k);
+    }
+    const double zm = a.zm[z], zr = a.zr[z], ze = a.ze[z], zwrate = a.zwrate[z], zvol0 = a.zvol[z];
+    // FP64: positions, zone centre, side areas and volumes
+    const double rn = 1. / (double)N;
+    double zx = xp[0].x * rn, zy = xp[0].y * rn;
+#pragma unroll
+    for (int k = 1; k < N; ++k) {
+        zx += xp[k].x * rn;
+        zy += xp[k].y * rn;
+    }
+    const double2 zxp = mk(zx, zy);
     const double third = 1. / 3.;
-    const double sa = 0.5 * cross(sub(xp2, xp), sub(zxp, xp));
-    const double sv = third * sa * (xp.x + xp2.x + zxp.x);
-    const double zareap = zsum4(sa, g, n);
-    const double zvolp = zsum4(sv, g, n);
-    const bool bad = act && (sv <= 0.);
-
-    // FP64 zone EOS and density (PolyGas.cc:63-109, Hydro.cc:1034-1054),
-    // quotients split over the zone's lanes
+    double sa[N];
+    double zareap = 0., zvolp = 0.;
+    bad = false;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const int nk = (k + 1 == N) ? 0 : k + 1;
+        sa[k] = 0.5 * cross(sub(xp[nk], xp[k]), sub(zxp, xp[k]));
+        const double sv = third * sa[k] * (xp[k].x + xp[nk].x + zxp.x);
+        zareap = (k == 0) ? sa[k] : zareap + sa[k];
+        zvolp = (k == 0) ? sv : zvolp + sv;
+        bad = bad || (sv <= 0.);
+    }
+    // FP64 zone EOS and density (PolyGas.cc:63-109, Hydro.cc:1034-1054)
     const double e = dmax(ze, 0.);
     const double p = c.gm1 * zr * e;
     const double pre = c.gm1 * e;
     const double per = c.gm1 * zr;
-    const double rA = ((k == 0) ? per * p : 1.) / ((k == 0) ? zr * zr : zm);
-    const double q = shfl(rA, g);
-    const double minv = shfl(rA, g + 1);
+    const double q = (per * p) / (zr * zr);
+    const double minv = 1. / zm;
     const double csqd = dmax(c.ssmin2, pre + q);
     const double zss = sqrt(csqd);
     const double dv = (zvolp - zvol0) * minv;
     const double bulk = zr * csqd;
     const double denom = 1. + 0.5 * per * dv;
     const double src = zwrate * dth * minv;
-    const double rB = ((k == 0) ? zm : per * src - zr * bulk * dv) / ((k == 0) ? zvolp : denom);
-    const double zrp = shfl(rB, g);
-    const double zp = p + shfl(rB, g + 1);
-    const double mf3 = shfl(mf, lp);
-    if (act) a.cmass_f[s] = (float)(zrp * zareap * 0.5 * (mf + mf3));
-    if (zok && k == 0) a.zp[z] = zp;
+    const double zrp = zm / zvolp;
+    const double zp = p + (per * src - zr * bulk * dv) / denom;
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+        a.cmass_f[s0 + k] = (float)(zrp * zareap * 0.5 * (mf[k] + mf[(k == 0) ? N - 1 : k - 1]));
+    a.zp[z] = zp;
 
     // FP32 from here, relative to the zone's first point
-    const double2 xref = shfl2(xp, g);
-    const float2 r = f2(sub(xp, xref));
-    const float2 r2 = shflf2(r, ln);
-    const float2 zc = f2(sub(zxp, xref));
-    // velocities relative to the zone's first point as well: QCS works on
-    // velocity differences, which absolute FP32 values would round away
-    const double2 uref = shfl2(u0, g);
-    const float2 uf = f2(sub(u0, uref));
-    const float2 u2f = shflf2(uf, ln);
-    const float2 upf = shflf2(uf, lp);
+    float2 r[N], ex[N];
+    float elen[N], rinv[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) r[k] = f2(sub(xp[k], xp[0]));
+    const float2 zc = f2(sub(zxp, xp[0]));
     const float rnf = (float)rn;
-    const float2 zuc = fk(zsum4(uf.x * rnf, g, n), zsum4(uf.y * rnf, g, n));
-    const float2 ex = fmul(0.5f, fadd(r, r2));
-    const float2 ssurf = fk(-(ex.y - zc.y), ex.x - zc.x);
-    const float elen = flen(fsub(r2, r));
-    const float saf = (float)sa;
-    const float fac = (n == 3 ? 3.f : 4.f);
-    // zone minimum over the group's 4 lanes; the idle lane of a triangle
-    // contributes +inf
-    float zdl = act ? fac * saf / elen : __int_as_float(0x7f800000);
-    zdl = fminf(zdl, __shfl_xor_sync(kFull, zdl, 1));
-    zdl = fminf(zdl, __shfl_xor_sync(kFull, zdl, 2));
-    const float rinv_el = 1.f / elen;
-
+    float zux = uf[0].x * rnf, zuy = uf[0].y * rnf;
+#pragma unroll
+    for (int k = 1; k < N; ++k) {
+        zux += uf[k].x * rnf;
+        zuy += uf[k].y * rnf;
+    }
+    const float2 zuc = fk(zux, zuy);
+    const float fac = (N == 3 ? 3.f : 4.f);
+    float zdl = __int_as_float(0x7f800000);
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const int nk = (k + 1 == N) ? 0 : k + 1;
+        ex[k] = fmul(0.5f, fadd(r[k], r[nk]));
+        elen[k] = flen(fsub(r[nk], r[k]));
+        rinv[k] = 1.f / elen[k];
+        zdl = fminf(zdl, fac * (float)sa[k] / elen[k]);
+    }
     const float zssf = (float)zss, zrpf = (float)zrp;
-    // PolyGas::calcForce in FP64: the pressure forces of a zone cancel
-    // around its closed boundary, and calcWork takes the small residual of
-    // their work on moving points; FP32 surface vectors break that
-    // cancellation
-    const double2 ex64 = smul(0.5, add(xp, xp2));
-    const double2 sfp = smul(-zp, mk(-(ex64.y - zxp.y), ex64.x - zxp.x));
-    // TTS (TTS.cc:55-104)
-    const float srho = zrpf * (float)mf * ((float)zareap / saf);
-    float sstmp = fmaxf(zssf, (float)c.tts_ssmin);
-    sstmp = (float)c.alfa * sstmp * sstmp;
-    const float2 sft = fmul(-(sstmp * (srho - zrpf)), ssurf);
 
-    // QCS corner (QCS.cc:116-380), FP32
-    const float2 up0 = uf, xq0 = r;
-    const float2 up1 = fmul(0.5f, fadd(up0, u2f));
-    const float2 xq1 = ex;
-    const float2 up2 = zuc, xq2 = zc;
-    const float2 up3 = fmul(0.5f, fadd(upf, up0));
-    const float2 xq3 = shflf2(ex, lp);
-    const float cvolume = 0.5f * fcross(fsub(xq2, xq0), fsub(xq3, xq1));
-    const float2 v1 = fsub(xq3, xq0), v2 = fsub(xq1, xq0);
-    const float de1 = shflf(elen, lp), de2 = elen;
-    const float rinv_de1 = shflf(rinv_el, lp);
-    const float minelen = fminf(de1, de2);
-    float ccos = (minelen < 1.e-12f) ? 0.f : 4.f * fdot(v1, v2) / (de1 * de2);
-    const float cdiv = (fcross(fsub(up2, up0), fsub(xq3, xq1)) - fcross(fsub(up3, up1), fsub(xq2, xq0))) /
-                       (2.f * cvolume);
-    // sin^2 of the corner angle.  The reference forms 1 - ccos^2, which in
-    // FP32 loses the small sines of the acute corners of thin zones (3-degree
-    // corners at the centre of a pie mesh); v1 and v2 run to the edge
-    // midpoints, |v_i| = de_i / 2, so (4 cross / (de1 de2))^2 is the same
-    // quantity without the cancellation.  Zones with a corner under ~30
-    // degrees take the FP64 form (warp-uniform branch; never taken on
-    // rectangular meshes).  The learned cycle needs the flag before the
-    // corner forces, the plain one after them (fewer live registers).
-    float csin2 = 1.f;
-    int acute = 0;
-    auto corner_sin2 = [&]() {
+    // QCS corners (QCS.cc:116-380), FP32; sin^2 of the corner angle as
+    // (4 cross / (de1 de2))^2 (the reference's 1 - ccos^2 loses the small
+    // sines of acute corners in FP32); zones with a corner under ~30 degrees
+    // take the FP64 form below
+    float2 cqe1[N], cqe2[N];
+    float cw[N], cc[N];
+    bool acute = false;
+    bool defer_any = false;
+    uint32_t defer_bits = 0;
+    const float dead = kLearned ? __ldg(reinterpret_cast<const float*>(a.closure_img + kImgThr)) : 0.f;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const int pk = (k == 0) ? N - 1 : k - 1;
+        const int nk = (k + 1 == N) ? 0 : k + 1;
+        const float2 up0 = uf[k], xq0 = r[k];
+        const float2 up1 = fmul(0.5f, fadd(up0, uf[nk]));
+        const float2 xq1 = ex[k];
+        const float2 up2 = zuc, xq2 = zc;
+        const float2 up3 = fmul(0.5f, fadd(uf[pk], up0));
+        const float2 xq3 = ex[pk];
+        const float cvolume = 0.5f * fcross(fsub(xq2, xq0), fsub(xq3, xq1));
+        const float2 v1 = fsub(xq3, xq0), v2 = fsub(xq1, xq0);
+        const float de1 = elen[pk], de2 = elen[k];
+        const float minelen = fminf(de1, de2);
+        float ccos = (minelen < 1.e-12f) ? 0.f : 4.f * fdot(v1, v2) / (de1 * de2);
+        const float cdiv = (fcross(fsub(up2, up0), fsub(xq3, xq1)) - fcross(fsub(up3, up1), fsub(xq2, xq0))) /
+                           (2.f * cvolume);
         const float ssin = 4.f * fcross(v1, v2) / (de1 * de2);
-        csin2 = (minelen < 1.e-12f) ? 1.f : ssin * ssin;
-        acute = (act && csin2 < 0.25f) ? 1 : 0;
-        acute |= __shfl_xor_sync(kFull, acute, 1);
-        acute |= __shfl_xor_sync(kFull, acute, 2);
-    };
-    if constexpr (kLearned) corner_sin2();
-
-    // The learned cycle (closure_dev.cuh) forms no QCS corner force here:
-    // compressing corners outside the dead zone are deferred (their zones
-    // recorded with the corners' raw data) to the closure pass, which runs
-    // the network or, past its range, the plain QCS; the rest carry none.
-    // Zones with an acute corner keep the FP64 QCS below.
-    bool plain = cdiv < 0.f;
-    int cls = kClassZero;
+        const float csin2 = (minelen < 1.e-12f) ? 1.f : ssin * ssin;
+        acute = acute || (csin2 < 0.25f);
+        float crmu = 0.f;
+        if constexpr (kLearned) {
+            // learned cycle: no QCS force here; compressing corners past the
+            // dead zone are deferred to the closure pass
+            if (cdiv < 0.f) {
+                const float2 d1 = fsub(up0, uf[pk]), d2 = fsub(uf[nk], up0), dcz = fsub(zuc, up0);
+                const float m2 = fmaxf(fmaxf(flen2(d1), flen2(d2)), flen2(dcz));
+                const float lim = dead * zssf;
+                if (m2 > lim * lim) defer_bits |= 1u << k;
+                else ++cnt[1];
+            } else {
+                ++cnt[0];
+            }
+        } else if (cdiv < 0.f) {
+            const float2 dxx1 = fmul(0.5f, fsub(fsub(fadd(xq1, xq2), xq0), xq3));
+            const float2 dxx2 = fmul(0.5f, fsub(fsub(fadd(xq2, xq3), xq0), xq1));
+            const float dx1 = flen(dxx1), dx2 = flen(dxx2);
+            const float2 duav = fadd(fmul(0.25f, fadd(fadd(fadd(up0, up1), up2), up3)), f2(uref));
+            const float test1 = fabsf(fdot(dxx1, duav) * dx2);
+            const float test2 = fabsf(fdot(dxx2, duav) * dx1);
+            const float rr = (test1 > test2) ? dx1 / dx2 : dx2 / dx1;
+            const float evol = fminf(sqrtf(4.f * cvolume * rr), 2.f * minelen);
+            const float du = sqrtf(fmaxf(flen2(fsub(fsub(fadd(up1, up2), up0), up3)),
+                                         flen2(fsub(fsub(fadd(up2, up3), up0), up1))));
+            const float ztmp2 = (float)(c.q2 * 0.25 * c.gammap1) * du;
+            const float ztmp1 = (float)c.q1 * zssf;
+            crmu = (ztmp2 + sqrtf(ztmp2 * ztmp2 + ztmp1 * ztmp1)) * zrpf * evol;
+        }
+        cqe1[k] = fmul(crmu * rinv[pk], fsub(up0, uf[pk]));
+        cqe2[k] = fmul(crmu * rinv[k], fsub(uf[nk], up0));
+        cw[k] = (csin2 < 1.e-4f) ? 0.f : cvolume / csin2;
+        cc[k] = (csin2 < 1.e-4f) ? 0.f : ccos;
+    }
     if constexpr (kLearned) {
-        plain = false;
-        const float dead = __ldg(reinterpret_cast<const float*>(a.closure_img + kImgThr));
-        // dead-zone test on squares (closure_features' first step)
-        const float2 d1 = fsub(uf, upf), d2 = fsub(u2f, uf), dc = fsub(zuc, uf);
-        const float m2 = fmaxf(fmaxf(flen2(d1), flen2(d2)), flen2(dc));
-        const float lim = dead * zssf;
-        if (act && acute) cls = kClassAcute;
-        else if (act && cdiv < 0.f) cls = (m2 > lim * lim) ? kClassMlp : kClassDead;   // kClassMlp: deferred
-        const bool defer = cls == kClassMlp;
-        int zflag = defer ? 1 : 0;
-        zflag |= __shfl_xor_sync(kFull, zflag, 1);
-        zflag |= __shfl_xor_sync(kFull, zflag, 2);
-        const float2 xpp = shflf2(r, lp);
-        const unsigned zbits = __ballot_sync(kFull, zflag && k == 0);
-        int base = 0;
-        if (lane == 0 && zbits) base = atomicAdd(a.closure_nrec, __popc(zbits));
-        base = __shfl_sync(kFull, base, 0);
-        if (zflag) {
-            const int idx = base + __popc(zbits & ((1u << g) - 1u));
-            float4* rec = reinterpret_cast<float4*>(a.closure_rec + ((int64_t)idx * 4 + k) * kRecFloats);
-            const float2 uav = fadd(fmul(0.25f, fadd(fadd(fadd(up0, up1), up2), up3)), f2(uref));
-            rec[0] = make_float4(r.x, r.y, xpp.x, xpp.y);
-            rec[1] = make_float4(r2.x, r2.y, zc.x, zc.y);
-            rec[2] = make_float4(uf.x, uf.y, upf.x, upf.y);
-            rec[3] = make_float4(u2f.x, u2f.y, zuc.x, zuc.y);
-            rec[4] = make_float4(uav.x, uav.y, zssf, zrpf);
-            rec[5] = make_float4(defer ? 1.f : 0.f, 0.f, 0.f, 0.f);
-            if (k == 0) a.closure_zhdr[idx] = make_int2((int)(s - k), n);
+        if (acute) {   // the zone keeps the FP64 QCS: its corners are counted as acute
+            cnt[0] = cnt[1] = 0;
+            cnt[2] = N;
+            defer_bits = 0;
+        }
+        defer_any = defer_bits != 0;
+        // record the zone for the closure pass (warp-aggregated slot)
+        const unsigned am = __activemask();
+        const unsigned m = __ballot_sync(am, defer_any);
+        if (defer_any) {
+            const int lane = threadIdx.x & 31;
+            const int leader = __ffs(m) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(a.closure_nrec, __popc(m));
+            base = __shfl_sync(m, base, leader);
+            const int idx = base + __popc(m & ((1u << lane) - 1u));
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                const int pk = (k == 0) ? N - 1 : k - 1;
+                const int nk = (k + 1 == N) ? 0 : k + 1;
+                const float2 up1 = fmul(0.5f, fadd(uf[k], uf[nk]));
+                const float2 up3 = fmul(0.5f, fadd(uf[pk], uf[k]));
+                const float2 uav = fadd(fmul(0.25f, fadd(fadd(fadd(uf[k], up1), zuc), up3)), f2(uref));
+                float4* rec = reinterpret_cast<float4*>(a.closure_rec + ((int64_t)idx * 4 + k) * kRecFloats);
+                rec[0] = make_float4(r[k].x, r[k].y, r[pk].x, r[pk].y);
+                rec[1] = make_float4(r[nk].x, r[nk].y, zc.x, zc.y);
+                rec[2] = make_float4(uf[k].x, uf[k].y, uf[pk].x, uf[pk].y);
+                rec[3] = make_float4(uf[nk].x, uf[nk].y, zuc.x, zuc.y);
+                rec[4] = make_float4(uav.x, uav.y, zssf, zrpf);
+                rec[5] = make_float4((defer_bits >> k) & 1u ? 1.f : 0.f, 0.f, 0.f, 0.f);
+            }
+            if (N == 3) {   // the idle fourth row of a 3-sided zone
+                float4* rec = reinterpret_cast<float4*>(a.closure_rec + ((int64_t)idx * 4 + 3) * kRecFloats);
+                for (int i = 0; i < kRecFloats / 4; ++i) rec[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            a.closure_zhdr[idx] = make_int2((int)s0, N);
         }
     }
-    float crmu = 0.f;
-    if (plain) {
-        const float2 dxx1 = fmul(0.5f, fsub(fsub(fadd(xq1, xq2), xq0), xq3));
-        const float2 dxx2 = fmul(0.5f, fsub(fsub(fadd(xq2, xq3), xq0), xq1));
-        const float dx1 = flen(dxx1), dx2 = flen(dxx2);
-        const float2 duav = fadd(fmul(0.25f, fadd(fadd(fadd(up0, up1), up2), up3)), f2(uref));
-        const float test1 = fabsf(fdot(dxx1, duav) * dx2);
-        const float test2 = fabsf(fdot(dxx2, duav) * dx1);
-        const float rr = (test1 > test2) ? dx1 / dx2 : dx2 / dx1;
-        const float evol = fminf(sqrtf(4.f * cvolume * rr), 2.f * minelen);
-        const float du = sqrtf(fmaxf(flen2(fsub(fsub(fadd(up1, up2), up0), up3)),
-                                     flen2(fsub(fsub(fadd(up2, up3), up0), up1))));
-        const float ztmp2 = (float)(c.q2 * 0.25 * c.gammap1) * du;
-        const float ztmp1 = (float)c.q1 * zssf;
-        crmu = (ztmp2 + sqrtf(ztmp2 * ztmp2 + ztmp1 * ztmp1)) * zrpf * evol;
+    float2 sfq[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const int nk = (k + 1 == N) ? 0 : k + 1;
+        sfq[k] = fmul(rinv[k], fadd(fmul(cw[k], fadd(cqe2[k], fmul(cc[k], cqe1[k]))),
+                                    fmul(cw[nk], fadd(cqe1[nk], fmul(cc[nk], cqe2[nk])))));
     }
-    const float2 cqe1 = fmul(crmu * rinv_de1, fsub(up0, upf));
-    const float2 cqe2 = fmul(crmu * rinv_el, fsub(u2f, up0));
-    if constexpr (!kLearned) corner_sin2();
-    const float cw = (csin2 < 1.e-4f) ? 0.f : cvolume / csin2;
-    ccos = (csin2 < 1.e-4f) ? 0.f : ccos;
-    const float cw2 = shflf(cw, ln), ccos2 = shflf(ccos, ln);
-    const float2 cqe12 = shflf2(cqe1, ln), cqe22 = shflf2(cqe2, ln);
-    float2 sfq = fmul(rinv_el, fadd(fmul(cw, fadd(cqe2, fmul(ccos, cqe1))),
-                                    fmul(cw2, fadd(cqe12, fmul(ccos2, cqe22)))));
-    if (__any_sync(kFull, acute)) {
-        const double2 q = qcs_sfq_fp64(xp, xp2, zxp, u0, rn, g, n, lp, ln, zss, zrp, c);
-        if (acute) sfq = f2(q);
+    if (acute) {
+        double2 q64[N];
+        qcs_sfq_fp64_zone<N>(a, c, cur, s0, xp, zxp, zss, zrp, q64);
+#pragma unroll
+        for (int k = 0; k < N; ++k) sfq[k] = f2(q64[k]);
     }
-
     // QCS::setVelDiff, calcDtNew (FP64 reduction)
-    float dux = fabsf(fdot(fsub(u2f, uf), fsub(r2, r))) * rinv_el;
-    dux = (act && elen > 0.f) ? dux : 0.f;
-    float ztmp = fmaxf(dux, __shfl_xor_sync(kFull, dux, 1));
-    ztmp = fmaxf(ztmp, __shfl_xor_sync(kFull, ztmp, 2));   // idle triangle lanes carry 0
+    float ztmp = 0.f;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const int nk = (k + 1 == N) ? 0 : k + 1;
+        const float dux = fabsf(fdot(fsub(uf[nk], uf[k]), fsub(r[nk], r[k]))) * rinv[k];
+        ztmp = fmaxf(ztmp, (elen[k] > 0.f) ? dux : 0.f);
+    }
     const double zdu = c.q1 * zss + 2. * c.q2 * (double)ztmp;
     const double cdu = dmax(zdu, dmax(zss, 1.e-99));
-    const double zdthyd = zok ? (double)zdl * c.cfl / cdu : 1.e99;
+    zdthyd = (double)zdl * c.cfl / cdu;
 
-    const double2 sfpq = add(sfp, mk((double)sfq.x, (double)sfq.y));
-    const double2 ftot = add(sfpq, mk((double)sft.x, (double)sft.y));
-    const double2 ftot3 = shfl2(ftot, lp);
-    if (act) {
-        a.cforce_f[s] = f2(sub(ftot, ftot3));
-        a.sftot[s] = sfpq;
+    // side forces: PolyGas in FP64 (its surface vectors cancel around the
+    // zone and calcWork takes the residual), TTS in FP32; corner force and
+    // sfp + sfq for calcWork
+    float sstmp = fmaxf(zssf, (float)c.tts_ssmin);
+    sstmp = (float)c.alfa * sstmp * sstmp;
+    const float zareapf = (float)zareap;
+    double2 ftot[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const int nk = (k + 1 == N) ? 0 : k + 1;
+        const double2 ex64 = smul(0.5, add(xp[k], xp[nk]));
+        const double2 sfp = smul(-zp, mk(-(ex64.y - zxp.y), ex64.x - zxp.x));
+        const float2 ssurf = fk(-(ex[k].y - zc.y), ex[k].x - zc.x);
+        const float srho = zrpf * (float)mf[k] * (zareapf / (float)sa[k]);
+        const float2 sft = fmul(-(sstmp * (srho - zrpf)), ssurf);
+        const double2 sfpq = add(sfp, mk((double)sfq[k].x, (double)sfq[k].y));
+        ftot[k] = add(sfpq, mk((double)sft.x, (double)sft.y));
+        a.sftot[s0 + k] = sfpq;
     }
+#pragma unroll
+    for (int k = 0; k < N; ++k) a.cforce_f[s0 + k] = f2(sub(ftot[k], ftot[(k == 0) ? N - 1 : k - 1]));
+}
 
-    // pass A counts the corners without compression, in the dead zone and in
-    // acute zones; the closure pass counts the deferred ones by class
-    constexpr int kCounted[3] = {kClassZero, kClassDead, kClassAcute};
-    __shared__ unsigned wcount[kLearned ? kZoneThreads / 32 : 1][3];
-    if constexpr (kLearned) {
-        for (int q = 0; q < 3; ++q) {
-            const unsigned nq = __popc(__ballot_sync(kFull, act && cls == kCounted[q]));
-            if (lane == 0) wcount[threadIdx.x >> 5][q] = nq;
+#ifndef PNT_MIXED_ZT_MIN_BLOCKS
+#define PNT_MIXED_ZT_MIN_BLOCKS 4
+#endif
+constexpr int kZoneThreadsZT = 128;   // one zone per thread
+
+template <bool kQuads, bool kLearned>
+__global__ void __launch_bounds__(kZoneThreadsZT, PNT_MIXED_ZT_MIN_BLOCKS) pass_a_mixed_zt(DevArrays a, HydroConst c) {
+    const Ctl* ctl = a.ctl;
+    if (skip_cycle(ctl)) return;
+    const int64_t z = (int64_t)blockIdx.x * kZoneThreadsZT + threadIdx.x;
+    double zdthyd = 1.e99;
+    bool bad = false;
+    int cnt[3] = {0, 0, 0};
+    if (z < a.numz) {
+        const int cur = ctl->cycle & 1;
+        const double dt = ctl->dt;
+        if (kQuads) {
+            pass_a_mixed_zone<4, kLearned>(a, c, cur, dt, z, 4 * z, zdthyd, bad, cnt);
+        } else {
+            const int n = a.znump[z];
+            const int64_t s0 = a.zfirst[z];
+            if (n == 4) pass_a_mixed_zone<4, kLearned>(a, c, cur, dt, z, s0, zdthyd, bad, cnt);
+            else pass_a_mixed_zone<3, kLearned>(a, c, cur, dt, z, s0, zdthyd, bad, cnt);
         }
     }
-
+    __shared__ unsigned wcount[kLearned ? kZoneThreadsZT / 32 : 1][3];
+    if constexpr (kLearned) {
+        for (int q = 0; q < 3; ++q) {
+            const unsigned t = __reduce_add_sync(kFull, (unsigned)cnt[q]);
+            if ((threadIdx.x & 31) == 0) wcount[threadIdx.x >> 5][q] = t;
+        }
+    }
     const int nbad = __syncthreads_count(bad);
     if constexpr (kLearned) {
+        constexpr int kCounted[3] = {kClassZero, kClassDead, kClassAcute};
         if (threadIdx.x < 3) {
             unsigned t = 0;
-            for (int w = 0; w < kZoneThreads / 32; ++w) t += wcount[w][threadIdx.x];
+            for (int w = 0; w < kZoneThreadsZT / 32; ++w) t += wcount[w][threadIdx.x];
             if (t) atomicAdd(a.closure_counts + kCounted[threadIdx.x] * 64 + (blockIdx.x & 63), (unsigned long long)t);
         }
     }
     if (blockIdx.x >= (unsigned)a.npartA) return;   // partials are sized for this grid
-    block_fold<true, kZoneThreads>(zdthyd, a.part_dtnew + blockIdx.x);
+    block_fold<true, kZoneThreadsZT>(zdthyd, a.part_dtnew + blockIdx.x);
     if (threadIdx.x == 0) a.part_badA[blockIdx.x] = nbad;
 }
 
@@ -673,27 +732,26 @@ namespace {
 
 cudaError_t launch_cycle_mixed_impl(const DevArrays& a, const HydroConst& c, cudaStream_t stream, cudaEvent_t* ev,
                                     bool learned) {
-    const int zb = (int)zone_blocks(a.numz);
     const int zbc = (int)zone_blocks(a.numz, kZoneThreadsC);
     const int pb = (int)((a.nump + kPointThreads - 1) / kPointThreads);
     if (ev) cudaEventRecord(ev[0], stream);
+    const int zba = (int)((a.numz + kZoneThreadsZT - 1) / kZoneThreadsZT);
     if (learned) {
-        if (a.quads) pass_a_mixed<true, true><<<zb, kZoneThreads, 0, stream>>>(a, c);
-        else pass_a_mixed<false, true><<<zb, kZoneThreads, 0, stream>>>(a, c);
-        if (ev) cudaEventRecord(ev[1], stream);
-        closure_pass<<<a.closure_grid, kMlpRows, kMlpSmemBytes, stream>>>(a, c);
+        if (a.quads) pass_a_mixed_zt<true, true><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
+        else pass_a_mixed_zt<false, true><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
     } else {
-        if (a.quads) pass_a_mixed<true, false><<<zb, kZoneThreads, 0, stream>>>(a, c);
-        else pass_a_mixed<false, false><<<zb, kZoneThreads, 0, stream>>>(a, c);
-        if (ev) cudaEventRecord(ev[1], stream);
+        if (a.quads) pass_a_mixed_zt<true, false><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
+        else pass_a_mixed_zt<false, false><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
     }
+    if (ev) cudaEventRecord(ev[1], stream);
+    if (learned) closure_pass<<<a.closure_grid, kMlpRows, kMlpSmemBytes, stream>>>(a, c);
     if (ev) cudaEventRecord(ev[2], stream);
     pass_b_mixed<<<pb, kPointThreads, 0, stream>>>(a, c);
     if (ev) cudaEventRecord(ev[3], stream);
     if (a.quads) pass_c_mixed<true><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
     else pass_c_mixed<false><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
     if (ev) cudaEventRecord(ev[4], stream);
-    launch_finalize(a, c, zb, zbc, stream);
+    launch_finalize(a, c, zba, zbc, stream);
     if (ev) cudaEventRecord(ev[5], stream);
     return cudaGetLastError();
 }
