@@ -57,9 +57,9 @@ MLP_FLOP_PER_ROW = 2 * (16 * 64 + 64 * 64 + 64 * 16)   # tensor-core MMA shapes,
 # DRAM bytes (read + write) of one pass A launch per zone, from the ncu
 # capture of profiles/pass_a_closure_sedov1024.md (1,048,576 zones; the
 # bench scales them by its zone count)
-PASS_A_TRAFFIC_PER_ZONE = {"learned": (127.181e6 + 99.845e6) / 1048576,
-                           "mixed": (125.929e6 + 88.921e6) / 1048576,
-                           "fp64": (126.054e6 + 148.091e6) / 1048576}
+PASS_A_TRAFFIC_PER_ZONE = {"learned": (126.038e6 + 98.280e6) / 1048576,
+                           "mixed": (125.964e6 + 86.100e6) / 1048576,
+                           "fp64": (125.949e6 + 128.223e6) / 1048576}
 
 
 def algorithmic_bytes(nump, nums, numz):
