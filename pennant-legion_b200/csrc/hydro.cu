@@ -270,7 +270,8 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
         (st = h->alloc(&a.cmass, ns)) || (st = h->alloc(&a.cforce, ns)) || (st = h->alloc(&a.sftot, ns)) ||
         (st = h->alloc(&a.part_dtnew, nzb)) || (st = h->alloc(&a.part_badA, nzb)) ||
         (st = h->alloc(&a.part_dvov, nzbc)) || (st = h->alloc(&a.part_badC, nzbc)) ||
-        (st = h->alloc(&a.ctl, 1)))
+        (st = h->alloc(&a.fin_part, 2 * kFinBlocks)) || (st = h->alloc(&a.fin_bad, 2 * kFinBlocks)) ||
+        (st = h->alloc(&a.fin_ticket, 1)) || (st = h->alloc(&a.ctl, 1)))
         return st;
     a.npartA = (int32_t)nzb;
     a.npartC = (int32_t)nzbc;
@@ -312,7 +313,8 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
         (e = up(a.zetot, zetot.data(), nz * 8)) || (e = up(a.zwrate, zwrate.data(), nz * 8)) ||
         (e = up(a.zvol, m.zvol.data(), nz * 8)) || (e = up(a.ctl, &ctl, sizeof(Ctl))))
         return fail(PNT_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
-    if ((e = cudaMemsetAsync(a.zp, 0, nz * 8, s)) || (e = cudaMemsetAsync(a.px[1], 0, np * 16, s)) ||
+    if ((e = cudaMemsetAsync(a.zp, 0, nz * 8, s)) || (e = cudaMemsetAsync(a.fin_ticket, 0, 4, s)) ||
+        (e = cudaMemsetAsync(a.px[1], 0, np * 16, s)) ||
         (e = cudaMemsetAsync(a.pu[1], 0, np * 16, s)))
         return fail(PNT_ERR_CUDA, "memset: %s", cudaGetErrorString(e));
     CUDA_TRY(cudaStreamSynchronize(s));

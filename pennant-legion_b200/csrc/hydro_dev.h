@@ -76,6 +76,11 @@ struct DevArrays {
     int32_t* part_badA;
     double* part_dvov;
     int32_t* part_badC;
+    // the finalize blocks' results (kFinBlocks each of dt, dvov / bad
+    // counts) and the ticket that picks the last block
+    double* fin_part;
+    int32_t* fin_bad;
+    uint32_t* fin_ticket;
     Ctl* ctl;
     // learned closure (precision = learned): parameter image and the corner
     // class counters [class][64] (closure_dev.cuh)
@@ -103,6 +108,7 @@ inline int64_t zone_blocks(int32_t numz, int threads = kZoneThreads) {
 // Events a cycle records when timed: before pass A, after A, after the
 // closure pass (right after A when there is none), after B, C, finalize.
 constexpr int kNumEvents = 6;
+constexpr int kFinBlocks = 64;   // blocks of the finalize reduction
 constexpr int kNumKernels = 5;   // A, B, C, finalize, closure pass
 
 // One hydro cycle (passes A, B, C and the finalize step) on `stream`.  With

@@ -92,24 +92,13 @@ __global__ void __launch_bounds__(kZoneThreadsC) pass_c(DevArrays a, HydroConst 
     if (threadIdx.x == 0) a.part_badC[blockIdx.x] = nbad;
 }
 
-constexpr int kFinThreads = 1024;
+// finalize: kFinBlocks blocks reduce slices of the pass A / pass C
+// partials; the last block to finish (ticket counter) reduces the blocks'
+// results and ends the cycle.  Minimum, maximum and integer sums are exact
+// in any order, so the result does not depend on which block is last.
+constexpr int kFinThreads = 512;
 
-__global__ void __launch_bounds__(kFinThreads) finalize(DevArrays a, HydroConst c, int nblocksA, int nblocksC) {
-    Ctl* ctl = a.ctl;
-    if (skip_cycle(ctl)) return;
-    double dtn = 1.e99, dvm = 1.e-99;
-    int badA = 0, badC = 0;
-#pragma unroll 4
-    for (int i = threadIdx.x; i < nblocksA; i += kFinThreads) {
-        dtn = dmin(dtn, a.part_dtnew[i]);
-        badA += a.part_badA[i];
-    }
-#pragma unroll 4
-    for (int i = threadIdx.x; i < nblocksC; i += kFinThreads) {
-        const double v = a.part_dvov[i];
-        dvm = (v > dvm) ? v : dvm;
-        badC += a.part_badC[i];
-    }
+__device__ __forceinline__ void fin_block_reduce(double& dtn, double& dvm, int& badA, int& badC) {
     __shared__ double sdt[kFinThreads / 32], sdv[kFinThreads / 32];
     __shared__ int sba[kFinThreads / 32], sbc[kFinThreads / 32];
     for (int o = 16; o > 0; o >>= 1) {
@@ -122,15 +111,61 @@ __global__ void __launch_bounds__(kFinThreads) finalize(DevArrays a, HydroConst 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) { sdt[warp] = dtn; sdv[warp] = dvm; sba[warp] = badA; sbc[warp] = badC; }
     __syncthreads();
-    if (threadIdx.x != 0) return;
-    for (int i = 1; i < kFinThreads / 32; ++i) {
-        dtn = dmin(dtn, sdt[i]);
-        dvm = (sdv[i] > dvm) ? sdv[i] : dvm;
+    if (threadIdx.x == 0) {
+        for (int i = 1; i < kFinThreads / 32; ++i) {
+            dtn = dmin(dtn, sdt[i]);
+            dvm = (sdv[i] > dvm) ? sdv[i] : dvm;
+        }
+        badA = 0;
+        badC = 0;
+        for (int i = 0; i < kFinThreads / 32; ++i) { badA += sba[i]; badC += sbc[i]; }
     }
-    badA = 0;
-    badC = 0;
-    for (int i = 0; i < kFinThreads / 32; ++i) { badA += sba[i]; badC += sbc[i]; }
-    finish_cycle(ctl, c, dtn, dvm, badA, badC);
+    __syncthreads();   // the shared slots are reused by the last block
+}
+
+__global__ void __launch_bounds__(kFinThreads) finalize(DevArrays a, HydroConst c, int nblocksA, int nblocksC) {
+    Ctl* ctl = a.ctl;
+    if (skip_cycle(ctl)) return;
+    double dtn = 1.e99, dvm = 1.e-99;
+    int badA = 0, badC = 0;
+    const int stride = gridDim.x * kFinThreads;
+    for (int i = blockIdx.x * kFinThreads + threadIdx.x; i < nblocksA; i += stride) {
+        dtn = dmin(dtn, a.part_dtnew[i]);
+        badA += a.part_badA[i];
+    }
+    for (int i = blockIdx.x * kFinThreads + threadIdx.x; i < nblocksC; i += stride) {
+        const double v = a.part_dvov[i];
+        dvm = (v > dvm) ? v : dvm;
+        badC += a.part_badC[i];
+    }
+    fin_block_reduce(dtn, dvm, badA, badC);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        a.fin_part[blockIdx.x] = dtn;
+        a.fin_part[kFinBlocks + blockIdx.x] = dvm;
+        a.fin_bad[blockIdx.x] = badA;
+        a.fin_bad[kFinBlocks + blockIdx.x] = badC;
+        __threadfence();
+        last = atomicAdd(a.fin_ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    dtn = 1.e99;
+    dvm = 1.e-99;
+    badA = badC = 0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += kFinThreads) {
+        dtn = dmin(dtn, __ldcg(a.fin_part + i));
+        const double v = __ldcg(a.fin_part + kFinBlocks + i);
+        dvm = (v > dvm) ? v : dvm;
+        badA += __ldcg(a.fin_bad + i);
+        badC += __ldcg(a.fin_bad + kFinBlocks + i);
+    }
+    fin_block_reduce(dtn, dvm, badA, badC);
+    if (threadIdx.x == 0) {
+        *a.fin_ticket = 0u;
+        finish_cycle(ctl, c, dtn, dvm, badA, badC);
+    }
 }
 
 }  // namespace
@@ -149,13 +184,13 @@ cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStrea
     if (a.quads) pass_c<true><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
     else pass_c<false><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
     if (ev) cudaEventRecord(ev[4], stream);
-    finalize<<<1, kFinThreads, 0, stream>>>(a, c, zba, zbc);
+    finalize<<<kFinBlocks, kFinThreads, 0, stream>>>(a, c, zba, zbc);
     if (ev) cudaEventRecord(ev[5], stream);
     return cudaGetLastError();
 }
 
 void launch_finalize(const DevArrays& a, const HydroConst& c, int nA, int nC, cudaStream_t stream) {
-    finalize<<<1, kFinThreads, 0, stream>>>(a, c, nA, nC);
+    finalize<<<kFinBlocks, kFinThreads, 0, stream>>>(a, c, nA, nC);
 }
 
 }  // namespace pnt
