@@ -178,3 +178,23 @@ def test_sedov480_to_t1_matches_oracle_fingerprint():
     assert s["cycle"] == fp["cycle"]
     assert s["time"] == float.fromhex(fp["time"])
     _fp_compare(fp, h, "sedov480")
+
+
+def test_copy_state_restarts_bitwise():
+    """pnt_hydro_copy_state: an object restarted from another's state
+    continues exactly as the source does (same fields after the same cycles),
+    and refuses objects of another mesh."""
+    text = open(golden("sedov.pnt")).read().replace("cstop   10", "cstop   60")
+    d = pb.Deck(text=text)
+    src = pb.Hydro(pb.Mesh(deck=d), d.params())
+    src.run(max_cycles=25)
+    dst = pb.Hydro(pb.Mesh(deck=pb.Deck(text=text)), d.params())
+    dst.copy_state_from(src)
+    assert dst.scalars()["cycle"] == 25 and dst.scalars()["time"] == src.scalars()["time"]
+    s1, s2 = src.run(), dst.run()
+    assert s1["cycle"] == s2["cycle"] == 60 and s1["time"] == s2["time"]
+    for k in ("px", "pu", "zr", "ze", "zp", "zetot", "zvol", "zwrate"):
+        assert src.download(k).tobytes() == dst.download(k).tobytes(), k
+    other = pb.Hydro(pb.Mesh(deck=pb.Deck(path=golden("sedovsmall.pnt"))), d.params())
+    with pytest.raises(pb.PntError):
+        other.copy_state_from(src)
