@@ -259,11 +259,18 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
     double* smf;
     uint16_t* mask;
     const int64_t nzb = zone_blocks((int32_t)nz);
-    const int64_t nzbc = zone_blocks((int32_t)nz, kZoneThreadsC);
+    // pass C is persistent: one partial per CTA of its grid
+    {
+        int nsm = 148;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+        const cudaError_t e = prepare_pass_c(p.precision != PNT_PREC_FP64, a.quads != 0, a.numz, nsm, &a.gridC);
+        if (e != cudaSuccess) return fail(PNT_ERR_CUDA, "pass C setup: %s", cudaGetErrorString(e));
+    }
+    const int64_t nzbc = a.gridC;
     pnt_status st = PNT_OK;
     if ((st = h->alloc(&zfirst, nz)) || (st = h->alloc(&znump, nz)) || (st = h->alloc(&mapsp1, ns)) ||
         (st = h->alloc(&smf, ns)) || (st = h->alloc(&poff, np + 1)) || (st = h->alloc(&pcorner, ns)) ||
-        (st = h->alloc(&mask, np)) || (st = h->alloc(&a.px[0], np)) || (st = h->alloc(&a.px[1], np)) ||
+        (st = h->alloc(&mask, np + 2)) || (st = h->alloc(&a.px[0], np)) || (st = h->alloc(&a.px[1], np)) ||
         (st = h->alloc(&a.pu[0], np)) || (st = h->alloc(&a.pu[1], np)) || (st = h->alloc(&a.zm, nz)) ||
         (st = h->alloc(&a.zr, nz)) || (st = h->alloc(&a.ze, nz)) || (st = h->alloc(&a.zetot, nz)) ||
         (st = h->alloc(&a.zwrate, nz)) || (st = h->alloc(&a.zvol, nz)) || (st = h->alloc(&a.zp, nz)) ||
@@ -314,6 +321,7 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
         (e = up(a.zvol, m.zvol.data(), nz * 8)) || (e = up(a.ctl, &ctl, sizeof(Ctl))))
         return fail(PNT_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
     if ((e = cudaMemsetAsync(a.zp, 0, nz * 8, s)) || (e = cudaMemsetAsync(a.fin_ticket, 0, 4, s)) ||
+        (e = cudaMemsetAsync(mask + np, 0, 4, s)) ||
         (e = cudaMemsetAsync(a.px[1], 0, np * 16, s)) ||
         (e = cudaMemsetAsync(a.pu[1], 0, np * 16, s)))
         return fail(PNT_ERR_CUDA, "memset: %s", cudaGetErrorString(e));

@@ -92,13 +92,10 @@ struct DevArrays {
     int2* closure_zhdr;
     int32_t* closure_nrec;
     int32_t closure_grid;   // CTAs of the persistent closure pass
+    int32_t gridC;          // CTAs of the persistent pass C (pass_c_staged.cuh)
 };
 
-#ifndef PNT_ZONE_THREADS_C
-#define PNT_ZONE_THREADS_C 128
-#endif
 constexpr int kZoneThreads = 256;   // pass A: 64 zones x 4 side lanes per block
-constexpr int kZoneThreadsC = PNT_ZONE_THREADS_C;   // pass C: 32 zones per block
 constexpr int kPointThreads = 256;
 
 inline int64_t zone_blocks(int32_t numz, int threads = kZoneThreads) {
@@ -123,6 +120,13 @@ cudaError_t launch_cycle_learned(const DevArrays& a, const HydroConst& c, cudaSt
                                  cudaEvent_t* ev = nullptr);
 // Raises the learned pass A's dynamic shared-memory limit on the current device.
 cudaError_t prepare_learned_kernels();
+// Pass C of the FP64 (mixed = false) or mixed/learned cycle (pass_c.cu):
+// prepare_pass_c raises the kernel's shared-memory limit on the current
+// device and returns its persistent grid (resident CTAs per SM x nsm, at
+// most one per tile); launch_pass_c launches it with a.gridC CTAs, which
+// write a.gridC partials.
+cudaError_t prepare_pass_c(bool mixed, bool quads, int32_t numz, int nsm, int32_t* grid);
+void launch_pass_c(const DevArrays& a, const HydroConst& c, bool mixed, cudaStream_t stream);
 // The finalize step shared by both cycles (nA / nC partials of passes A / C).
 void launch_finalize(const DevArrays& a, const HydroConst& c, int nA, int nC, cudaStream_t stream);
 

@@ -21,10 +21,12 @@
 // shuffles; 168 registers, 3 blocks of 128 per SM (13% faster than the
 // four-lanes-per-zone form pass_a_zone at a developed 1024^2 Sedov state;
 // it is bound by the ~50 correctly rounded FP64 divisions and square roots
-// of a zone).  Pass C and the batched kernels keep four lanes per zone: one
-// lane per side/corner, zone-local side data moved by warp shuffles, zone
-// sums formed by every lane in the serial side order, zone quotients split
-// over the lanes.  1/elen is formed
+// of a zone).  Pass C is the persistent staged kernel of pass_c.cu (one
+// thread per zone, inputs gathered into shared memory by asynchronous
+// copies).  The batched kernels keep four lanes per zone: one lane per
+// side/corner, zone-local side data moved by warp shuffles, zone sums formed
+// by every lane in the serial side order, zone quotients split over the
+// lanes.  1/elen is formed
 // once per side and shared with the neighbouring corner; QCS terms the
 // reference computes and then discards (evol and du unless cdiv < 0, zkur
 // when cdiv > 0) are not computed, which leaves every stored value
@@ -74,22 +76,6 @@ __global__ void __launch_bounds__(kPointThreads) pass_b(DevArrays a, HydroConst 
     const int64_t p = (int64_t)blockIdx.x * kPointThreads + threadIdx.x;
     if (p >= a.nump) return;
     pass_b_point(a, c, ctl->cycle & 1, ctl->dt, p);
-}
-
-template <bool kQuads>
-__global__ void __launch_bounds__(kZoneThreadsC) pass_c(DevArrays a, HydroConst c) {
-    const Ctl* ctl = a.ctl;
-    if (skip_cycle(ctl)) return;
-    const int64_t tid = (int64_t)blockIdx.x * kZoneThreadsC + threadIdx.x;
-    const int64_t z = tid >> 2;
-    double zdvov;
-    bool bad;
-    pass_c_zone<kQuads>(a, c, ctl->cycle & 1, ctl->dt, ctl->dtinv, z, (int)(tid & 3), threadIdx.x & 31,
-                        z < a.numz, zdvov, bad);
-    const int nbad = __syncthreads_count(bad);
-    if (blockIdx.x >= (unsigned)a.npartC) return;   // partials are sized for this grid
-    block_fold<false, kZoneThreadsC>(zdvov, a.part_dvov + blockIdx.x);
-    if (threadIdx.x == 0) a.part_badC[blockIdx.x] = nbad;
 }
 
 // finalize: kFinBlocks blocks reduce slices of the pass A / pass C
@@ -171,7 +157,6 @@ __global__ void __launch_bounds__(kFinThreads) finalize(DevArrays a, HydroConst 
 }  // namespace
 cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStream_t stream, cudaEvent_t* ev) {
     const int zb = (int)zone_blocks(a.numz);
-    const int zbc = (int)zone_blocks(a.numz, kZoneThreadsC);
     const int pb = (int)((a.nump + kPointThreads - 1) / kPointThreads);
     if (ev) cudaEventRecord(ev[0], stream);
     const int zba = (int)((a.numz + kZoneThreadsZT - 1) / kZoneThreadsZT);
@@ -181,10 +166,9 @@ cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStrea
     if (ev) cudaEventRecord(ev[2], stream);   // no closure pass
     pass_b<<<pb, kPointThreads, 0, stream>>>(a, c);
     if (ev) cudaEventRecord(ev[3], stream);
-    if (a.quads) pass_c<true><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
-    else pass_c<false><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
+    launch_pass_c(a, c, false, stream);
     if (ev) cudaEventRecord(ev[4], stream);
-    finalize<<<kFinBlocks, kFinThreads, 0, stream>>>(a, c, zba, zbc);
+    finalize<<<kFinBlocks, kFinThreads, 0, stream>>>(a, c, zba, a.gridC);
     if (ev) cudaEventRecord(ev[5], stream);
     return cudaGetLastError();
 }

@@ -651,88 +651,12 @@ __global__ void __launch_bounds__(kMlpRows, 3) closure_pass(DevArrays a, HydroCo
     }
 }
 
-// ---------------------------------------------------------------------
-// Pass C, mixed: FP64 corrector with the FP32 sfp + sfq input
-// ---------------------------------------------------------------------
-template <bool kQuads>
-__global__ void __launch_bounds__(kZoneThreadsC) pass_c_mixed(DevArrays a, HydroConst c) {
-    const Ctl* ctl = a.ctl;
-    if (skip_cycle(ctl)) return;
-    const int cur = ctl->cycle & 1;
-    const double dt = ctl->dt;
-    const int64_t tid = (int64_t)blockIdx.x * kZoneThreadsC + threadIdx.x;
-    const int64_t z = tid >> 2;
-    const int k = (int)(tid & 3);
-    const int lane = threadIdx.x & 31;
-    const int g = lane & ~3;
-    const bool zok = z < a.numz;
-    int n = 4;
-    int64_t s = 4 * z + k;
-    if (!kQuads) {
-        n = zok ? a.znump[z] : 4;
-        s = (zok ? (int64_t)a.zfirst[z] : 0) + k;
-    }
-    const bool act = zok && k < n;
-    const int ln = g + (k + 1 >= n ? 0 : k + 1);
-
-    const int32_t p1 = act ? __ldg(a.mapsp1 + s) : 0;
-    const double2 x0 = act ? a.px[cur][p1] : mk(0., 0.);
-    const double2 u0 = act ? a.pu[cur][p1] : mk(0., 0.);
-    const double2 x = act ? a.px[cur ^ 1][p1] : mk(0., 0.);
-    const double2 u = act ? a.pu[cur ^ 1][p1] : mk(0., 0.);
-    const unsigned mask = act ? a.bcmask[p1] : 0u;
-    const double2 sft = act ? a.sftot[s] : mk(0., 0.);
-    const double zm = zok ? a.zm[z] : 1.;
-    const double zetot0 = zok ? a.zetot[z] : 0.;
-    const double zvol0 = zok ? a.zvol[z] : 1.;
-    const double zp = zok ? a.zp[z] : 0.;
-
-    const double dth = 0.5 * dt;
-    const double2 xp = add(x0, smul(dth, u0));
-    double2 u0b = u0;
-    if (mask) {
-        for (int b = 0; b < c.nbc; ++b)
-            if (mask & (1u << b)) u0b = project(u0b, c.vfix[b][0], c.vfix[b][1]);
-    }
-    const double2 x2 = shfl2(x, ln);
-    const double2 xp2 = shfl2(xp, ln);
-    const double2 u0b2 = shfl2(u0b, ln);
-    const double2 u2 = shfl2(u, ln);
-    const double rn = 1. / (double)n;
-    const double2 zx = mk(zsum4(x.x * rn, g, n), zsum4(x.y * rn, g, n));
-    const double third = 1. / 3.;
-    const double sa = 0.5 * cross(sub(x2, x), sub(zx, x));
-    const double sv = third * sa * (x.x + x2.x + zx.x);
-    const double zvol = zsum4(sv, g, n);
-    const bool bad = act && (sv <= 0.);
-    const double sd1 = dot(sft, add(u0b, u));
-    const double sd2 = dot(neg(sft), add(u0b2, u2));
-    const double dwork = -dth * (sd1 * xp.x + sd2 * xp2.x);
-    const double zw = zsum4(dwork, g, n);
-    const double zetot = zetot0 + zw;
-    const double zwrate = (zw + zp * (zvol - zvol0)) * ctl->dtinv;
-    const double qv = ((k == 0) ? zm : (k == 1 ? zetot : zvol - zvol0)) /
-                      ((k == 0) ? zvol : (k == 1 ? zm + 1.e-99 : zvol0));
-    const double zdvov = (zok && k == 2) ? fabs(qv) : 1.e-99;
-    __syncwarp();
-    if (zok) {
-        if (k == 0) { a.zvol[z] = zvol; a.zr[z] = qv; }
-        else if (k == 1) { a.zetot[z] = zetot; a.ze[z] = qv; }
-        else if (k == 2) a.zwrate[z] = zwrate;
-    }
-    const int nbad = __syncthreads_count(bad);
-    if (blockIdx.x >= (unsigned)a.npartC) return;   // partials are sized for this grid
-    block_fold<false, kZoneThreadsC>(zdvov, a.part_dvov + blockIdx.x);
-    if (threadIdx.x == 0) a.part_badC[blockIdx.x] = nbad;
-}
-
 }  // namespace
 
 namespace {
 
 cudaError_t launch_cycle_mixed_impl(const DevArrays& a, const HydroConst& c, cudaStream_t stream, cudaEvent_t* ev,
                                     bool learned) {
-    const int zbc = (int)zone_blocks(a.numz, kZoneThreadsC);
     const int pb = (int)((a.nump + kPointThreads - 1) / kPointThreads);
     if (ev) cudaEventRecord(ev[0], stream);
     const int zba = (int)((a.numz + kZoneThreadsZT - 1) / kZoneThreadsZT);
@@ -748,10 +672,9 @@ cudaError_t launch_cycle_mixed_impl(const DevArrays& a, const HydroConst& c, cud
     if (ev) cudaEventRecord(ev[2], stream);
     pass_b_mixed<<<pb, kPointThreads, 0, stream>>>(a, c);
     if (ev) cudaEventRecord(ev[3], stream);
-    if (a.quads) pass_c_mixed<true><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
-    else pass_c_mixed<false><<<zbc, kZoneThreadsC, 0, stream>>>(a, c);
+    launch_pass_c(a, c, true, stream);
     if (ev) cudaEventRecord(ev[4], stream);
-    launch_finalize(a, c, zba, zbc, stream);
+    launch_finalize(a, c, zba, a.gridC, stream);
     if (ev) cudaEventRecord(ev[5], stream);
     return cudaGetLastError();
 }

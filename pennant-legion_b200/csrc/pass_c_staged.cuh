@@ -1,0 +1,324 @@
+// pass_c_staged.cuh -- pass C (the corrector zone pass: calcCtrs, calcVols,
+// calcWork, calcWorkRate, calcEnergy, calcRho, calcDvol at the end of
+// Hydro::doCycle, Hydro.cc:924-983) as a persistent kernel that stages its
+// gathered inputs in shared memory.
+//
+// Pass C reads, per side, the start-of-cycle and new position and velocity
+// of the side's first point (a gather through mapsp1) and the side's sfp +
+// sfq, and per zone four scalars.  Loaded straight into registers this is a
+// chain of two dependent memory latencies per zone (index, then points)
+// with few loads in flight, and four lanes per zone add ~36 shuffles per
+// lane: that kernel ran at 31% of peak DRAM throughput.  Here each CTA walks
+// its tiles of kTile zones, one thread per zone: a thread issues all the
+// asynchronous copies (`cp.async`, global -> shared, no registers held) of
+// its zone's inputs at once, with the point indices already in registers
+// (loaded one tile ahead), waits for them and computes the zone from shared
+// memory.  kStages > 1 keeps kStages - 1 further tiles in flight during the
+// compute; on the B200 more resident CTAs beat deeper pipelines (1024^2
+// Sedov: 1 stage and 10 CTAs of 64 per SM 56 us, 2 stages 59 us, 3 stages
+// 72 us), so the default is one stage.  A thread copies and reads only its
+// own zone's slots (structure-of-arrays across the tile's threads, so
+// shared-memory accesses are conflict-free), so `cp.async.wait_group` alone
+// orders them; no block barrier inside the loop.
+//
+// The zone arithmetic is the four-lane pass C's, one zone per thread:
+// kMixed = false keeps the reference's serial side order and operation
+// order (zone sums start from 0.0, bit-identical to pass_c_zone when the
+// including file is compiled with -fmad=false); kMixed = true is the mixed
+// cycle's form (sums start from the first side, zetot = zetot0 + the zone's
+// work).
+#pragma once
+
+#include "hydro_dev.h"
+
+#include <cuda_runtime.h>
+
+namespace pnt {
+namespace stagedc {
+
+#ifndef PNT_STAGED_C_TILE
+#define PNT_STAGED_C_TILE 64
+#endif
+#ifndef PNT_STAGED_C_STAGES
+#define PNT_STAGED_C_STAGES 1
+#endif
+constexpr int kTile = PNT_STAGED_C_TILE;       // zones (threads) per tile
+constexpr int kStages = PNT_STAGED_C_STAGES;   // tiles resident per CTA
+static_assert(kTile % 32 == 0 && kStages >= 1, "tile of whole warps");
+
+// Bytes of one stage per zone: per side x0.x (8), u0 (16), x (16), u (16),
+// sftot (16), the 32-bit bcmask word holding the point's mask (4); per zone
+// zm, zetot, zvol, zp (32).
+constexpr int kOffX0x = 0;
+constexpr int kOffU0 = kOffX0x + 4 * 8 * kTile;
+constexpr int kOffX = kOffU0 + 4 * 16 * kTile;
+constexpr int kOffU = kOffX + 4 * 16 * kTile;
+constexpr int kOffSf = kOffU + 4 * 16 * kTile;
+constexpr int kOffMw = kOffSf + 4 * 16 * kTile;
+constexpr int kOffZs = kOffMw + 4 * 4 * kTile;
+constexpr int kOffMeta = kOffZs + 4 * 8 * kTile;
+constexpr int kStageBytes = kOffMeta + 4 * kTile;
+constexpr int kSmemBytes = kStages * kStageBytes;
+
+__device__ __forceinline__ unsigned saddr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp16(void* s, const void* g) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp8(void* s, const void* g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(saddr(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp4(void* s, const void* g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(saddr(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void wait_groups() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Where one zone's inputs live: its first side, side count and point indices.
+struct ZoneIdx {
+    int4 p;
+    int32_t s0;
+    int32_t n;
+};
+
+template <bool kQuads>
+__device__ __forceinline__ ZoneIdx load_idx(const DevArrays& a, int64_t z) {
+    ZoneIdx r{make_int4(0, 0, 0, 0), 0, 0};
+    if (z >= a.numz) return r;
+    if (kQuads) {
+        r.s0 = (int32_t)(4 * z);
+        r.n = 4;
+        r.p = __ldg(reinterpret_cast<const int4*>(a.mapsp1) + z);
+    } else {
+        r.s0 = a.zfirst[z];
+        r.n = a.znump[z];
+        r.p.x = a.mapsp1[r.s0];
+        r.p.y = a.mapsp1[r.s0 + 1];
+        r.p.z = a.mapsp1[r.s0 + 2];
+        r.p.w = r.n == 4 ? a.mapsp1[r.s0 + 3] : 0;
+    }
+    return r;
+}
+
+__device__ __forceinline__ int pick(const int4& v, int k) {
+    return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
+}
+
+// Issues the copies of zone z's inputs into slot t of stage st.  bcmask is
+// 16-bit per point; its 32-bit word is copied (the buffer is padded to a
+// whole word) and the point's parity kept in the zone's meta word.
+__device__ __forceinline__ void issue(const DevArrays& a, int cur, unsigned char* st, int t, int64_t z,
+                                      const ZoneIdx& ix) {
+    if (z >= a.numz) return;
+    const double2* px0 = a.px[cur];
+    const double2* pu0 = a.pu[cur];
+    const double2* px1 = a.px[cur ^ 1];
+    const double2* pu1 = a.pu[cur ^ 1];
+    const uint32_t* mw = reinterpret_cast<const uint32_t*>(a.bcmask);
+    int meta = ix.n;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (k < ix.n) {
+            const int p = pick(ix.p, k);
+            cp8(st + kOffX0x + (k * kTile + t) * 8, &px0[p].x);
+            cp16(st + kOffU0 + (k * kTile + t) * 16, pu0 + p);
+            cp16(st + kOffX + (k * kTile + t) * 16, px1 + p);
+            cp16(st + kOffU + (k * kTile + t) * 16, pu1 + p);
+            cp16(st + kOffSf + (k * kTile + t) * 16, a.sftot + ix.s0 + k);
+            cp4(st + kOffMw + (k * kTile + t) * 4, mw + (p >> 1));
+            meta |= (p & 1) << (4 + k);
+        }
+    }
+    cp8(st + kOffZs + (0 * kTile + t) * 8, a.zm + z);
+    cp8(st + kOffZs + (1 * kTile + t) * 8, a.zetot + z);
+    cp8(st + kOffZs + (2 * kTile + t) * 8, a.zvol + z);
+    cp8(st + kOffZs + (3 * kTile + t) * 8, a.zp + z);
+    reinterpret_cast<int*>(st + kOffMeta)[t] = meta;
+}
+
+__device__ __forceinline__ double2 mk2(double x, double y) { return make_double2(x, y); }
+__device__ __forceinline__ double2 proj(double2 v, double ux, double uy) {
+    const double d = v.x * ux + v.y * uy;
+    return mk2(v.x - ux * d, v.y - uy * d);
+}
+
+// One zone's corrector from stage st, slot t: writes zvol, zr, zetot, ze,
+// zwrate; returns |dV/V0| and adds the zone's inverted sides to nbad.
+template <bool kQuads, bool kMixed>
+__device__ __forceinline__ double zone(const DevArrays& a, const HydroConst& c, const unsigned char* st, int t,
+                                       int64_t z, double dt, double dtinv, int& nbad) {
+    const int meta = reinterpret_cast<const int*>(st + kOffMeta)[t];
+    const int n = kQuads ? 4 : (meta & 15);
+    const double* sx0x = reinterpret_cast<const double*>(st + kOffX0x);
+    const double2* su0 = reinterpret_cast<const double2*>(st + kOffU0);
+    const double2* sx = reinterpret_cast<const double2*>(st + kOffX);
+    const double2* su = reinterpret_cast<const double2*>(st + kOffU);
+    const double2* ssf = reinterpret_cast<const double2*>(st + kOffSf);
+    const uint32_t* smw = reinterpret_cast<const uint32_t*>(st + kOffMw);
+    const double* szs = reinterpret_cast<const double*>(st + kOffZs);
+    const double zm = szs[t], zetot0 = szs[kTile + t], zvol0 = szs[2 * kTile + t], zp = szs[3 * kTile + t];
+    const double dth = 0.5 * dt;
+
+    double2 x[4], ub[4];
+    double xpx[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (k < n) {
+            x[k] = sx[k * kTile + t];
+            const double2 u0 = su0[k * kTile + t];
+            xpx[k] = sx0x[k * kTile + t] + u0.x * dth;   // advPosHalf's x, from pu0 before the BCs
+            // applyFixedBC on pu0 (Hydro.cc:1008-1032), planes in deck order
+            const unsigned mask = (smw[k * kTile + t] >> (((meta >> (4 + k)) & 1) * 16)) & 0xffffu;
+            double2 u0b = u0;
+            if (mask) {
+                for (int b = 0; b < c.nbc; ++b)
+                    if (mask & (1u << b)) u0b = proj(u0b, c.vfix[b][0], c.vfix[b][1]);
+            }
+            ub[k] = u0b;
+        } else {
+            x[k] = mk2(0., 0.);
+            ub[k] = mk2(0., 0.);
+            xpx[k] = 0.;
+        }
+    }
+    // calcCtrs + calcVols at the new positions (Mesh.cc:797-837, :928-989)
+    const double rn = 1. / (double)n;
+    double zxx, zxy;
+    if (kMixed) {
+        zxx = x[0].x * rn + x[1].x * rn + x[2].x * rn;
+        zxy = x[0].y * rn + x[1].y * rn + x[2].y * rn;
+    } else {
+        zxx = __dadd_rn(0.0, x[0].x * rn) + x[1].x * rn + x[2].x * rn;
+        zxy = __dadd_rn(0.0, x[0].y * rn) + x[1].y * rn + x[2].y * rn;
+    }
+    if (n == 4) {
+        zxx = zxx + x[3].x * rn;
+        zxy = zxy + x[3].y * rn;
+    }
+    const double third = 1. / 3.;
+    double zvol = 0., zetot = zetot0, zw = 0.;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (k < n) {
+            const int k2 = (k + 1 == n) ? 0 : k + 1;
+            const double2 x2 = x[k2];
+            const double sa = 0.5 * ((x2.x - x[k].x) * (zxy - x[k].y) - (x2.y - x[k].y) * (zxx - x[k].x));
+            const double sv = third * sa * (x[k].x + x2.x + zxx);
+            nbad += (sv <= 0.) ? 1 : 0;
+            // calcWork (Hydro.cc:1339-1406): the side's force against the
+            // average velocity of its two points, at the half-step positions
+            const double2 sf = ssf[k * kTile + t];
+            const double2 u = su[k * kTile + t];
+            const double2 u2 = su[k2 * kTile + t];
+            const double sd1 = sf.x * (ub[k].x + u.x) + sf.y * (ub[k].y + u.y);
+            const double sd2 = (-sf.x) * (ub[k2].x + u2.x) + (-sf.y) * (ub[k2].y + u2.y);
+            const double dwork = -dth * (sd1 * xpx[k] + sd2 * xpx[k2]);
+            if (kMixed) {
+                zvol = (k == 0) ? sv : zvol + sv;
+                zw = (k == 0) ? dwork : zw + dwork;
+            } else {
+                zvol = (k == 0) ? __dadd_rn(0.0, sv) : zvol + sv;
+                zw = (k == 0) ? __dadd_rn(0.0, dwork) : zw + dwork;
+                zetot = zetot + dwork;
+            }
+        }
+    }
+    if (kMixed) zetot = zetot0 + zw;
+    // calcWorkRate (Hydro.cc:1483-1510), calcEnergy (:1545-1564),
+    // calcRho (:1034-1054), calcDvol (:1622-1644)
+    const double dvol = zvol - zvol0;
+    const double zwrate = (zw + zp * dvol) * dtinv;
+    a.zvol[z] = zvol;
+    a.zr[z] = zm / zvol;
+    a.zetot[z] = zetot;
+    a.ze[z] = zetot / (zm + 1.e-99);
+    a.zwrate[z] = zwrate;
+    return fabs((zvol - zvol0) / zvol0);
+}
+
+// The persistent pass C: CTA b walks tiles b, b + gridDim.x, ...; writes
+// its maximum |dV/V0| and inverted-side count to part_dvov / part_badC
+// [blockIdx.x] (gridDim.x partials).
+template <bool kQuads, bool kMixed>
+__device__ __forceinline__ void pass_c_tiles(const DevArrays& a, const HydroConst& c, unsigned char* smem,
+                                             double& dvm, int& nbad) {
+    const Ctl* ctl = a.ctl;
+    const int cur = ctl->cycle & 1;
+    const double dt = ctl->dt, dtinv = ctl->dtinv;
+    const int t = threadIdx.x;
+    const int64_t ntiles = ((int64_t)a.numz + kTile - 1) / kTile;
+    const int64_t step = gridDim.x;
+    int64_t tile = blockIdx.x;
+    constexpr int kAhead = kStages - 1;
+    // prologue: tiles 0 .. kAhead-1 of this CTA in flight
+#pragma unroll
+    for (int j = 0; j < kAhead; ++j) {
+        const int64_t tj = tile + j * step;
+        if (tj < ntiles) {
+            const int64_t z = tj * kTile + t;
+            issue(a, cur, smem + j * kStageBytes, t, z, load_idx<kQuads>(a, z));
+        }
+        commit();
+    }
+    ZoneIdx nix{};
+    {
+        const int64_t tn = tile + kAhead * step;
+        if (kQuads && tn < ntiles) nix = load_idx<kQuads>(a, tn * kTile + t);
+    }
+    for (int j = 0; tile < ntiles; ++j, tile += step) {
+        // tile j + kAhead into the stage tile j - 1 used
+        const int64_t ti = tile + kAhead * step;
+        if (ti < ntiles) {
+            const int64_t z = ti * kTile + t;
+            if (!kQuads) nix = load_idx<kQuads>(a, z);
+            issue(a, cur, smem + ((j + kAhead) % kStages) * kStageBytes, t, z, nix);
+        }
+        commit();
+        if (kQuads) {
+            const int64_t tn = ti + step;
+            if (tn < ntiles) nix = load_idx<kQuads>(a, tn * kTile + t);
+        }
+        wait_groups<kAhead>();   // this thread's copies of tile j have landed
+        const int64_t z = tile * kTile + t;
+        if (z < a.numz) {
+            const double d = zone<kQuads, kMixed>(a, c, smem + (j % kStages) * kStageBytes, t, z, dt, dtinv, nbad);
+            dvm = (d > dvm) ? d : dvm;
+        }
+    }
+    wait_groups<0>();
+}
+
+// Raises kernel k's dynamic shared-memory limit to kSmemBytes and returns
+// its persistent grid: resident CTAs per SM x nsm, at most one per tile.
+template <typename K>
+inline cudaError_t prepare(K k, int32_t numz, int nsm, int32_t* grid) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    if (e != cudaSuccess) return e;
+    int occ = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kTile, kSmemBytes);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) return cudaErrorInvalidConfiguration;
+    const int64_t ntiles = ((int64_t)numz + kTile - 1) / kTile;
+    int64_t g = (int64_t)occ * nsm;
+    if (g > ntiles) g = ntiles;
+    *grid = (int32_t)(g < 1 ? 1 : g);
+    return cudaSuccess;
+}
+
+// Block sum of a per-thread count (called by every thread of the block).
+template <int kThreads>
+__device__ __forceinline__ int block_isum(int v) {
+    __shared__ int ws[kThreads / 32];
+    v = (int)__reduce_add_sync(0xffffffffu, (unsigned)v);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+    __syncthreads();
+    int s = 0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) s += ws[w];
+    return s;
+}
+
+}  // namespace stagedc
+}  // namespace pnt
