@@ -7,14 +7,17 @@
 // uneven size share the GPU without a launch per mesh, and instances that
 // are done are skipped tile by tile.  The per-zone and per-point
 // arithmetic is the FP64 body shared with the single-mesh kernels
-// (hydro_fp64_body.cuh), so every instance is bit-identical to its own
-// single-mesh run; tiles only change which CTA does the work.  The batch
+// (pass A: pass_a_zone_thread of hydro_fp64_body.cuh, one thread per zone;
+// pass C: the staged corrector of pass_c_staged.cuh), so every instance is
+// bit-identical to its own single-mesh run; tiles only change which CTA
+// does the work.  The batch
 // cycle is captured in a CUDA graph.  Tile size and CTAs per SM are picked
 // by pnt_batch_tune, which times candidate shapes on the run's own cycles
 // (the results do not depend on the shape).
 //
 // Compiled with -fmad=false (FP64 parity).
 #include "hydro_fp64_body.cuh"
+#include "pass_c_staged.cuh"
 #include "pnt_internal.h"
 
 #include <algorithm>
@@ -49,13 +52,15 @@ struct BatchDev {
     int32_t ninst;
 };
 
-constexpr int kBatchThreads = 256;          // 64 zones x 4 side lanes, or 256 points
-constexpr int kZonesPerIter = kBatchThreads / 4;
+constexpr int kBatchThreads = 256;          // points per point-pass iteration; finalize warps
+constexpr int kBatchZT = 128;               // pass A: one zone per thread
+constexpr int kZonesPerIter = 64;           // zone tiles are whole multiples of this
 
 __device__ __forceinline__ bool inst_skip(const Ctl& ctl) { return ctl.done || ctl.cycle >= ctl.stop_at; }
 
-template <bool kPassA>
-__global__ void __launch_bounds__(kBatchThreads, 3) batch_zone_pass(BatchDev b) {
+// Pass A: one thread per zone (pass_a_zone_thread), 128 zones per step
+// through the tile; one partial per tile.
+__global__ void __launch_bounds__(kBatchZT, 3) batch_pass_a(BatchDev b) {
     for (int t = blockIdx.x; t < b.nztiles; t += gridDim.x) {
         const Tile tile = b.ztiles[t];
         const Ctl& ctl = b.ctls[tile.inst];
@@ -63,33 +68,64 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_zone_pass(BatchDev b) 
         const HydroConst& c = b.consts[tile.inst];
         const int cur = ctl.cycle & 1;
         const double dt = ctl.dt;
-        double fold = kPassA ? 1.e99 : 1.e-99;
+        double fold = 1.e99;
         int nbad = 0;
-        for (int zb = tile.beg; zb < tile.end; zb += kZonesPerIter) {
-            const int64_t z = (int64_t)zb + (threadIdx.x >> 2);
-            const int k = threadIdx.x & 3;
-            const bool zok = z < tile.end;
-            double v;
-            bool bad;
-            if (kPassA) {
-                if (tile.quads) pass_a_zone<true>(b.a, c, cur, dt, z, k, threadIdx.x & 31, zok, v, bad);
-                else pass_a_zone<false>(b.a, c, cur, dt, z, k, threadIdx.x & 31, zok, v, bad);
-                fold = dmin(fold, v);
+        for (int zb = tile.beg; zb < tile.end; zb += kBatchZT) {
+            const int64_t z = (int64_t)zb + threadIdx.x;
+            if (z >= tile.end) continue;
+            double v = 1.e99;
+            if (tile.quads) {
+                pass_a_zone_thread<4>(b.a, c, cur, dt, z, 4 * z, v, nbad);
             } else {
-                if (tile.quads) pass_c_zone<true>(b.a, c, cur, dt, ctl.dtinv, z, k, threadIdx.x & 31, zok, v, bad);
-                else pass_c_zone<false>(b.a, c, cur, dt, ctl.dtinv, z, k, threadIdx.x & 31, zok, v, bad);
-                fold = (v > fold) ? v : fold;
+                const int n = b.a.znump[z];
+                const int64_t s0 = b.a.zfirst[z];
+                if (n == 4) pass_a_zone_thread<4>(b.a, c, cur, dt, z, s0, v, nbad);
+                else pass_a_zone_thread<3>(b.a, c, cur, dt, z, s0, v, nbad);
             }
-            nbad += __syncthreads_count(bad);
+            fold = dmin(fold, v);
         }
-        if (kPassA) {
-            block_fold<true, kBatchThreads>(fold, b.a.part_dtnew + t);
-            if (threadIdx.x == 0) b.a.part_badA[t] = nbad;
-        } else {
-            block_fold<false, kBatchThreads>(fold, b.a.part_dvov + t);
-            if (threadIdx.x == 0) b.a.part_badC[t] = nbad;
+        nbad = tiles::block_isum<kBatchZT>(nbad);
+        block_fold<true, kBatchZT>(fold, b.a.part_dtnew + t);
+        if (threadIdx.x == 0) b.a.part_badA[t] = nbad;
+        __syncthreads();   // the reductions' shared slots are reused by the next tile
+    }
+}
+
+// Pass C: the staged corrector of pass_c_staged.cuh, one stage, its
+// kTile zones per step through the tile (copies issued, waited for,
+// computed); one partial per tile.
+__global__ void __launch_bounds__(stagedc::kTile) batch_pass_c(BatchDev b) {
+    extern __shared__ __align__(16) unsigned char smem_c[];
+    const int th = threadIdx.x;
+    for (int t = blockIdx.x; t < b.nztiles; t += gridDim.x) {
+        const Tile tile = b.ztiles[t];
+        const Ctl& ctl = b.ctls[tile.inst];
+        if (inst_skip(ctl)) continue;   // uniform over the CTA
+        const HydroConst& c = b.consts[tile.inst];
+        const int cur = ctl.cycle & 1;
+        const double dt = ctl.dt, dtinv = ctl.dtinv;
+        double dvm = 1.e-99;
+        int nbad = 0;
+        for (int zb = tile.beg; zb < tile.end; zb += stagedc::kTile) {
+            const int64_t z = (int64_t)zb + th;
+            const bool zok = z < tile.end;
+            if (zok) {
+                const tiles::ZoneIdx ix =
+                    tile.quads ? tiles::load_idx<true>(b.a, z) : tiles::load_idx<false>(b.a, z);
+                stagedc::issue(b.a, cur, smem_c, th, z, ix);
+            }
+            tiles::commit();
+            tiles::wait_groups<0>();
+            if (zok) {
+                const double d = tile.quads ? stagedc::zone<true, false>(b.a, c, smem_c, th, z, dt, dtinv, nbad)
+                                            : stagedc::zone<false, false>(b.a, c, smem_c, th, z, dt, dtinv, nbad);
+                dvm = (d > dvm) ? d : dvm;
+            }
         }
-        __syncthreads();   // block_fold's shared slots are reused by the next tile
+        nbad = tiles::block_isum<stagedc::kTile>(nbad);
+        block_fold<false, stagedc::kTile>(dvm, b.a.part_dvov + t);
+        if (threadIdx.x == 0) b.a.part_badC[t] = nbad;
+        __syncthreads();
     }
 }
 
@@ -182,6 +218,7 @@ struct pnt_batch {
     int* running_host = nullptr;                 // pinned
     Shape shape{256, 3};
     int nsm = 148;
+    int grid_c = 148;                            // resident pass C CTAs (occupancy x SMs)
     // device tile lists (rebuilt when the shape changes)
     Tile* ztiles = nullptr;
     Tile* ptiles = nullptr;
@@ -275,11 +312,11 @@ struct pnt_batch {
         const int grid_p = std::max(1, std::min(b.nptiles, nsm * 4));
         const int grid_f = (ninst * 32 + kBatchThreads - 1) / kBatchThreads;
         if (ev) cudaEventRecord(ev[0], stream);
-        batch_zone_pass<true><<<grid_z, kBatchThreads, 0, stream>>>(b);
+        batch_pass_a<<<grid_z, kBatchZT, 0, stream>>>(b);
         if (ev) cudaEventRecord(ev[1], stream);
         batch_point_pass<<<grid_p, kBatchThreads, 0, stream>>>(b);
         if (ev) cudaEventRecord(ev[2], stream);
-        batch_zone_pass<false><<<grid_z, kBatchThreads, 0, stream>>>(b);
+        batch_pass_c<<<std::max(1, std::min(b.nztiles, grid_c)), stagedc::kTile, stagedc::kSmemBytes, stream>>>(b);
         if (ev) cudaEventRecord(ev[3], stream);
         batch_finalize<<<grid_f, kBatchThreads, 0, stream>>>(b);
         if (ev) cudaEventRecord(ev[4], stream);
@@ -500,7 +537,7 @@ pnt_status pnt_batch_create(const pnt_mesh* const* meshes, const pnt_params* par
         Ctl* d_ctls;
         if ((st = bt->alloc(&d_zfirst, NZ)) || (st = bt->alloc(&d_znump, NZ)) || (st = bt->alloc(&d_mapsp1, NS)) ||
             (st = bt->alloc(&d_smf, NS)) || (st = bt->alloc(&d_poff, NP + 1)) || (st = bt->alloc(&d_pcorner, NS)) ||
-            (st = bt->alloc(&d_mask, NP)) || (st = bt->alloc(&a.px[0], NP)) || (st = bt->alloc(&a.px[1], NP)) ||
+            (st = bt->alloc(&d_mask, NP + 2)) || (st = bt->alloc(&a.px[0], NP)) || (st = bt->alloc(&a.px[1], NP)) ||
             (st = bt->alloc(&a.pu[0], NP)) || (st = bt->alloc(&a.pu[1], NP)) || (st = bt->alloc(&a.zm, NZ)) ||
             (st = bt->alloc(&a.zr, NZ)) || (st = bt->alloc(&a.ze, NZ)) || (st = bt->alloc(&a.zetot, NZ)) ||
             (st = bt->alloc(&a.zwrate, NZ)) || (st = bt->alloc(&a.zvol, NZ)) || (st = bt->alloc(&a.zp, NZ)) ||
@@ -537,6 +574,16 @@ pnt_status pnt_batch_create(const pnt_mesh* const* meshes, const pnt_params* par
                 ;
         }
         if (e == cudaSuccess) e = cudaMemset(a.zp, 0, NZ * 8);
+        if (e == cudaSuccess) e = cudaMemset(d_mask + NP, 0, 4);   // pass C copies 32-bit mask words
+        if (e == cudaSuccess) {
+            // the staged pass C: its shared-memory limit and resident CTAs per SM
+            e = cudaFuncSetAttribute(batch_pass_c, cudaFuncAttributeMaxDynamicSharedMemorySize, stagedc::kSmemBytes);
+            int occ = 0;
+            if (e == cudaSuccess)
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pass_c, stagedc::kTile, stagedc::kSmemBytes);
+            if (e == cudaSuccess && occ < 1) e = cudaErrorInvalidConfiguration;
+            bt->grid_c = bt->nsm * std::max(occ, 1);
+        }
         if (e != cudaSuccess) {
             delete bt;
             return fail(PNT_ERR_CUDA, "batch setup: %s", cudaGetErrorString(e));

@@ -34,6 +34,7 @@
 // batched kernels); this file is compiled with -fmad=false, so the results
 // match a serial CPU run of the reference bit for bit.
 #include "hydro_fp64_body.cuh"
+#include "zone_tiles.cuh"
 
 namespace pnt {
 namespace {
@@ -51,7 +52,7 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_PASS_A_ZT_MIN_BLOCKS) pass
     if (skip_cycle(ctl)) return;
     const int64_t z = (int64_t)blockIdx.x * kZoneThreadsZT + threadIdx.x;
     double zdthyd = 1.e99;
-    bool bad = false;
+    int bad = 0;
     if (z < a.numz) {
         const int cur = ctl->cycle & 1;
         const double dt = ctl->dt;
@@ -64,7 +65,7 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_PASS_A_ZT_MIN_BLOCKS) pass
             else pass_a_zone_thread<3>(a, c, cur, dt, z, s0, zdthyd, bad);
         }
     }
-    const int nbad = __syncthreads_count(bad);
+    const int nbad = tiles::block_isum<kZoneThreadsZT>(bad);
     if (blockIdx.x >= (unsigned)a.npartA) return;   // partials are sized for this grid
     block_fold<true, kZoneThreadsZT>(zdthyd, a.part_dtnew + blockIdx.x);
     if (threadIdx.x == 0) a.part_badA[blockIdx.x] = nbad;

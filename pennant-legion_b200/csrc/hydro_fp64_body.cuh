@@ -292,11 +292,12 @@ __device__ __forceinline__ void pass_a_zone(const DevArrays& a, const HydroConst
 // Pass A, one thread per zone of N sides (N = 3 or 4, static so the side
 // arrays stay in registers): the arithmetic of pass_a_zone, side by side in
 // the zone's side order, so zone sums keep the reference's serial order and
-// every zone-level quantity is formed once.
+// every zone-level quantity is formed once.  nbad counts the zone's
+// inverted sides (checkBadSides counts sides, Mesh.cc:1531-1550).
 // ---------------------------------------------------------------------
 template <int N>
 __device__ __forceinline__ void pass_a_zone_thread(const DevArrays& a, const HydroConst& c, int cur, double dt,
-                                                   int64_t z, int64_t s0, double& zdthyd, bool& bad) {
+                                                   int64_t z, int64_t s0, double& zdthyd, int& nbad) {
     const double2* __restrict__ px0 = a.px[cur];
     const double2* __restrict__ pu0 = a.pu[cur];
     double2 xp[N], u0[N];
@@ -325,7 +326,6 @@ __device__ __forceinline__ void pass_a_zone_thread(const DevArrays& a, const Hyd
     const double fac = (N == 3 ? 3. : 4.);
     double sa[N], elen[N], rinv[N];
     double zareap = 0., zvolp = 0., zdl = 1.e99;
-    bad = false;
 #pragma unroll
     for (int k = 0; k < N; ++k) {
         const int nk = (k + 1 == N) ? 0 : k + 1;
@@ -333,7 +333,7 @@ __device__ __forceinline__ void pass_a_zone_thread(const DevArrays& a, const Hyd
         const double sv = third * sa[k] * (xp[k].x + xp[nk].x + zxp.x);
         zareap = (k == 0) ? __dadd_rn(0.0, sa[k]) : zareap + sa[k];
         zvolp = (k == 0) ? __dadd_rn(0.0, sv) : zvolp + sv;
-        bad = bad || (sv <= 0.);
+        nbad += (sv <= 0.) ? 1 : 0;
         elen[k] = length(sub(xp[nk], xp[k]));
         rinv[k] = 1. / elen[k];
     }

@@ -29,6 +29,7 @@
 // error against the FP64 run (tests/test_gpu_mixed.py).
 #include "closure_dev.cuh"
 #include "hydro_dev.h"
+#include "zone_tiles.cuh"
 
 #include <cuda_runtime.h>
 
@@ -176,11 +177,11 @@ __device__ __forceinline__ void qcs_sfq_fp64_zone(const DevArrays& a, const Hydr
     }
 }
 
-// cnt[3]: this zone's corners without compression, in the dead zone, in an
-// acute zone (learned cycle).
+// nbad counts the zone's inverted sides; cnt[3]: its corners without
+// compression, in the dead zone, in an acute zone (learned cycle).
 template <int N, bool kLearned>
 __device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const HydroConst& c, int cur, double dt,
-                                                  int64_t z, int64_t s0, double& zdthyd, bool& bad, int* cnt) {
+                                                  int64_t z, int64_t s0, double& zdthyd, int& nbad, int* cnt) {
     const double2* __restrict__ px0 = a.px[cur];
     const double2* __restrict__ pu0 = a.pu[cur];
     double2 xp[N];
@@ -212,7 +213,6 @@ __device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const Hydr
     const double third = 1. / 3.;
     double sa[N];
     double zareap = 0., zvolp = 0.;
-    bad = false;
 #pragma unroll
     for (int k = 0; k < N; ++k) {
         const int nk = (k + 1 == N) ? 0 : k + 1;
@@ -220,7 +220,7 @@ __device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const Hydr
         const double sv = third * sa[k] * (xp[k].x + xp[nk].x + zxp.x);
         zareap = (k == 0) ? sa[k] : zareap + sa[k];
         zvolp = (k == 0) ? sv : zvolp + sv;
-        bad = bad || (sv <= 0.);
+        nbad += (sv <= 0.) ? 1 : 0;
     }
     // FP64 zone EOS and density (PolyGas.cc:63-109, Hydro.cc:1034-1054)
     const double e = dmax(ze, 0.);
@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_MIXED_ZT_MIN_BLOCKS) pass_
     if (skip_cycle(ctl)) return;
     const int64_t z = (int64_t)blockIdx.x * kZoneThreadsZT + threadIdx.x;
     double zdthyd = 1.e99;
-    bool bad = false;
+    int bad = 0;
     int cnt[3] = {0, 0, 0};
     if (z < a.numz) {
         const int cur = ctl->cycle & 1;
@@ -450,7 +450,7 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_MIXED_ZT_MIN_BLOCKS) pass_
             if ((threadIdx.x & 31) == 0) wcount[threadIdx.x >> 5][q] = t;
         }
     }
-    const int nbad = __syncthreads_count(bad);
+    const int nbad = tiles::block_isum<kZoneThreadsZT>(bad);   // its barrier also orders wcount
     if constexpr (kLearned) {
         constexpr int kCounted[3] = {kClassZero, kClassDead, kClassAcute};
         if (threadIdx.x < 3) {

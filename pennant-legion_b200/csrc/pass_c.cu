@@ -19,7 +19,7 @@ __global__ void __launch_bounds__(stagedc::kTile) pass_c_staged(DevArrays a, Hyd
     double dvm = 1.e-99;
     int nbad = 0;
     stagedc::pass_c_tiles<kQuads, kMixed>(a, c, smem_c, dvm, nbad);
-    const int nb = stagedc::block_isum<stagedc::kTile>(nbad);
+    const int nb = tiles::block_isum<stagedc::kTile>(nbad);
     fp64::block_fold<false, stagedc::kTile>(dvm, a.part_dvov + blockIdx.x);
     if (threadIdx.x == 0) a.part_badC[blockIdx.x] = nb;
 }
@@ -34,7 +34,7 @@ Kernel pick_kernel(bool mixed, bool quads) {
 }  // namespace
 
 cudaError_t prepare_pass_c(bool mixed, bool quads, int32_t numz, int nsm, int32_t* grid) {
-    return stagedc::prepare(pick_kernel(mixed, quads), numz, nsm, grid);
+    return tiles::prepare(pick_kernel(mixed, quads), stagedc::kTile, stagedc::kSmemBytes, numz, nsm, grid);
 }
 
 void launch_pass_c(const DevArrays& a, const HydroConst& c, bool mixed, cudaStream_t stream) {

@@ -5,21 +5,13 @@
 //
 // Pass C reads, per side, the start-of-cycle and new position and velocity
 // of the side's first point (a gather through mapsp1) and the side's sfp +
-// sfq, and per zone four scalars.  Loaded straight into registers this is a
-// chain of two dependent memory latencies per zone (index, then points)
-// with few loads in flight, and four lanes per zone add ~36 shuffles per
-// lane: that kernel ran at 31% of peak DRAM throughput.  Here each CTA walks
-// its tiles of kTile zones, one thread per zone: a thread issues all the
-// asynchronous copies (`cp.async`, global -> shared, no registers held) of
-// its zone's inputs at once, with the point indices already in registers
-// (loaded one tile ahead), waits for them and computes the zone from shared
-// memory.  kStages > 1 keeps kStages - 1 further tiles in flight during the
-// compute; on the B200 more resident CTAs beat deeper pipelines (1024^2
+// sfq, and per zone four scalars.  Loaded straight into registers by four
+// lanes per zone (a chain of two dependent memory latencies, ~36 shuffles
+// per lane) it ran at 31% of peak DRAM throughput; here the zone-tile
+// driver of zone_tiles.cuh stages them in shared memory, one thread per
+// zone.  On the B200 more resident CTAs beat deeper pipelines (1024^2
 // Sedov: 1 stage and 10 CTAs of 64 per SM 56 us, 2 stages 59 us, 3 stages
-// 72 us), so the default is one stage.  A thread copies and reads only its
-// own zone's slots (structure-of-arrays across the tile's threads, so
-// shared-memory accesses are conflict-free), so `cp.async.wait_group` alone
-// orders them; no block barrier inside the loop.
+// 72 us), so the default is one stage.
 //
 // The zone arithmetic is the four-lane pass C's, one zone per thread:
 // kMixed = false keeps the reference's serial side order and operation
@@ -29,7 +21,7 @@
 // work).
 #pragma once
 
-#include "hydro_dev.h"
+#include "zone_tiles.cuh"
 
 #include <cuda_runtime.h>
 
@@ -60,58 +52,17 @@ constexpr int kOffMeta = kOffZs + 4 * 8 * kTile;
 constexpr int kStageBytes = kOffMeta + 4 * kTile;
 constexpr int kSmemBytes = kStages * kStageBytes;
 
-__device__ __forceinline__ unsigned saddr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void cp16(void* s, const void* g) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr(s)), "l"(g) : "memory");
-}
-__device__ __forceinline__ void cp8(void* s, const void* g) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(saddr(s)), "l"(g) : "memory");
-}
-__device__ __forceinline__ void cp4(void* s, const void* g) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(saddr(s)), "l"(g) : "memory");
-}
-__device__ __forceinline__ void commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void wait_groups() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// Where one zone's inputs live: its first side, side count and point indices.
-struct ZoneIdx {
-    int4 p;
-    int32_t s0;
-    int32_t n;
-};
-
-template <bool kQuads>
-__device__ __forceinline__ ZoneIdx load_idx(const DevArrays& a, int64_t z) {
-    ZoneIdx r{make_int4(0, 0, 0, 0), 0, 0};
-    if (z >= a.numz) return r;
-    if (kQuads) {
-        r.s0 = (int32_t)(4 * z);
-        r.n = 4;
-        r.p = __ldg(reinterpret_cast<const int4*>(a.mapsp1) + z);
-    } else {
-        r.s0 = a.zfirst[z];
-        r.n = a.znump[z];
-        r.p.x = a.mapsp1[r.s0];
-        r.p.y = a.mapsp1[r.s0 + 1];
-        r.p.z = a.mapsp1[r.s0 + 2];
-        r.p.w = r.n == 4 ? a.mapsp1[r.s0 + 3] : 0;
-    }
-    return r;
-}
-
-__device__ __forceinline__ int pick(const int4& v, int k) {
-    return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
-}
+using tiles::cp16;
+using tiles::cp4;
+using tiles::cp8;
+using tiles::ZoneIdx;
+using tiles::pick;
 
 // Issues the copies of zone z's inputs into slot t of stage st.  bcmask is
 // 16-bit per point; its 32-bit word is copied (the buffer is padded to a
 // whole word) and the point's parity kept in the zone's meta word.
 __device__ __forceinline__ void issue(const DevArrays& a, int cur, unsigned char* st, int t, int64_t z,
                                       const ZoneIdx& ix) {
-    if (z >= a.numz) return;
     const double2* px0 = a.px[cur];
     const double2* pu0 = a.pu[cur];
     const double2* px1 = a.px[cur ^ 1];
@@ -238,9 +189,8 @@ __device__ __forceinline__ double zone(const DevArrays& a, const HydroConst& c, 
     return fabs((zvol - zvol0) / zvol0);
 }
 
-// The persistent pass C: CTA b walks tiles b, b + gridDim.x, ...; writes
-// its maximum |dV/V0| and inverted-side count to part_dvov / part_badC
-// [blockIdx.x] (gridDim.x partials).
+// The persistent pass C over the CTA's tiles: the maximum |dV/V0| into
+// dvm, the inverted sides into nbad.
 template <bool kQuads, bool kMixed>
 __device__ __forceinline__ void pass_c_tiles(const DevArrays& a, const HydroConst& c, unsigned char* smem,
                                              double& dvm, int& nbad) {
@@ -248,76 +198,14 @@ __device__ __forceinline__ void pass_c_tiles(const DevArrays& a, const HydroCons
     const int cur = ctl->cycle & 1;
     const double dt = ctl->dt, dtinv = ctl->dtinv;
     const int t = threadIdx.x;
-    const int64_t ntiles = ((int64_t)a.numz + kTile - 1) / kTile;
-    const int64_t step = gridDim.x;
-    int64_t tile = blockIdx.x;
-    constexpr int kAhead = kStages - 1;
-    // prologue: tiles 0 .. kAhead-1 of this CTA in flight
-#pragma unroll
-    for (int j = 0; j < kAhead; ++j) {
-        const int64_t tj = tile + j * step;
-        if (tj < ntiles) {
-            const int64_t z = tj * kTile + t;
-            issue(a, cur, smem + j * kStageBytes, t, z, load_idx<kQuads>(a, z));
-        }
-        commit();
-    }
-    ZoneIdx nix{};
-    {
-        const int64_t tn = tile + kAhead * step;
-        if (kQuads && tn < ntiles) nix = load_idx<kQuads>(a, tn * kTile + t);
-    }
-    for (int j = 0; tile < ntiles; ++j, tile += step) {
-        // tile j + kAhead into the stage tile j - 1 used
-        const int64_t ti = tile + kAhead * step;
-        if (ti < ntiles) {
-            const int64_t z = ti * kTile + t;
-            if (!kQuads) nix = load_idx<kQuads>(a, z);
-            issue(a, cur, smem + ((j + kAhead) % kStages) * kStageBytes, t, z, nix);
-        }
-        commit();
-        if (kQuads) {
-            const int64_t tn = ti + step;
-            if (tn < ntiles) nix = load_idx<kQuads>(a, tn * kTile + t);
-        }
-        wait_groups<kAhead>();   // this thread's copies of tile j have landed
-        const int64_t z = tile * kTile + t;
-        if (z < a.numz) {
-            const double d = zone<kQuads, kMixed>(a, c, smem + (j % kStages) * kStageBytes, t, z, dt, dtinv, nbad);
-            dvm = (d > dvm) ? d : dvm;
-        }
-    }
-    wait_groups<0>();
-}
-
-// Raises kernel k's dynamic shared-memory limit to kSmemBytes and returns
-// its persistent grid: resident CTAs per SM x nsm, at most one per tile.
-template <typename K>
-inline cudaError_t prepare(K k, int32_t numz, int nsm, int32_t* grid) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
-    if (e != cudaSuccess) return e;
-    int occ = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kTile, kSmemBytes);
-    if (e != cudaSuccess) return e;
-    if (occ < 1) return cudaErrorInvalidConfiguration;
-    const int64_t ntiles = ((int64_t)numz + kTile - 1) / kTile;
-    int64_t g = (int64_t)occ * nsm;
-    if (g > ntiles) g = ntiles;
-    *grid = (int32_t)(g < 1 ? 1 : g);
-    return cudaSuccess;
-}
-
-// Block sum of a per-thread count (called by every thread of the block).
-template <int kThreads>
-__device__ __forceinline__ int block_isum(int v) {
-    __shared__ int ws[kThreads / 32];
-    v = (int)__reduce_add_sync(0xffffffffu, (unsigned)v);
-    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
-    __syncthreads();
-    int s = 0;
-#pragma unroll
-    for (int w = 0; w < kThreads / 32; ++w) s += ws[w];
-    return s;
+    tiles::for_tiles<kQuads, kTile, kStages, kStageBytes>(
+        a, smem, [&](unsigned char* st, int64_t z, const ZoneIdx& ix) { issue(a, cur, st, t, z, ix); },
+        [&](const unsigned char* st, int64_t z) {
+            if (z < a.numz) {
+                const double d = zone<kQuads, kMixed>(a, c, st, t, z, dt, dtinv, nbad);
+                dvm = (d > dvm) ? d : dvm;
+            }
+        });
 }
 
 }  // namespace stagedc
