@@ -37,7 +37,7 @@ namespace {
 using namespace fp64;
 
 // ----------------------------------------------------------------------
-// Harvest (FP64, the arithmetic of pass_a_zone)
+// Harvest (FP64, the arithmetic of pass A, four lanes per zone)
 // ----------------------------------------------------------------------
 struct HarvestArgs {
     double dead, qa, qb;

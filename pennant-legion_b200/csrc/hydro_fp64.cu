@@ -18,15 +18,12 @@
 // Pass A runs one thread per zone (pass_a_zone_thread): the zone's sides
 // in the reference's side order, each zone-level quantity (centre, sums,
 // EOS) formed once, 4-way independent corner work for latency hiding, no
-// shuffles; 168 registers, 3 blocks of 128 per SM (13% faster than the
-// four-lanes-per-zone form pass_a_zone at a developed 1024^2 Sedov state;
+// shuffles; 168 registers, 3 blocks of 128 per SM (13% faster than four
+// lanes per zone at a developed 1024^2 Sedov state;
 // it is bound by the ~50 correctly rounded FP64 divisions and square roots
 // of a zone).  Pass C is the persistent staged kernel of pass_c.cu (one
 // thread per zone, inputs gathered into shared memory by asynchronous
-// copies).  The batched kernels keep four lanes per zone: one lane per
-// side/corner, zone-local side data moved by warp shuffles, zone sums formed
-// by every lane in the serial side order, zone quotients split over the
-// lanes.  1/elen is formed
+// copies); the batched kernels run the same two bodies.  1/elen is formed
 // once per side and shared with the neighbouring corner; QCS terms the
 // reference computes and then discards (evol and du unless cdiv < 0, zkur
 // when cdiv > 0) are not computed, which leaves every stored value

@@ -1,13 +1,14 @@
-// hydro_fp64_body.cuh -- the FP64 hydro cycle, one zone lane / point at a
-// time, shared by the single-mesh kernels (hydro_fp64.cu) and the batched
-// persistent kernels (batch.cu) so both run exactly the same arithmetic.
+// hydro_fp64_body.cuh -- the FP64 hydro cycle's pass A zone body (one
+// thread per zone), pass B point body and end-of-cycle step, shared by the
+// single-mesh kernels (hydro_fp64.cu) and the batched persistent kernels
+// (batch.cu) so both run exactly the same arithmetic; pass C's body is in
+// pass_c_staged.cuh.  The four-lane helpers (zsum, shfl2) serve the
+// closure harvest (closure.cu), whose four consecutive lanes form a zone.
 //
 // Every expression keeps the reference's operation order, including
 // Vec2.hh's `v / r` = v * (1/r) (Vec2.hh:145-149); translation units that
 // include this header are compiled with -fmad=false, so results match a
-// serial CPU run of the reference bit for bit.  Zone bodies must be called
-// by all 32 lanes of a warp together (they exchange values by shuffles);
-// four consecutive lanes form a zone.
+// serial CPU run of the reference bit for bit.
 #pragma once
 
 #include "hydro_dev.h"
@@ -57,32 +58,8 @@ __device__ __forceinline__ double zsum(double v, int g, int n) {
     if (n == 4) s = s + d;
     return s;
 }
-__device__ __forceinline__ double zsum_from(double init, double v, int g, int n) {
-    const double a = shfl(v, g), b = shfl(v, g + 1), c = shfl(v, g + 2), d = shfl(v, g + 3);
-    double s = init + a;
-    s = s + b;
-    s = s + c;
-    if (n == 4) s = s + d;
-    return s;
-}
 __device__ __forceinline__ double2 zsum2(double2 v, int g, int n) {
     return mk(zsum(v.x, g, n), zsum(v.y, g, n));
-}
-__device__ __forceinline__ double zmin_fold(double init, double v, int g, int n) {
-    const double a = shfl(v, g), b = shfl(v, g + 1), c = shfl(v, g + 2), d = shfl(v, g + 3);
-    double s = dmin(init, a);
-    s = dmin(s, b);
-    s = dmin(s, c);
-    if (n == 4) s = dmin(s, d);
-    return s;
-}
-__device__ __forceinline__ double zmax_fold(double init, double v, int g, int n) {
-    const double a = shfl(v, g), b = shfl(v, g + 1), c = shfl(v, g + 2), d = shfl(v, g + 3);
-    double s = dmax(init, a);
-    s = dmax(s, b);
-    s = dmax(s, c);
-    if (n == 4) s = dmax(s, d);
-    return s;
 }
 
 __device__ __forceinline__ bool skip_cycle(const Ctl* ctl) {
@@ -108,185 +85,6 @@ __device__ __forceinline__ void block_fold(double v, double* out) {
     }
 }
 
-
-// ---------------------------------------------------------------------
-// Pass A, one lane: side k of zone z (z valid iff zok).  Writes the side's
-// corner mass, corner force and sfp + sfq, and the zone's half-step
-// pressure; returns the zone's Courant dt and whether the side inverted.
-// ---------------------------------------------------------------------
-template <bool kQuads>
-__device__ __forceinline__ void pass_a_zone(const DevArrays& a, const HydroConst& c, int cur, double dt,
-                                            int64_t z, int k, int lane, bool zok, double& zdthyd, bool& bad) {
-    const double2* __restrict__ px0 = a.px[cur];
-    const double2* __restrict__ pu0 = a.pu[cur];
-    const int g = lane & ~3;
-    int n = 4;
-    int64_t s = 4 * z + k;
-    if (!kQuads) {
-        n = zok ? a.znump[z] : 4;
-        s = (zok ? (int64_t)a.zfirst[z] : 0) + k;
-    }
-    const bool act = zok && k < n;
-    const int lp = g + (k == 0 ? n - 1 : k - 1);   // lane of side mapss3[s]
-    const int ln = g + (k + 1 >= n ? 0 : k + 1);   // lane of side mapss4[s]
-
-    const int32_t p1 = act ? __ldg(a.mapsp1 + s) : 0;
-    const double2 x0 = act ? px0[p1] : mk(0., 0.);
-    const double2 u0 = act ? pu0[p1] : mk(0., 0.);
-    const double mf = act ? __ldg(a.smf + s) : 0.;
-    const double zm = zok ? a.zm[z] : 1.;
-    const double zr = zok ? a.zr[z] : 1.;
-    const double ze = zok ? a.ze[z] : 0.;
-    const double zwrate = zok ? a.zwrate[z] : 0.;
-    const double zvol0 = zok ? a.zvol[z] : 1.;
-
-    // advPosHalf (Hydro.cc:986-1006)
-    const double dth = 0.5 * dt;
-    const double2 xp = add(x0, smul(dth, u0));
-    const double2 xp2 = shfl2(xp, ln);   // pxp of mapsp2[s] = mapsp1[mapss4[s]]
-    const double2 u02 = shfl2(u0, ln);
-    const double rn = 1. / (double)n;    // px1 / n (Mesh.cc:835)
-
-    // calcCtrs (Mesh.cc:797-837)
-    const double2 zxp = zsum2(mk(xp.x * rn, xp.y * rn), g, n);
-    const double2 ex = smul(0.5, add(xp, xp2));
-    // calcVols (Mesh.cc:928-989)
-    const double third = 1. / 3.;
-    const double sa = 0.5 * cross(sub(xp2, xp), sub(zxp, xp));
-    const double sv = third * sa * (xp.x + xp2.x + zxp.x);
-    const double zareap = zsum(sa, g, n);
-    const double zvolp = zsum(sv, g, n);
-    bad = act && (sv <= 0.);
-    // calcSurfVecs (Mesh.cc:1104-1123), calcEdgeLen (:1151-1179)
-    const double2 ssurf = rotateCCW(sub(ex, zxp));
-    const double elen = length(sub(xp2, xp));
-    const double rinv_el = 1. / elen;       // shared by QCS cqe1/cqe2/sfq
-    // calcCharLen (Mesh.cc:1216-1244)
-    const double fac = (n == 3 ? 3. : 4.);
-    const double zdl = zmin_fold(1.e99, fac * sa / elen, g, n);
-    // PolyGas::calcStateHalf (PolyGas.cc:63-109) with calcRho: the four
-    // zone quotients are split over the zone's lanes (one division each)
-    const double e = dmax(ze, 0.);
-    const double p = c.gm1 * zr * e;
-    const double pre = c.gm1 * e;
-    const double per = c.gm1 * zr;
-    const double rA = ((k == 0) ? per * p : 1.) / ((k == 0) ? zr * zr : zm);
-    const double q = shfl(rA, g);            // per*p/(r*r)
-    const double minv = shfl(rA, g + 1);     // 1/zm
-    const double csqd = dmax(c.ssmin2, pre + q);
-    const double zss = sqrt(csqd);
-    const double dv = (zvolp - zvol0) * minv;
-    const double bulk = zr * csqd;
-    const double denom = 1. + 0.5 * per * dv;
-    const double src = zwrate * dth * minv;
-    const double rB = ((k == 0) ? zm : per * src - zr * bulk * dv) / ((k == 0) ? zvolp : denom);
-    const double zrp = shfl(rB, g);          // zm/zvolp
-    const double zp = p + shfl(rB, g + 1);
-
-    // calcCrnrMass (Hydro.cc:1083-1117)
-    const double mf3 = shfl(mf, lp);
-    if (act) a.cmass[s] = zrp * zareap * 0.5 * (mf + mf3);
-    if (zok && k == 0) a.zp[z] = zp;
-
-    // PolyGas::calcForce (PolyGas.cc:164-184)
-    const double2 sfp = smul(-zp, ssurf);
-    // TTS::calcForce (TTS.cc:55-104)
-    const double vfacinv = zareap / sa;
-    const double srho = zrp * mf * vfacinv;
-    double sstmp = dmax(zss, c.tts_ssmin);
-    sstmp = c.alfa * sstmp * sstmp;
-    const double sdp = sstmp * (srho - zrp);
-    const double2 sft = smul(-sdp, ssurf);
-
-    // QCS::setCornerDiv (QCS.cc:116-242); corner c = this side s2,
-    // s = mapss3[s2] is the previous lane.
-    const double2 zuc = zsum2(mk(u0.x * rn, u0.y * rn), g, n);
-    const double2 up0 = u0;                 // point p = mapsp2[s] = mapsp1[s2]
-    const double2 xq0 = xp;
-    const double2 upp = shfl2(u0, lp);      // pu0 at mapsp1[s]
-    const double2 up1 = smul(0.5, add(up0, u02));
-    const double2 xq1 = ex;                 // exp[s2]
-    const double2 up2 = zuc;
-    const double2 xq2 = zxp;
-    const double2 up3 = smul(0.5, add(upp, up0));
-    const double2 xq3 = shfl2(ex, lp);      // exp[s]
-    const double cvolume = 0.5 * cross(sub(xq2, xq0), sub(xq3, xq1));
-    const double2 v1 = sub(xq3, xq0);
-    const double2 v2 = sub(xq1, xq0);
-    const double de1 = shfl(elen, lp);      // elen[s]
-    const double rinv_de1 = shfl(rinv_el, lp);
-    const double de2 = elen;                // elen[s2]
-    const double minelen = dmin(de1, de2);
-    double ccos = ((minelen < 1.e-12) ? 0. : 4. * dot(v1, v2) / (de1 * de2));
-    const double cdiv = (cross(sub(up2, up0), sub(xq3, xq1)) - cross(sub(up3, up1), sub(xq2, xq0))) /
-                        (2.0 * cvolume);
-    // evol and du are kept by the reference only where cdiv < 0
-    double evol = 0., du = 0.;
-    if (cdiv < 0.0) {
-        const double2 dxx1 = smul(0.5, sub(sub(add(xq1, xq2), xq0), xq3));
-        const double2 dxx2 = smul(0.5, sub(sub(add(xq2, xq3), xq0), xq1));
-        const double dx1 = length(dxx1);
-        const double dx2 = length(dxx2);
-        const double2 duav = smul(0.25, add(add(add(up0, up1), up2), up3));
-        const double test1 = fabs(dot(dxx1, duav) * dx2);
-        const double test2 = fabs(dot(dxx2, duav) * dx1);
-        const double num = (test1 > test2 ? dx1 : dx2);
-        const double den = (test1 > test2 ? dx2 : dx1);
-        const double r = num / den;
-        evol = sqrt(4.0 * cvolume * r);
-        evol = dmin(evol, 2.0 * minelen);
-        const double dv1 = length2(sub(sub(add(up1, up2), up0), up3));
-        const double dv2 = length2(sub(sub(add(up2, up3), up0), up1));
-        du = sqrt(dmax(dv1, dv2));
-    }
-
-    // QCS::setQCnForce (QCS.cc:246-327): crmu is 0 wherever cdiv > 0
-    double crmu = 0.;
-    if (!(cdiv > 0.0)) {
-        const double ztmp2 = c.q2 * 0.25 * c.gammap1 * du;
-        const double ztmp1 = c.q1 * zss;
-        const double zkur = ztmp2 + sqrt(ztmp2 * ztmp2 + ztmp1 * ztmp1);
-        crmu = zkur * zrp * evol;
-    }
-    const double2 t1 = smul(crmu, sub(up0, upp));
-    const double2 cqe1 = mk(t1.x * rinv_de1, t1.y * rinv_de1);   // / elen[s]
-    const double2 t2 = smul(crmu, sub(u02, up0));
-    const double2 cqe2 = mk(t2.x * rinv_el, t2.y * rinv_el);     // / elen[s2]
-
-    // QCS::setForce (QCS.cc:331-380): side s uses corners s and mapss4[s]
-    const double csin2 = 1.0 - ccos * ccos;
-    const double cw = ((csin2 < 1.e-4) ? 0. : cvolume / csin2);
-    ccos = ((csin2 < 1.e-4) ? 0. : ccos);
-    const double cw2 = shfl(cw, ln);
-    const double ccos2 = shfl(ccos, ln);
-    const double2 cqe12 = shfl2(cqe1, ln);
-    const double2 cqe22 = shfl2(cqe2, ln);
-    const double2 fs = add(smul(cw, add(cqe2, smul(ccos, cqe1))), smul(cw2, add(cqe12, smul(ccos2, cqe22))));
-    const double2 sfq = mk(fs.x * rinv_el, fs.y * rinv_el);      // / elen[s]
-
-    // QCS::setVelDiff (QCS.cc:384-448)
-    const double2 dxs = sub(xp2, xp);
-    const double2 dus = sub(u02, u0);
-    double dux = dot(dus, dxs);
-    dux = (elen > 0. ? fabs(dux) / elen : 0.);
-    const double ztmp = zmax_fold(0., dux, g, n);
-    const double zdu = c.q1 * zss + 2. * c.q2 * ztmp;
-
-    // calcDtNew (Hydro.cc:1591-1619), per zone
-    const double cdu = dmax(zdu, dmax(zss, 1.e-99));
-    zdthyd = zok ? zdl * c.cfl / cdu : 1.e99;
-
-    // sumCrnrForce (Hydro.cc:1159-1193), side part: the corner force this
-    // side contributes to point mapsp1[s]
-    const double2 ftot = add(add(sfp, sfq), sft);
-    const double2 ftot3 = shfl2(ftot, lp);
-    const double2 cf = sub(ftot, ftot3);
-
-    if (act) {
-        a.cforce[s] = cf;
-        a.sftot[s] = add(sfp, sfq);
-    }
-}
 
 // ---------------------------------------------------------------------
 // Pass A, one thread per zone of N sides (N = 3 or 4, static so the side
@@ -500,80 +298,6 @@ __device__ __forceinline__ void pass_b_point(const DevArrays& a, const HydroCons
     const double2 x = add(x0, smul(dt * 0.5, add(u0, u)));
     a.px[cur ^ 1][p] = x;
     a.pu[cur ^ 1][p] = u;
-}
-
-// ---------------------------------------------------------------------
-// Pass C, one lane: returns |dV/V0| (on lane 2 of the zone; 1e-99 on the
-// others) and whether the side inverted.
-// ---------------------------------------------------------------------
-template <bool kQuads>
-__device__ __forceinline__ void pass_c_zone(const DevArrays& a, const HydroConst& c, int cur, double dt,
-                                            double dtinv, int64_t z, int k, int lane, bool zok, double& zdvov,
-                                            bool& bad) {
-    const int g = lane & ~3;
-    int n = 4;
-    int64_t s = 4 * z + k;
-    if (!kQuads) {
-        n = zok ? a.znump[z] : 4;
-        s = (zok ? (int64_t)a.zfirst[z] : 0) + k;
-    }
-    const bool act = zok && k < n;
-    const int ln = g + (k + 1 >= n ? 0 : k + 1);
-
-    const int32_t p1 = act ? __ldg(a.mapsp1 + s) : 0;
-    const double2 x0 = act ? a.px[cur][p1] : mk(0., 0.);
-    const double2 u0 = act ? a.pu[cur][p1] : mk(0., 0.);
-    const double2 x = act ? a.px[cur ^ 1][p1] : mk(0., 0.);
-    const double2 u = act ? a.pu[cur ^ 1][p1] : mk(0., 0.);
-    const unsigned mask = act ? a.bcmask[p1] : 0u;
-    const double2 sft = act ? a.sftot[s] : mk(0., 0.);
-    const double zm = zok ? a.zm[z] : 1.;
-    const double zetot0 = zok ? a.zetot[z] : 0.;
-    const double zvol0 = zok ? a.zvol[z] : 1.;
-    const double zp = zok ? a.zp[z] : 0.;
-
-    const double dth = 0.5 * dt;
-    const double2 xp = add(x0, smul(dth, u0));   // pxp, from pu0 before the BCs
-    double2 u0b = u0;                             // pu0 after applyFixedBC
-    if (mask) {
-        for (int b = 0; b < c.nbc; ++b)
-            if (mask & (1u << b)) u0b = project(u0b, c.vfix[b][0], c.vfix[b][1]);
-    }
-    const double2 x2 = shfl2(x, ln);
-    const double2 xp2 = shfl2(xp, ln);
-    const double2 u0b2 = shfl2(u0b, ln);
-    const double2 u2 = shfl2(u, ln);
-    const double rn = 1. / (double)n;
-
-    // calcCtrs + calcVols at the new positions (Mesh.cc:797-837, :928-989)
-    const double2 zx = zsum2(mk(x.x * rn, x.y * rn), g, n);
-    const double third = 1. / 3.;
-    const double sa = 0.5 * cross(sub(x2, x), sub(zx, x));
-    const double sv = third * sa * (x.x + x2.x + zx.x);
-    const double zvol = zsum(sv, g, n);
-    bad = act && (sv <= 0.);
-
-    // calcWork (Hydro.cc:1339-1406)
-    const double sd1 = dot(sft, add(u0b, u));
-    const double sd2 = dot(neg(sft), add(u0b2, u2));
-    const double dwork = -dth * (sd1 * xp.x + sd2 * xp2.x);
-    const double zetot = zsum_from(zetot0, dwork, g, n);
-    const double zw = zsum(dwork, g, n);
-    // calcWorkRate (Hydro.cc:1483-1510), calcEnergy (:1545-1564), calcRho (:1034-1054)
-    const double dvol = zvol - zvol0;
-    const double zwrate = (zw + zp * dvol) * dtinv;
-    // calcRho, calcEnergy and calcDvol (Hydro.cc:1622-1644) quotients, one
-    // per lane: lane 0 zr, lane 1 ze, lane 2 dV/V0
-    const double qv = ((k == 0) ? zm : (k == 1 ? zetot : zvol - zvol0)) /
-                      ((k == 0) ? zvol : (k == 1 ? zm + 1.e-99 : zvol0));
-    zdvov = (zok && k == 2) ? fabs(qv) : 1.e-99;
-
-    __syncwarp();   // every lane's zone loads precede the in-place stores
-    if (zok) {
-        if (k == 0) { a.zvol[z] = zvol; a.zr[z] = qv; }
-        else if (k == 1) { a.zetot[z] = zetot; a.ze[z] = qv; }
-        else if (k == 2) a.zwrate[z] = zwrate;
-    }
 }
 
 // ---------------------------------------------------------------------
