@@ -105,6 +105,41 @@ pnt_status pnt_mesh_point_corners(const pnt_mesh* mesh, const int32_t** offsets,
                                   const int32_t** sides);
 void pnt_mesh_destroy(pnt_mesh* mesh);
 
+/* Multi-piece runs: replaces the numpcs decomposition of Mesh(inp, numpcs)
+ * with its private, master and ghost points (Mesh.cc:211-241, :441-617).
+ * Piece `piece` of `npieces` (1-64) of a single-piece mesh is the zone range
+ * [numz*piece/npieces, numz*(piece+1)/npieces): its zones, their sides and
+ * every point they touch, numbered in global order, with the single-piece
+ * initial geometry.  For a piece mesh pnt_mesh_describe gives the local
+ * connectivity, and pnt_mesh_point_corners lists, per local point, local
+ * sides s < nums and halo slots nums + h merged in global side order: the
+ * halo slots hold corners of that point that other pieces own, so the
+ * corner sums at shared points keep the single-piece order.  A hydro object
+ * created from a piece steps with pnt_hydro_piece_* and exchanges halo
+ * corners with its neighbours every cycle. */
+pnt_status pnt_mesh_piece(const pnt_mesh* mesh, int32_t npieces, int32_t piece, pnt_mesh** out);
+
+typedef struct {
+    int32_t piece, npieces;
+    int32_t zone0;               /* global id of local zone 0 (local zones are contiguous) */
+    int32_t side0;               /* global id of local side 0 (local sides are contiguous) */
+    const int32_t* gpoint;       /* [nump] global id of each local point (NULL for one piece) */
+    int32_t nhalo;               /* halo corner slots after the nums local sides */
+    const int32_t* halo_side;    /* [nhalo] global side of each halo slot */
+    int32_t nnbr;                /* neighbour pieces (sharing points), ascending */
+    const int32_t* nbr;          /* [nnbr] */
+    /* recv_off[j] .. recv_off[j+1]: halo slots neighbour nbr[j] fills, in
+     * global side order; send_side[send_off[j] .. send_off[j+1]): local
+     * sides whose corner mass and force neighbour nbr[j] needs, in global
+     * side order (the same sides as its halo slots from this piece). */
+    const int32_t* recv_off;     /* [nnbr+1] */
+    const int32_t* send_off;     /* [nnbr+1] */
+    const int32_t* send_side;    /* [send_off[nnbr]] */
+} pnt_piece_desc;
+
+/* Pointers stay owned by the mesh. */
+pnt_status pnt_mesh_piece_describe(const pnt_mesh* mesh, pnt_piece_desc* out);
+
 /* ------------------------------------------------------------------ */
 /* Parameters: deck keys and defaults of Driver (Driver.cc:78-87),       */
 /* Hydro (Hydro.cc:206-214), PolyGas (PolyGas.cc:57-60), TTS             */
@@ -222,6 +257,41 @@ enum {
 /* bytes must equal the field's size (element count x element size). */
 pnt_status pnt_hydro_download(pnt_hydro* hydro, int32_t field, void* host_dst, size_t bytes);
 pnt_status pnt_hydro_upload(pnt_hydro* hydro, int32_t field, const void* host_src, size_t bytes);
+/* Multi-piece cycle (a hydro object created from a pnt_mesh_piece mesh;
+ * pnt_hydro_cycle/run/enqueue/time_* refuse it).  One cycle on the
+ * object's stream, every piece in step:
+ *   pnt_hydro_piece_forces   pass A (and the learned closure pass) on the
+ *                            local zones, then the corner mass and force of
+ *                            the send lists into the send buffer;
+ *   (caller)                 for each neighbour nbr[j]: send its send range
+ *                            and receive its halo range (byte offsets below);
+ *   pnt_hydro_piece_advance  passes B and C on the local points and zones
+ *                            and this piece's reduction into red[4] =
+ *                            {dtnew, -dvovmax, inverted sides in pass A, in
+ *                            pass C};
+ *   (caller)                 red[0:2] <- minimum over pieces, red[2:4] <-
+ *                            sum over pieces;
+ *   pnt_hydro_piece_finish   calcDt, the bad-side status, time/cycle and the
+ *                            next dt from the reduced red (Hydro.cc:961-970,
+ *                            Driver.cc:213-245).
+ * Every piece then holds exactly the single-piece values of its zones and
+ * points (shared points are advanced by each piece that holds them, from
+ * the same corner sums in the same order). */
+typedef struct {
+    void* send;                   /* device: corner masses of send_side[] ... */
+    size_t send_cforce_offset;    /* ... and their corner forces from this byte offset */
+    void* halo_cmass;             /* device: halo slot h's corner mass at h*cmass_bytes */
+    void* halo_cforce;            /* device: halo slot h's corner force at h*cforce_bytes */
+    int32_t cmass_bytes;          /* 8 and 16 (fp64) or 4 and 8 (mixed, learned) */
+    int32_t cforce_bytes;
+    double* red;                  /* device [4] */
+    void* stream;                 /* the object's cudaStream_t */
+} pnt_piece_buffers;
+pnt_status pnt_hydro_piece_buffers(pnt_hydro* hydro, pnt_piece_buffers* out);
+pnt_status pnt_hydro_piece_forces(pnt_hydro* hydro);
+pnt_status pnt_hydro_piece_advance(pnt_hydro* hydro);
+pnt_status pnt_hydro_piece_finish(pnt_hydro* hydro);
+
 /* Device address of the current copy of a field (valid until the next
  * cycle swaps the point buffers) and the object's cudaStream_t. */
 pnt_status pnt_hydro_device_ptr(pnt_hydro* hydro, int32_t field, void** dptr);

@@ -12,6 +12,7 @@
 #include <cstring>
 #include <fstream>
 #include <sstream>
+#include <unordered_map>
 
 namespace pnt {
 
@@ -283,6 +284,142 @@ pnt_status finish_mesh(Mesh& m) {
     return PNT_OK;
 }
 
+// ---------------------------------------------------------------------
+// Multi-piece decomposition: the role of Mesh(inp, numpcs) with its
+// private, master and ghost points (Mesh.cc:211-241, :441-617), here as
+// contiguous zone ranges in the reference's numbering.  A piece keeps its
+// zones' sides and every point they touch, with local ids in global order,
+// and copies the single-piece initial geometry, so each zone and point
+// computes exactly what it computes in the single-piece run.  The corners
+// of a shared point that other pieces own become halo slots after the
+// local sides; the point -> corner CSR lists local and halo slots merged in
+// global side order, so the corner-force and corner-mass sums at shared
+// points keep the single-piece summation order (the reference sums shared
+// points through Legion reductions instead, Hydro.cc:571-574, 766-769).
+// ---------------------------------------------------------------------
+pnt_status make_piece(const Mesh& g, int npieces, int piece, Mesh& m) {
+    if (g.npieces != 1) return fail(PNT_ERR_INVALID_ARG, "the mesh is already a piece");
+    if (npieces < 1 || npieces > 64 || piece < 0 || piece >= npieces)
+        return fail(PNT_ERR_INVALID_ARG, "piece %d of %d: 1-64 pieces", piece, npieces);
+    const int64_t np = g.nump, nz = g.numz, ns = g.nums;
+    if (npieces > nz) return fail(PNT_ERR_INVALID_ARG, "%d pieces for %lld zones", npieces, (long long)nz);
+    std::vector<int32_t> zbeg(npieces + 1);
+    for (int q = 0; q <= npieces; ++q) zbeg[q] = (int32_t)(nz * q / npieces);
+    auto piece_of = [&](int32_t z) {
+        return (int)(std::upper_bound(zbeg.begin(), zbeg.end(), z) - zbeg.begin()) - 1;
+    };
+    // the pieces that touch each point (bit q: a zone of piece q has it)
+    std::vector<uint64_t> pmask(np, 0);
+    for (int q = 0; q < npieces; ++q)
+        for (int64_t s = g.zfirst[zbeg[q]]; s < (zbeg[q + 1] < nz ? g.zfirst[zbeg[q + 1]] : ns); ++s)
+            pmask[g.mapsp1[s]] |= 1ull << q;
+    const int32_t z0 = zbeg[piece], z1 = zbeg[piece + 1];
+    const int32_t s0 = g.zfirst[z0], s1 = z1 < nz ? g.zfirst[z1] : (int32_t)ns;
+
+    m = Mesh();
+    m.piece = piece;
+    m.npieces = npieces;
+    m.zone0 = z0;
+    m.side0 = s0;
+    std::vector<int32_t> lp(np, -1);
+    for (int64_t p = 0; p < np; ++p)
+        if ((pmask[p] >> piece) & 1) {
+            lp[p] = (int32_t)m.gpoint.size();
+            m.gpoint.push_back((int32_t)p);
+        }
+    m.nump = (int32_t)m.gpoint.size();
+    m.numz = z1 - z0;
+    m.nums = s1 - s0;
+    m.px.resize(2 * (size_t)m.nump);
+    for (int32_t p = 0; p < m.nump; ++p) {
+        m.px[2 * p] = g.px[2 * (size_t)m.gpoint[p]];
+        m.px[2 * p + 1] = g.px[2 * (size_t)m.gpoint[p] + 1];
+    }
+    m.znump.assign(g.znump.begin() + z0, g.znump.begin() + z1);
+    m.zfirst.resize(m.numz);
+    m.all_quads = true;
+    for (int32_t z = 0; z < m.numz; ++z) {
+        m.zfirst[z] = g.zfirst[z0 + z] - s0;
+        if (m.znump[z] != 4) m.all_quads = false;
+    }
+    m.mapsp1.resize(m.nums);
+    m.mapsp2.resize(m.nums);
+    m.mapsz.resize(m.nums);
+    m.mapss3.resize(m.nums);
+    m.mapss4.resize(m.nums);
+    for (int32_t s = 0; s < m.nums; ++s) {
+        const int32_t t = s0 + s;
+        m.mapsp1[s] = lp[g.mapsp1[t]];
+        m.mapsp2[s] = lp[g.mapsp2[t]];
+        m.mapsz[s] = g.mapsz[t] - z0;
+        m.mapss3[s] = g.mapss3[t] - s0;
+        m.mapss4[s] = g.mapss4[t] - s0;
+    }
+    m.zx.assign(g.zx.begin() + 2 * (size_t)z0, g.zx.begin() + 2 * (size_t)z1);
+    m.zarea.assign(g.zarea.begin() + z0, g.zarea.begin() + z1);
+    m.zvol.assign(g.zvol.begin() + z0, g.zvol.begin() + z1);
+    m.sarea.assign(g.sarea.begin() + s0, g.sarea.begin() + s1);
+    m.svol.assign(g.svol.begin() + s0, g.svol.begin() + s1);
+    m.smf.assign(g.smf.begin() + s0, g.smf.begin() + s1);
+
+    // halo slots: corners at local points owned by other pieces, grouped by
+    // owner, in global side order
+    std::vector<std::pair<int, int32_t>> hs;
+    for (int32_t p = 0; p < m.nump; ++p) {
+        const int32_t gp = m.gpoint[p];
+        for (int32_t c = g.poff[gp]; c < g.poff[gp + 1]; ++c) {
+            const int32_t t = g.pcorner[c];
+            if (t < s0 || t >= s1) hs.push_back({piece_of(g.mapsz[t]), t});
+        }
+    }
+    std::sort(hs.begin(), hs.end());
+    m.nhalo = (int32_t)hs.size();
+    std::unordered_map<int32_t, int32_t> hslot;
+    hslot.reserve(hs.size() * 2 + 1);
+    m.recv_off.push_back(0);
+    for (size_t h = 0; h < hs.size(); ++h) {
+        m.halo_side.push_back(hs[h].second);
+        hslot[hs[h].second] = (int32_t)h;
+        if (m.nbr.empty() || m.nbr.back() != hs[h].first) {
+            if (!m.nbr.empty()) m.recv_off.push_back((int32_t)h);
+            m.nbr.push_back(hs[h].first);
+        }
+    }
+    if (!m.nbr.empty()) m.recv_off.push_back(m.nhalo);
+    // point -> corner CSR over local and halo slots, global side order
+    m.poff.assign(m.nump + 1, 0);
+    m.pcorner.clear();
+    m.pcorner.reserve(m.nums + m.nhalo);
+    for (int32_t p = 0; p < m.nump; ++p) {
+        const int32_t gp = m.gpoint[p];
+        for (int32_t c = g.poff[gp]; c < g.poff[gp + 1]; ++c) {
+            const int32_t t = g.pcorner[c];
+            m.pcorner.push_back((t >= s0 && t < s1) ? t - s0 : m.nums + hslot[t]);
+        }
+        m.poff[p + 1] = (int32_t)m.pcorner.size();
+    }
+    // send lists: each neighbour needs the local corners at the points it
+    // shares, in global side order
+    std::vector<std::vector<int32_t>> sl(m.nbr.size());
+    std::vector<int> slot_of(npieces, -1);
+    for (size_t j = 0; j < m.nbr.size(); ++j) slot_of[m.nbr[j]] = (int)j;
+    for (int32_t s = 0; s < m.nums; ++s) {
+        uint64_t bits = pmask[g.mapsp1[s0 + s]] & ~(1ull << piece);
+        while (bits) {
+            const int q = __builtin_ctzll(bits);
+            bits &= bits - 1;
+            if (slot_of[q] < 0) return fail(PNT_ERR_INVALID_ARG, "piece %d shares a point with %d but owns none of its corners", piece, q);
+            sl[slot_of[q]].push_back(s);
+        }
+    }
+    m.send_off.push_back(0);
+    for (auto& v : sl) {
+        m.send_side.insert(m.send_side.end(), v.begin(), v.end());
+        m.send_off.push_back((int32_t)m.send_side.size());
+    }
+    return PNT_OK;
+}
+
 }  // namespace pnt
 
 using namespace pnt;
@@ -446,6 +583,43 @@ pnt_status pnt_mesh_point_corners(const pnt_mesh* mesh, const int32_t** offsets,
 }
 
 void pnt_mesh_destroy(pnt_mesh* mesh) { delete mesh; }
+
+pnt_status pnt_mesh_piece(const pnt_mesh* mesh, int32_t npieces, int32_t piece, pnt_mesh** out) {
+    if (!mesh || !out) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    pnt_mesh* pm = new (std::nothrow) pnt_mesh();
+    if (!pm) return fail(PNT_ERR_NOMEM, "out of memory");
+    pnt_status st;
+    try {
+        st = make_piece(mesh->m, npieces, piece, pm->m);
+    } catch (const std::bad_alloc&) {
+        st = fail(PNT_ERR_NOMEM, "out of host memory building piece %d", piece);
+    }
+    if (st) {
+        delete pm;
+        return st;
+    }
+    *out = pm;
+    return PNT_OK;
+}
+
+pnt_status pnt_mesh_piece_describe(const pnt_mesh* mesh, pnt_piece_desc* out) {
+    if (!mesh || !out) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    const Mesh& m = mesh->m;
+    out->piece = m.piece;
+    out->npieces = m.npieces;
+    out->zone0 = m.zone0;
+    out->side0 = m.side0;
+    out->gpoint = m.npieces > 1 ? m.gpoint.data() : nullptr;
+    out->nhalo = m.nhalo;
+    out->halo_side = m.halo_side.data();
+    out->nnbr = (int32_t)m.nbr.size();
+    out->nbr = m.nbr.data();
+    out->send_off = m.npieces > 1 ? m.send_off.data() : nullptr;
+    out->send_side = m.send_side.data();
+    out->recv_off = m.npieces > 1 ? m.recv_off.data() : nullptr;
+    return PNT_OK;
+}
 
 pnt_status pnt_params_default(pnt_params* p) {
     if (!p) return fail(PNT_ERR_INVALID_ARG, "null argument");

@@ -57,10 +57,19 @@ struct pnt_hydro {
     cudaGraphExec_t graph = nullptr;
     int graph_cycles = 0;
     // the cycle of the selected precision
-    cudaError_t (*launch)(const DevArrays&, const HydroConst&, cudaStream_t, cudaEvent_t*) = launch_cycle_fp64;
+    cudaError_t (*launch)(const DevArrays&, const HydroConst&, cudaStream_t, cudaEvent_t*, int) = launch_cycle_fp64;
     // learned closure: this object's copy of the parameter image (set by
     // pnt_hydro_set_closure) and the corner class counters
     bool learned = false;
+    // multi-piece runs (a hydro object over a piece mesh): the send lists,
+    // the send buffer (corner masses, then corner forces at send_foff) and
+    // the per-corner byte sizes of the cycle's precision
+    bool piece = false;
+    int32_t nsend = 0, nhalo = 0;
+    int32_t* send_side = nullptr;
+    unsigned char* send = nullptr;
+    size_t send_foff = 0;
+    int32_t cmass_bytes = 8, cforce_bytes = 16;
 
     ~pnt_hydro() {
         DeviceGuard dg(device);
@@ -84,16 +93,21 @@ struct pnt_hydro {
         return PNT_OK;
     }
 
-    pnt_status check_ready() const {
+    pnt_status check_closure() const {
         if (learned && !a.closure_img)
             return fail(PNT_ERR_STATE, "precision learned needs a closure (pnt_hydro_set_closure)");
         return PNT_OK;
+    }
+    // whole cycles (a piece steps with pnt_hydro_piece_*)
+    pnt_status check_ready() const {
+        if (piece) return fail(PNT_ERR_STATE, "a piece object steps with pnt_hydro_piece_forces/advance/finish");
+        return check_closure();
     }
 
     pnt_status launch_cycles(int n) {
         if (pnt_status st = check_ready()) return st;
         for (int i = 0; i < n; ++i) {
-            const cudaError_t e = launch(a, hc, stream, nullptr);
+            const cudaError_t e = launch(a, hc, stream, nullptr, kPhaseAll);
             if (e != cudaSuccess) return fail(PNT_ERR_CUDA, "cycle launch: %s", cudaGetErrorString(e));
         }
         return PNT_OK;
@@ -106,7 +120,7 @@ struct pnt_hydro {
         cudaGraph_t g = nullptr;
         CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         for (int i = 0; i < graph_cycles; ++i) {
-            const cudaError_t e = launch(a, hc, stream, nullptr);
+            const cudaError_t e = launch(a, hc, stream, nullptr, kPhaseAll);
             if (e != cudaSuccess) {
                 cudaStreamEndCapture(stream, &g);
                 if (g) cudaGraphDestroy(g);
@@ -269,12 +283,12 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
     const int64_t nzbc = a.gridC;
     pnt_status st = PNT_OK;
     if ((st = h->alloc(&zfirst, nz)) || (st = h->alloc(&znump, nz)) || (st = h->alloc(&mapsp1, ns)) ||
-        (st = h->alloc(&smf, ns)) || (st = h->alloc(&poff, np + 1)) || (st = h->alloc(&pcorner, ns)) ||
+        (st = h->alloc(&smf, ns)) || (st = h->alloc(&poff, np + 1)) || (st = h->alloc(&pcorner, m.pcorner.size())) ||
         (st = h->alloc(&mask, np + 2)) || (st = h->alloc(&a.px[0], np)) || (st = h->alloc(&a.px[1], np)) ||
         (st = h->alloc(&a.pu[0], np)) || (st = h->alloc(&a.pu[1], np)) || (st = h->alloc(&a.zm, nz)) ||
         (st = h->alloc(&a.zr, nz)) || (st = h->alloc(&a.ze, nz)) || (st = h->alloc(&a.zetot, nz)) ||
         (st = h->alloc(&a.zwrate, nz)) || (st = h->alloc(&a.zvol, nz)) || (st = h->alloc(&a.zp, nz)) ||
-        (st = h->alloc(&a.cmass, ns)) || (st = h->alloc(&a.cforce, ns)) || (st = h->alloc(&a.sftot, ns)) ||
+        (st = h->alloc(&a.cmass, ns + m.nhalo)) || (st = h->alloc(&a.cforce, ns + m.nhalo)) || (st = h->alloc(&a.sftot, ns)) ||
         (st = h->alloc(&a.part_dtnew, nzb)) || (st = h->alloc(&a.part_badA, nzb)) ||
         (st = h->alloc(&a.part_dvov, nzbc)) || (st = h->alloc(&a.part_badC, nzbc)) ||
         (st = h->alloc(&a.fin_part, 2 * kFinBlocks)) || (st = h->alloc(&a.fin_bad, 2 * kFinBlocks)) ||
@@ -292,6 +306,22 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
     a.poff = poff;
     a.pcorner = pcorner;
     a.bcmask = mask;
+    if (m.npieces > 1) {
+        // a piece: halo corner slots follow the local sides in cmass/cforce
+        h->piece = true;
+        h->nhalo = m.nhalo;
+        h->nsend = (int32_t)m.send_side.size();
+        const bool fp64 = p.precision == PNT_PREC_FP64;
+        h->cmass_bytes = fp64 ? 8 : 4;
+        h->cforce_bytes = fp64 ? 16 : 8;
+        h->send_foff = ((size_t)h->nsend * h->cmass_bytes + 15) / 16 * 16;
+        if ((st = h->alloc(&h->send_side, (size_t)h->nsend)) ||
+            (st = h->alloc(&h->send, h->send_foff + (size_t)h->nsend * h->cforce_bytes)) ||
+            (st = h->alloc(&a.piece_red, 4)))
+            return st;
+        if (h->nsend > 0)
+            CUDA_TRY(cudaMemcpy(h->send_side, m.send_side.data(), (size_t)h->nsend * 4, cudaMemcpyHostToDevice));
+    }
 
     // Driver::run start: time 0, cycle 0 and calcGlobalDt for cycle 0
     // (Driver.cc:213-245).
@@ -313,7 +343,7 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
     cudaError_t e = cudaSuccess;
     if ((e = up(zfirst, m.zfirst.data(), nz * 4)) || (e = up(znump, m.znump.data(), nz * 4)) ||
         (e = up(mapsp1, m.mapsp1.data(), ns * 4)) || (e = up(smf, m.smf.data(), ns * 8)) ||
-        (e = up(poff, m.poff.data(), (np + 1) * 4)) || (e = up(pcorner, m.pcorner.data(), ns * 4)) ||
+        (e = up(poff, m.poff.data(), (np + 1) * 4)) || (e = up(pcorner, m.pcorner.data(), m.pcorner.size() * 4)) ||
         (e = up(mask, bcmask.data(), np * 2)) || (e = up(a.px[0], m.px.data(), np * 16)) ||
         (e = up(a.pu[0], pu.data(), np * 16)) || (e = up(a.zm, zm.data(), nz * 8)) ||
         (e = up(a.zr, zr.data(), nz * 8)) || (e = up(a.ze, ze.data(), nz * 8)) ||
@@ -463,13 +493,14 @@ pnt_status pnt_hydro_enqueue(pnt_hydro* h, int32_t ncycles) {
 pnt_status pnt_hydro_time_kernels(pnt_hydro* h, int32_t ncycles, double* kernel_ms, int32_t nkernels) {
     if (!h || !kernel_ms || ncycles <= 0 || nkernels <= 0) return fail(PNT_ERR_INVALID_ARG, "bad argument");
     DeviceGuard dg(h->device);
+    if (pnt_status st0 = h->check_ready()) return st0;
     std::vector<cudaEvent_t> ev((size_t)ncycles * kNumEvents, nullptr);
     pnt_status st = PNT_OK;
     for (auto& e : ev) {
         if (cudaEventCreate(&e) != cudaSuccess) { st = fail(PNT_ERR_CUDA, "cudaEventCreate failed"); break; }
     }
     for (int32_t i = 0; i < ncycles && !st; ++i) {
-        const cudaError_t e = h->launch(h->a, h->hc, h->stream, &ev[(size_t)i * kNumEvents]);
+        const cudaError_t e = h->launch(h->a, h->hc, h->stream, &ev[(size_t)i * kNumEvents], kPhaseAll);
         if (e != cudaSuccess) st = fail(PNT_ERR_CUDA, "cycle launch: %s", cudaGetErrorString(e));
     }
     if (!st && cudaStreamSynchronize(h->stream) != cudaSuccess) st = fail(PNT_ERR_CUDA, "synchronize failed");
@@ -566,6 +597,50 @@ pnt_status pnt_hydro_device_ptr(pnt_hydro* h, int32_t field, void** dptr) {
     const FieldInfo fi = field_info(h, field, h->ctl_host->cycle & 1);
     if (!fi.dev) return fail(PNT_ERR_INVALID_ARG, "unknown field %d", field);
     *dptr = fi.dev;
+    return PNT_OK;
+}
+
+pnt_status pnt_hydro_piece_buffers(pnt_hydro* h, pnt_piece_buffers* out) {
+    if (!h || !out) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    if (!h->piece) return fail(PNT_ERR_STATE, "not a piece object");
+    out->send = h->send;
+    out->send_cforce_offset = h->send_foff;
+    out->halo_cmass = reinterpret_cast<unsigned char*>(h->a.cmass) + (size_t)h->nums * h->cmass_bytes;
+    out->halo_cforce = reinterpret_cast<unsigned char*>(h->a.cforce) + (size_t)h->nums * h->cforce_bytes;
+    out->cmass_bytes = h->cmass_bytes;
+    out->cforce_bytes = h->cforce_bytes;
+    out->red = h->a.piece_red;
+    out->stream = (void*)h->stream;
+    return PNT_OK;
+}
+
+pnt_status pnt_hydro_piece_forces(pnt_hydro* h) {
+    if (!h) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    if (!h->piece) return fail(PNT_ERR_STATE, "not a piece object");
+    if (pnt_status st = h->check_closure()) return st;
+    DeviceGuard dg(h->device);
+    CUDA_TRY(h->launch(h->a, h->hc, h->stream, nullptr, kPhaseForces));
+    launch_piece_pack(h->a, h->send_side, h->nsend, h->send, h->send_foff, h->params.precision != PNT_PREC_FP64,
+                      h->stream);
+    CUDA_TRY(cudaGetLastError());
+    return PNT_OK;
+}
+
+pnt_status pnt_hydro_piece_advance(pnt_hydro* h) {
+    if (!h) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    if (!h->piece) return fail(PNT_ERR_STATE, "not a piece object");
+    if (pnt_status st = h->check_closure()) return st;
+    DeviceGuard dg(h->device);
+    CUDA_TRY(h->launch(h->a, h->hc, h->stream, nullptr, kPhaseAdvance));
+    return PNT_OK;
+}
+
+pnt_status pnt_hydro_piece_finish(pnt_hydro* h) {
+    if (!h) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    if (!h->piece) return fail(PNT_ERR_STATE, "not a piece object");
+    DeviceGuard dg(h->device);
+    launch_piece_finish(h->a, h->hc, h->stream);
+    CUDA_TRY(cudaGetLastError());
     return PNT_OK;
 }
 

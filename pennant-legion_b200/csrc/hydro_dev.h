@@ -93,6 +93,10 @@ struct DevArrays {
     int32_t* closure_nrec;
     int32_t closure_grid;   // CTAs of the persistent closure pass
     int32_t gridC;          // CTAs of the persistent pass C (pass_c_staged.cuh)
+    // multi-piece runs: the finalize step writes this piece's [dtnew,
+    // -dvovmax, inverted sides in A, in C] here instead of ending the cycle
+    // (nullptr for a single piece)
+    double* piece_red;
 };
 
 constexpr int kZoneThreads = 256;   // pass A: 64 zones x 4 side lanes per block
@@ -108,16 +112,30 @@ constexpr int kNumEvents = 6;
 constexpr int kFinBlocks = 64;   // blocks of the finalize reduction
 constexpr int kNumKernels = 5;   // A, B, C, finalize, closure pass
 
-// One hydro cycle (passes A, B, C and the finalize step) on `stream`.  With
-// `ev` non-null, the kNumEvents events above are recorded.
+// Phases of a cycle: the corner forces (pass A and the learned closure
+// pass) and the advance (passes B, C and the finalize step).
+constexpr int kPhaseForces = 1;
+constexpr int kPhaseAdvance = 2;
+constexpr int kPhaseAll = kPhaseForces | kPhaseAdvance;
+
+// One hydro cycle (passes A, B, C and the finalize step) on `stream`, or
+// the given phases of it.  With `ev` non-null (whole cycles only), the
+// kNumEvents events above are recorded.
 cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStream_t stream,
-                              cudaEvent_t* ev = nullptr);
+                              cudaEvent_t* ev = nullptr, int phases = kPhaseAll);
 // The mixed-precision cycle (hydro_mixed.cu).
 cudaError_t launch_cycle_mixed(const DevArrays& a, const HydroConst& c, cudaStream_t stream,
-                               cudaEvent_t* ev = nullptr);
+                               cudaEvent_t* ev = nullptr, int phases = kPhaseAll);
 // The learned-closure cycle: the mixed cycle with the closure in pass A.
 cudaError_t launch_cycle_learned(const DevArrays& a, const HydroConst& c, cudaStream_t stream,
-                                 cudaEvent_t* ev = nullptr);
+                                 cudaEvent_t* ev = nullptr, int phases = kPhaseAll);
+// Multi-piece runs (hydro_fp64.cu): gathers the corner mass and force of
+// the nsend local sides send_side[] into send (corner masses, then the
+// corner forces at byte offset foff; FP32 when mixed), and ends the cycle
+// from the globally reduced piece_red.
+void launch_piece_pack(const DevArrays& a, const int32_t* send_side, int32_t nsend, unsigned char* send,
+                       size_t foff, bool mixed, cudaStream_t stream);
+void launch_piece_finish(const DevArrays& a, const HydroConst& c, cudaStream_t stream);
 // Raises the learned pass A's dynamic shared-memory limit on the current device.
 cudaError_t prepare_learned_kernels();
 // Pass C of the FP64 (mixed = false) or mixed/learned cycle (pass_c.cu):

@@ -148,27 +148,71 @@ __global__ void __launch_bounds__(kFinThreads) finalize(DevArrays a, HydroConst 
     fin_block_reduce(dtn, dvm, badA, badC);
     if (threadIdx.x == 0) {
         *a.fin_ticket = 0u;
-        finish_cycle(ctl, c, dtn, dvm, badA, badC);
+        if (a.piece_red) {   // a piece: the caller reduces over pieces, then piece_finish
+            a.piece_red[0] = dtn;
+            a.piece_red[1] = -dvm;
+            a.piece_red[2] = (double)badA;
+            a.piece_red[3] = (double)badC;
+        } else {
+            finish_cycle(ctl, c, dtn, dvm, badA, badC);
+        }
     }
 }
 
+// Multi-piece runs: the corner values the neighbours need, and the end of
+// the cycle from the reduction over all pieces (min dtnew, max dvovmax,
+// summed inverted sides: exact in any order).
+__global__ void piece_pack(DevArrays a, const int32_t* __restrict__ send_side, int32_t nsend,
+                           unsigned char* __restrict__ send, size_t foff, bool mixed) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nsend) return;
+    const int32_t s = send_side[i];
+    if (mixed) {
+        reinterpret_cast<float*>(send)[i] = a.cmass_f[s];
+        reinterpret_cast<float2*>(send + foff)[i] = a.cforce_f[s];
+    } else {
+        reinterpret_cast<double*>(send)[i] = a.cmass[s];
+        reinterpret_cast<double2*>(send + foff)[i] = a.cforce[s];
+    }
+}
+
+__global__ void piece_finish(DevArrays a, HydroConst c) {
+    Ctl* ctl = a.ctl;
+    if (skip_cycle(ctl)) return;
+    const double* r = a.piece_red;
+    finish_cycle(ctl, c, r[0], -r[1], (int)r[2], (int)r[3]);
+}
+
 }  // namespace
-cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStream_t stream, cudaEvent_t* ev) {
-    const int zb = (int)zone_blocks(a.numz);
+cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStream_t stream, cudaEvent_t* ev,
+                              int phases) {
     const int pb = (int)((a.nump + kPointThreads - 1) / kPointThreads);
-    if (ev) cudaEventRecord(ev[0], stream);
     const int zba = (int)((a.numz + kZoneThreadsZT - 1) / kZoneThreadsZT);
-    if (a.quads) pass_a_zt<true><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
-    else pass_a_zt<false><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
-    if (ev) cudaEventRecord(ev[1], stream);
-    if (ev) cudaEventRecord(ev[2], stream);   // no closure pass
-    pass_b<<<pb, kPointThreads, 0, stream>>>(a, c);
-    if (ev) cudaEventRecord(ev[3], stream);
-    launch_pass_c(a, c, false, stream);
-    if (ev) cudaEventRecord(ev[4], stream);
-    finalize<<<kFinBlocks, kFinThreads, 0, stream>>>(a, c, zba, a.gridC);
-    if (ev) cudaEventRecord(ev[5], stream);
+    if (phases & kPhaseForces) {
+        if (ev) cudaEventRecord(ev[0], stream);
+        if (a.quads) pass_a_zt<true><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
+        else pass_a_zt<false><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
+        if (ev) cudaEventRecord(ev[1], stream);
+        if (ev) cudaEventRecord(ev[2], stream);   // no closure pass
+    }
+    if (phases & kPhaseAdvance) {
+        pass_b<<<pb, kPointThreads, 0, stream>>>(a, c);
+        if (ev) cudaEventRecord(ev[3], stream);
+        launch_pass_c(a, c, false, stream);
+        if (ev) cudaEventRecord(ev[4], stream);
+        finalize<<<kFinBlocks, kFinThreads, 0, stream>>>(a, c, zba, a.gridC);
+        if (ev) cudaEventRecord(ev[5], stream);
+    }
     return cudaGetLastError();
+}
+
+void launch_piece_pack(const DevArrays& a, const int32_t* send_side, int32_t nsend, unsigned char* send,
+                       size_t foff, bool mixed, cudaStream_t stream) {
+    if (nsend > 0) piece_pack<<<(nsend + 255) / 256, 256, 0, stream>>>(a, send_side, nsend, send, foff, mixed);
+}
+
+void launch_piece_finish(const DevArrays& a, const HydroConst& c, cudaStream_t stream) {
+    piece_finish<<<1, 1, 0, stream>>>(a, c);
 }
 
 void launch_finalize(const DevArrays& a, const HydroConst& c, int nA, int nC, cudaStream_t stream) {

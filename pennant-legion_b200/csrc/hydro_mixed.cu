@@ -656,37 +656,43 @@ __global__ void __launch_bounds__(kMlpRows, 3) closure_pass(DevArrays a, HydroCo
 namespace {
 
 cudaError_t launch_cycle_mixed_impl(const DevArrays& a, const HydroConst& c, cudaStream_t stream, cudaEvent_t* ev,
-                                    bool learned) {
+                                    bool learned, int phases) {
     const int pb = (int)((a.nump + kPointThreads - 1) / kPointThreads);
-    if (ev) cudaEventRecord(ev[0], stream);
     const int zba = (int)((a.numz + kZoneThreadsZT - 1) / kZoneThreadsZT);
-    if (learned) {
-        if (a.quads) pass_a_mixed_zt<true, true><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
-        else pass_a_mixed_zt<false, true><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
-    } else {
-        if (a.quads) pass_a_mixed_zt<true, false><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
-        else pass_a_mixed_zt<false, false><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
+    if (phases & kPhaseForces) {
+        if (ev) cudaEventRecord(ev[0], stream);
+        if (learned) {
+            if (a.quads) pass_a_mixed_zt<true, true><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
+            else pass_a_mixed_zt<false, true><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
+        } else {
+            if (a.quads) pass_a_mixed_zt<true, false><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
+            else pass_a_mixed_zt<false, false><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
+        }
+        if (ev) cudaEventRecord(ev[1], stream);
+        if (learned) closure_pass<<<a.closure_grid, kMlpRows, kMlpSmemBytes, stream>>>(a, c);
+        if (ev) cudaEventRecord(ev[2], stream);
     }
-    if (ev) cudaEventRecord(ev[1], stream);
-    if (learned) closure_pass<<<a.closure_grid, kMlpRows, kMlpSmemBytes, stream>>>(a, c);
-    if (ev) cudaEventRecord(ev[2], stream);
-    pass_b_mixed<<<pb, kPointThreads, 0, stream>>>(a, c);
-    if (ev) cudaEventRecord(ev[3], stream);
-    launch_pass_c(a, c, true, stream);
-    if (ev) cudaEventRecord(ev[4], stream);
-    launch_finalize(a, c, zba, a.gridC, stream);
-    if (ev) cudaEventRecord(ev[5], stream);
+    if (phases & kPhaseAdvance) {
+        pass_b_mixed<<<pb, kPointThreads, 0, stream>>>(a, c);
+        if (ev) cudaEventRecord(ev[3], stream);
+        launch_pass_c(a, c, true, stream);
+        if (ev) cudaEventRecord(ev[4], stream);
+        launch_finalize(a, c, zba, a.gridC, stream);
+        if (ev) cudaEventRecord(ev[5], stream);
+    }
     return cudaGetLastError();
 }
 
 }  // namespace
 
-cudaError_t launch_cycle_mixed(const DevArrays& a, const HydroConst& c, cudaStream_t stream, cudaEvent_t* ev) {
-    return launch_cycle_mixed_impl(a, c, stream, ev, false);
+cudaError_t launch_cycle_mixed(const DevArrays& a, const HydroConst& c, cudaStream_t stream, cudaEvent_t* ev,
+                               int phases) {
+    return launch_cycle_mixed_impl(a, c, stream, ev, false, phases);
 }
 
-cudaError_t launch_cycle_learned(const DevArrays& a, const HydroConst& c, cudaStream_t stream, cudaEvent_t* ev) {
-    return launch_cycle_mixed_impl(a, c, stream, ev, true);
+cudaError_t launch_cycle_learned(const DevArrays& a, const HydroConst& c, cudaStream_t stream, cudaEvent_t* ev,
+                                 int phases) {
+    return launch_cycle_mixed_impl(a, c, stream, ev, true, phases);
 }
 
 cudaError_t prepare_learned_kernels() {

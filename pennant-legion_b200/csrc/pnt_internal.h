@@ -40,12 +40,29 @@ struct Mesh {
     bool all_quads = false;            // every zone has 4 sides at 4z..4z+3
     // initial geometry (Mesh::init, Mesh.cc:619-623)
     std::vector<double> zx, zarea, zvol, sarea, svol, smf;
+    // Multi-piece runs (make_piece): this mesh is piece `piece` of
+    // `npieces`, local zones are the global zones zone0.., local sides the
+    // global sides side0.., gpoint maps local to global points.  The point
+    // -> corner CSR also lists halo slots nums + h: corners of the piece's
+    // points that belong to other pieces' sides (global side halo_side[h]),
+    // grouped by owning neighbour (nbr, recv_off) in global side order.
+    // send_side[send_off[j] .. send_off[j+1]) are the local sides whose
+    // corner values neighbour nbr[j] needs, in global side order.
+    int32_t piece = 0, npieces = 1;
+    int32_t zone0 = 0, side0 = 0;
+    std::vector<int32_t> gpoint;
+    int32_t nhalo = 0;
+    std::vector<int32_t> halo_side;
+    std::vector<int32_t> nbr, send_off, send_side, recv_off;
 };
 
 // GenMesh rect/pie generation (GenMesh.cc:790-1282), single piece.
 pnt_status generate_mesh(const Deck& d, Mesh& m);
 // Validates connectivity, builds zfirst/CSR and the initial geometry.
 pnt_status finish_mesh(Mesh& m);
+// Piece `piece` of `npieces` (at most 64) of a finished single-piece mesh:
+// the contiguous zone range [numz*piece/npieces, numz*(piece+1)/npieces).
+pnt_status make_piece(const Mesh& g, int npieces, int piece, Mesh& out);
 
 // The closure's device parameter image and device (closure.cu).
 const uint8_t* closure_image(const pnt_closure* c);

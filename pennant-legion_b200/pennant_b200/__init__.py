@@ -88,6 +88,24 @@ class MeshDesc(C.Structure):
     ]
 
 
+class PieceDesc(C.Structure):
+    _fields_ = [
+        ("piece", C.c_int32), ("npieces", C.c_int32), ("zone0", C.c_int32), ("side0", C.c_int32),
+        ("gpoint", C.POINTER(C.c_int32)), ("nhalo", C.c_int32), ("halo_side", C.POINTER(C.c_int32)),
+        ("nnbr", C.c_int32), ("nbr", C.POINTER(C.c_int32)), ("recv_off", C.POINTER(C.c_int32)),
+        ("send_off", C.POINTER(C.c_int32)), ("send_side", C.POINTER(C.c_int32)),
+    ]
+
+
+class PieceBuffers(C.Structure):
+    _fields_ = [
+        ("send", C.c_void_p), ("send_cforce_offset", C.c_size_t),
+        ("halo_cmass", C.c_void_p), ("halo_cforce", C.c_void_p),
+        ("cmass_bytes", C.c_int32), ("cforce_bytes", C.c_int32),
+        ("red", C.c_void_p), ("stream", C.c_void_p),
+    ]
+
+
 REPORT_FN = C.CFUNCTYPE(None, C.POINTER(Scalars), C.c_double, C.c_void_p)
 
 
@@ -117,6 +135,8 @@ def _load():
         "pnt_mesh_point_corners": (i32, [vp, C.POINTER(C.POINTER(C.c_int32)),
                                          C.POINTER(C.POINTER(C.c_int32))]),
         "pnt_mesh_destroy": (None, [vp]),
+        "pnt_mesh_piece": (i32, [vp, i32, i32, pp]),
+        "pnt_mesh_piece_describe": (i32, [vp, C.POINTER(PieceDesc)]),
         "pnt_params_default": (i32, [C.POINTER(Params)]),
         "pnt_params_from_deck": (i32, [vp, C.POINTER(Params)]),
         "pnt_hydro_create": (i32, [vp, C.POINTER(Params), i32, pp]),
@@ -133,6 +153,10 @@ def _load():
         "pnt_hydro_upload": (i32, [vp, i32, vp, sz]),
         "pnt_hydro_device_ptr": (i32, [vp, i32, pp]),
         "pnt_hydro_stream": (i32, [vp, pp]),
+        "pnt_hydro_piece_buffers": (i32, [vp, C.POINTER(PieceBuffers)]),
+        "pnt_hydro_piece_forces": (i32, [vp]),
+        "pnt_hydro_piece_advance": (i32, [vp]),
+        "pnt_hydro_piece_finish": (i32, [vp]),
         "pnt_batch_create": (i32, [C.POINTER(vp), C.POINTER(Params), i32, i32, pp]),
         "pnt_batch_destroy": (None, [vp]),
         "pnt_batch_set_shape": (i32, [vp, i32, i32]),
@@ -227,11 +251,14 @@ class Deck:
 
 
 class Mesh:
-    """Mesh + GenMesh for one piece, reference numbering."""
+    """Mesh + GenMesh for one piece, reference numbering (or a piece of a
+    mesh: Mesh.piece)."""
 
-    def __init__(self, deck: Deck | None = None, desc: dict | None = None):
+    def __init__(self, deck: Deck | None = None, desc: dict | None = None, _handle=None):
         h = C.c_void_p()
-        if deck is not None:
+        if _handle is not None:
+            h = _handle
+        elif deck is not None:
             check(lib.pnt_mesh_generate(deck.h, C.byref(h)))
         else:
             arrs = {k: np.ascontiguousarray(desc[k], dtype=np.float64 if k == "px" else np.int32)
@@ -264,11 +291,38 @@ class Mesh:
         return np.ctypeslib.as_array(getattr(d, name), shape=(n,)).copy()
 
     def point_corners(self):
+        """Point -> corner CSR (offsets, slots); for a piece the slots past
+        nums are halo slots."""
         off = C.POINTER(C.c_int32)()
         sides = C.POINTER(C.c_int32)()
         check(lib.pnt_mesh_point_corners(self.h, C.byref(off), C.byref(sides)))
-        return (np.ctypeslib.as_array(off, shape=(self.nump + 1,)).copy(),
-                np.ctypeslib.as_array(sides, shape=(self.nums,)).copy())
+        offs = np.ctypeslib.as_array(off, shape=(self.nump + 1,)).copy()
+        return offs, np.ctypeslib.as_array(sides, shape=(int(offs[-1]),)).copy()
+
+    def piece(self, npieces: int, piece: int) -> "Mesh":
+        """Piece `piece` of `npieces`: a contiguous zone range with its
+        points, local numbering in global order, halo corner slots."""
+        h = C.c_void_p()
+        check(lib.pnt_mesh_piece(self.h, npieces, piece, C.byref(h)))
+        return Mesh(_handle=h)
+
+    def piece_info(self) -> dict:
+        """Global ids and halo exchange lists of a piece mesh (numpy copies)."""
+        d = PieceDesc()
+        check(lib.pnt_mesh_piece_describe(self.h, C.byref(d)))
+
+        def arr(ptr, n):
+            return np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n > 0 and ptr else np.zeros(0, np.int32)
+
+        nn = d.nnbr
+        info = {"piece": d.piece, "npieces": d.npieces, "zone0": d.zone0, "side0": d.side0,
+                "nhalo": d.nhalo, "nbr": arr(d.nbr, nn)}
+        info["gpoint"] = arr(d.gpoint, self.nump) if d.npieces > 1 else np.arange(self.nump, dtype=np.int32)
+        info["halo_side"] = arr(d.halo_side, d.nhalo)
+        info["recv_off"] = arr(d.recv_off, nn + 1) if d.npieces > 1 else np.zeros(1, np.int32)
+        info["send_off"] = arr(d.send_off, nn + 1) if d.npieces > 1 else np.zeros(1, np.int32)
+        info["send_side"] = arr(d.send_side, int(info["send_off"][-1]))
+        return info
 
 
 class Hydro:

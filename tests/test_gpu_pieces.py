@@ -1,0 +1,93 @@
+"""Multi-piece runs on the GPU (needs a GPU): the mesh split over 2 or 3
+ranks (processes; on one GPU they share it and exchange through gloo and
+host memory, so no kernel waits on another), every rank stepping its piece
+with pennant_b200.pieces.PieceHydro.  Each piece's zones and points must be
+bit-identical to the single-piece run of the same deck, for the FP64 cycle
+(rect and pie meshes), the mixed cycle and the learned cycle."""
+import datetime
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from conftest import DECKS, PKG, golden
+import pennant_b200 as pb
+
+sys.path.insert(0, DECKS)
+from make_decks import sedov  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+CLOSURE = os.path.join(PKG, "closure", "qcs_mlp.bin")
+ZONE = ("zr", "ze", "zetot", "zvol", "zwrate")
+POINT = ("px", "pu")
+
+
+def _port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _deck(text, precision):
+    d = pb.Deck(text=text)
+    d.set("precision", precision)
+    return d
+
+
+def _rank(rank, world, port, text, precision, out):
+    import torch.distributed as dist
+    from pennant_b200.pieces import PieceHydro
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        d = _deck(text, precision)
+        clo = pb.Closure(path=CLOSURE) if precision == "learned" else None
+        ph = PieceHydro(pb.Mesh(deck=d), d.params(), device=0, closure=clo)
+        s = ph.run()
+        out[rank] = (s, ph.fields(ZONE + POINT), ph.info)
+        ph.close()
+    finally:
+        dist.destroy_process_group()
+
+
+def single(text, precision):
+    d = _deck(text, precision)
+    h = pb.Hydro(pb.Mesh(deck=d), d.params())
+    if precision == "learned":
+        h.set_closure(pb.Closure(path=CLOSURE))
+    s = h.run()
+    f = {k: h.download(k) for k in ZONE + POINT}
+    h.close()
+    return s, f
+
+
+CASES = {
+    "sedov-fp64": (sedov(24, tstop=0.05), "fp64", 2),
+    "sedov-fp64-3": (sedov(20, tstop=0.05), "fp64", 3),
+    "noh-pie-fp64": (open(golden("nohsmall.pnt")).read().replace("cstop   10", "cstop   60"), "fp64", 2),
+    "sedov-mixed": (sedov(24, tstop=0.05), "mixed", 2),
+    "sedov-learned": (sedov(32, tstop=0.2), "learned", 2),
+}
+
+
+@pytest.mark.timeout(600)
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_pieces_match_the_single_piece_run_bitwise(case):
+    text, precision, world = CASES[case]
+    s1, f1 = single(text, precision)
+    out = mp.get_context("spawn").Manager().dict()
+    mp.start_processes(_rank, args=(world, _port(), text, precision, out), nprocs=world, join=True,
+                       start_method="spawn")
+    assert sorted(out.keys()) == list(range(world))
+    for r in range(world):
+        s, f, info = out[r]
+        assert s["cycle"] == s1["cycle"] and s["time"] == s1["time"] and s["done"] == 1, (case, r, s, s1)
+        z = slice(info["zone0"], info["zone0"] + len(f["zr"]))
+        for k in ZONE:
+            assert f[k].tobytes() == f1[k][z].tobytes(), (case, r, k)
+        for k in POINT:
+            assert f[k].tobytes() == f1[k][info["gpoint"]].tobytes(), (case, r, k)
