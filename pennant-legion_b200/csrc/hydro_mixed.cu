@@ -177,11 +177,24 @@ __device__ __forceinline__ void qcs_sfq_fp64_zone(const DevArrays& a, const Hydr
     }
 }
 
+constexpr int kZoneThreadsZT = 128;   // pass A: one zone per thread
+
+// Per-side values parked in the thread's shared-memory slots between their
+// computation and their last use ([side][thread]: conflict-free).
+struct SideSpill {
+    double2* sfp_;
+    float2* sft_;
+    int t;
+    __device__ __forceinline__ double2& sfp(int k) const { return sfp_[k * kZoneThreadsZT + t]; }
+    __device__ __forceinline__ float2& sft(int k) const { return sft_[k * kZoneThreadsZT + t]; }
+};
+
 // nbad counts the zone's inverted sides; cnt[3]: its corners without
 // compression, in the dead zone, in an acute zone (learned cycle).
 template <int N, bool kLearned>
 __device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const HydroConst& c, int cur, double dt,
-                                                  int64_t z, int64_t s0, double& zdthyd, int& nbad, int* cnt) {
+                                                  int64_t z, int64_t s0, double& zdthyd, int& nbad, int* cnt,
+                                                  const SideSpill& sp) {
     const double2* __restrict__ px0 = a.px[cur];
     const double2* __restrict__ pu0 = a.pu[cur];
     double2 xp[N];
@@ -268,6 +281,25 @@ __device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const Hydr
     }
     const float zssf = (float)zss, zrpf = (float)zrp;
 
+    // The side forces that do not involve QCS, formed now so that the FP64
+    // positions, smf and side areas are dead during the corner loop: the
+    // PolyGas force in FP64 (its surface vectors cancel around the zone and
+    // calcWork takes the residual) and TTS in FP32, parked in shared memory.
+    {
+        float sstmp = fmaxf(zssf, (float)c.tts_ssmin);
+        sstmp = (float)c.alfa * sstmp * sstmp;
+        const float zareapf = (float)zareap;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const int nk = (k + 1 == N) ? 0 : k + 1;
+            const double2 ex64 = smul(0.5, add(xp[k], xp[nk]));
+            sp.sfp(k) = smul(-zp, mk(-(ex64.y - zxp.y), ex64.x - zxp.x));
+            const float2 ssurf = fk(-(ex[k].y - zc.y), ex[k].x - zc.x);
+            const float srho = zrpf * (float)mf[k] * (zareapf / (float)sa[k]);
+            sp.sft(k) = fmul(-(sstmp * (srho - zrpf)), ssurf);
+        }
+    }
+
     // QCS corners (QCS.cc:116-380), FP32; sin^2 of the corner angle as
     // (4 cross / (de1 de2))^2 (the reference's 1 - ccos^2 loses the small
     // sines of acute corners in FP32); zones with a corner under ~30 degrees
@@ -326,10 +358,12 @@ __device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const Hydr
             const float ztmp1 = (float)c.q1 * zssf;
             crmu = (ztmp2 + sqrtf(ztmp2 * ztmp2 + ztmp1 * ztmp1)) * zrpf * evol;
         }
-        cqe1[k] = fmul(crmu * rinv[pk], fsub(up0, uf[pk]));
-        cqe2[k] = fmul(crmu * rinv[k], fsub(uf[nk], up0));
-        cw[k] = (csin2 < 1.e-4f) ? 0.f : cvolume / csin2;
-        cc[k] = (csin2 < 1.e-4f) ? 0.f : ccos;
+        if constexpr (!kLearned) {
+            cqe1[k] = fmul(crmu * rinv[pk], fsub(up0, uf[pk]));
+            cqe2[k] = fmul(crmu * rinv[k], fsub(uf[nk], up0));
+            cw[k] = (csin2 < 1.e-4f) ? 0.f : cvolume / csin2;
+            cc[k] = (csin2 < 1.e-4f) ? 0.f : ccos;
+        }
     }
     if constexpr (kLearned) {
         if (acute) {   // the zone keeps the FP64 QCS: its corners are counted as acute
@@ -370,16 +404,29 @@ __device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const Hydr
             a.closure_zhdr[idx] = make_int2((int)s0, N);
         }
     }
+    // QCS::setForce (QCS.cc:331-380); in the learned cycle no corner outside
+    // an acute zone has a QCS force here (the closure pass adds the deferred
+    // ones), so sfq starts at zero there
     float2 sfq[N];
 #pragma unroll
     for (int k = 0; k < N; ++k) {
         const int nk = (k + 1 == N) ? 0 : k + 1;
-        sfq[k] = fmul(rinv[k], fadd(fmul(cw[k], fadd(cqe2[k], fmul(cc[k], cqe1[k]))),
-                                    fmul(cw[nk], fadd(cqe1[nk], fmul(cc[nk], cqe2[nk])))));
+        if constexpr (kLearned)
+            sfq[k] = fk(0.f, 0.f);
+        else
+            sfq[k] = fmul(rinv[k], fadd(fmul(cw[k], fadd(cqe2[k], fmul(cc[k], cqe1[k]))),
+                                        fmul(cw[nk], fadd(cqe1[nk], fmul(cc[nk], cqe2[nk])))));
     }
     if (acute) {
-        double2 q64[N];
-        qcs_sfq_fp64_zone<N>(a, c, cur, s0, xp, zxp, zss, zrp, q64);
+        // the half-step positions again (advPosHalf, as above), for the
+        // FP64 QCS of this rare zone
+        double2 xq[N], q64[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const int32_t p = __ldg(a.mapsp1 + s0 + k);
+            xq[k] = add(a.px[cur][p], smul(dth, a.pu[cur][p]));
+        }
+        qcs_sfq_fp64_zone<N>(a, c, cur, s0, xq, zxp, zss, zrp, q64);
 #pragma unroll
         for (int k = 0; k < N; ++k) sfq[k] = f2(q64[k]);
     }
@@ -395,22 +442,12 @@ __device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const Hydr
     const double cdu = dmax(zdu, dmax(zss, 1.e-99));
     zdthyd = (double)zdl * c.cfl / cdu;
 
-    // side forces: PolyGas in FP64 (its surface vectors cancel around the
-    // zone and calcWork takes the residual), TTS in FP32; corner force and
-    // sfp + sfq for calcWork
-    float sstmp = fmaxf(zssf, (float)c.tts_ssmin);
-    sstmp = (float)c.alfa * sstmp * sstmp;
-    const float zareapf = (float)zareap;
+    // corner force and sfp + sfq for calcWork
     double2 ftot[N];
 #pragma unroll
     for (int k = 0; k < N; ++k) {
-        const int nk = (k + 1 == N) ? 0 : k + 1;
-        const double2 ex64 = smul(0.5, add(xp[k], xp[nk]));
-        const double2 sfp = smul(-zp, mk(-(ex64.y - zxp.y), ex64.x - zxp.x));
-        const float2 ssurf = fk(-(ex[k].y - zc.y), ex[k].x - zc.x);
-        const float srho = zrpf * (float)mf[k] * (zareapf / (float)sa[k]);
-        const float2 sft = fmul(-(sstmp * (srho - zrpf)), ssurf);
-        const double2 sfpq = add(sfp, mk((double)sfq[k].x, (double)sfq[k].y));
+        const float2 sft = sp.sft(k);
+        const double2 sfpq = add(sp.sfp(k), mk((double)sfq[k].x, (double)sfq[k].y));
         ftot[k] = add(sfpq, mk((double)sft.x, (double)sft.y));
         a.sftot[s0 + k] = sfpq;
     }
@@ -421,7 +458,6 @@ __device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const Hydr
 #ifndef PNT_MIXED_ZT_MIN_BLOCKS
 #define PNT_MIXED_ZT_MIN_BLOCKS 4
 #endif
-constexpr int kZoneThreadsZT = 128;   // one zone per thread
 
 template <bool kQuads, bool kLearned>
 __global__ void __launch_bounds__(kZoneThreadsZT, PNT_MIXED_ZT_MIN_BLOCKS) pass_a_mixed_zt(DevArrays a, HydroConst c) {
@@ -431,16 +467,19 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_MIXED_ZT_MIN_BLOCKS) pass_
     double zdthyd = 1.e99;
     int bad = 0;
     int cnt[3] = {0, 0, 0};
+    __shared__ double2 s_sfp[4 * kZoneThreadsZT];
+    __shared__ float2 s_sft[4 * kZoneThreadsZT];
+    const SideSpill sp{s_sfp, s_sft, (int)threadIdx.x};
     if (z < a.numz) {
         const int cur = ctl->cycle & 1;
         const double dt = ctl->dt;
         if (kQuads) {
-            pass_a_mixed_zone<4, kLearned>(a, c, cur, dt, z, 4 * z, zdthyd, bad, cnt);
+            pass_a_mixed_zone<4, kLearned>(a, c, cur, dt, z, 4 * z, zdthyd, bad, cnt, sp);
         } else {
             const int n = a.znump[z];
             const int64_t s0 = a.zfirst[z];
-            if (n == 4) pass_a_mixed_zone<4, kLearned>(a, c, cur, dt, z, s0, zdthyd, bad, cnt);
-            else pass_a_mixed_zone<3, kLearned>(a, c, cur, dt, z, s0, zdthyd, bad, cnt);
+            if (n == 4) pass_a_mixed_zone<4, kLearned>(a, c, cur, dt, z, s0, zdthyd, bad, cnt, sp);
+            else pass_a_mixed_zone<3, kLearned>(a, c, cur, dt, z, s0, zdthyd, bad, cnt, sp);
         }
     }
     __shared__ unsigned wcount[kLearned ? kZoneThreadsZT / 32 : 1][3];
