@@ -235,24 +235,31 @@ __device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const Hydr
         zvolp = (k == 0) ? sv : zvolp + sv;
         nbad += (sv <= 0.) ? 1 : 0;
     }
-    // FP64 zone EOS and density (PolyGas.cc:63-109, Hydro.cc:1034-1054)
+    // Zone EOS and density (PolyGas.cc:63-109, Hydro.cc:1034-1054): the
+    // half-step pressure zp in FP64 (it feeds the FP64 pressure force); the
+    // sound speed and the half-step density feed only FP32 quantities (TTS,
+    // QCS, the corner mass, the Courant dt), so they are formed in FP32.
+    // q = per p / zr^2 is written gm1 pre (the same quantity, no division).
     const double e = dmax(ze, 0.);
     const double p = c.gm1 * zr * e;
     const double pre = c.gm1 * e;
     const double per = c.gm1 * zr;
-    const double q = (per * p) / (zr * zr);
+    const double q = c.gm1 * pre;
     const double minv = 1. / zm;
     const double csqd = dmax(c.ssmin2, pre + q);
-    const double zss = sqrt(csqd);
     const double dv = (zvolp - zvol0) * minv;
     const double bulk = zr * csqd;
     const double denom = 1. + 0.5 * per * dv;
     const double src = zwrate * dth * minv;
-    const double zrp = zm / zvolp;
     const double zp = p + (per * src - zr * bulk * dv) / denom;
+    const float zssf = sqrtf((float)csqd);
+    const float zrpf = (float)zm / (float)zvolp;
+    {
+        const float hz = 0.5f * zrpf * (float)zareap;
 #pragma unroll
-    for (int k = 0; k < N; ++k)
-        a.cmass_f[s0 + k] = (float)(zrp * zareap * 0.5 * (mf[k] + mf[(k == 0) ? N - 1 : k - 1]));
+        for (int k = 0; k < N; ++k)
+            a.cmass_f[s0 + k] = hz * ((float)mf[k] + (float)mf[(k == 0) ? N - 1 : k - 1]);
+    }
     a.zp[z] = zp;
 
     // FP32 from here, relative to the zone's first point
@@ -279,7 +286,6 @@ __device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const Hydr
         rinv[k] = 1.f / elen[k];
         zdl = fminf(zdl, fac * (float)sa[k] / elen[k]);
     }
-    const float zssf = (float)zss, zrpf = (float)zrp;
 
     // The side forces that do not involve QCS, formed now so that the FP64
     // positions, smf and side areas are dead during the corner loop: the
@@ -426,7 +432,7 @@ __device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const Hydr
             const int32_t p = __ldg(a.mapsp1 + s0 + k);
             xq[k] = add(a.px[cur][p], smul(dth, a.pu[cur][p]));
         }
-        qcs_sfq_fp64_zone<N>(a, c, cur, s0, xq, zxp, zss, zrp, q64);
+        qcs_sfq_fp64_zone<N>(a, c, cur, s0, xq, zxp, (double)zssf, (double)zrpf, q64);
 #pragma unroll
         for (int k = 0; k < N; ++k) sfq[k] = f2(q64[k]);
     }
@@ -438,9 +444,9 @@ __device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const Hydr
         const float dux = fabsf(fdot(fsub(uf[nk], uf[k]), fsub(r[nk], r[k]))) * rinv[k];
         ztmp = fmaxf(ztmp, (elen[k] > 0.f) ? dux : 0.f);
     }
-    const double zdu = c.q1 * zss + 2. * c.q2 * (double)ztmp;
-    const double cdu = dmax(zdu, dmax(zss, 1.e-99));
-    zdthyd = (double)zdl * c.cfl / cdu;
+    const float zdu = (float)c.q1 * zssf + 2.f * (float)c.q2 * ztmp;
+    const float cdu = fmaxf(zdu, fmaxf(zssf, 1.e-30f));
+    zdthyd = (double)(zdl * (float)c.cfl / cdu);
 
     // corner force and sfp + sfq for calcWork
     double2 ftot[N];
