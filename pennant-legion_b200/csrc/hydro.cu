@@ -272,15 +272,13 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
     int32_t *zfirst, *znump, *mapsp1, *poff, *pcorner;
     double* smf;
     uint16_t* mask;
-    const int64_t nzb = zone_blocks((int32_t)nz);
-    // pass C is persistent: one partial per CTA of its grid
+    // the persistent pass C's grid
     {
         int nsm = 148;
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
         const cudaError_t e = prepare_pass_c(p.precision != PNT_PREC_FP64, a.quads != 0, a.numz, nsm, &a.gridC);
         if (e != cudaSuccess) return fail(PNT_ERR_CUDA, "pass C setup: %s", cudaGetErrorString(e));
     }
-    const int64_t nzbc = a.gridC;
     pnt_status st = PNT_OK;
     if ((st = h->alloc(&zfirst, nz)) || (st = h->alloc(&znump, nz)) || (st = h->alloc(&mapsp1, ns)) ||
         (st = h->alloc(&smf, ns)) || (st = h->alloc(&poff, np + 1)) || (st = h->alloc(&pcorner, m.pcorner.size())) ||
@@ -289,13 +287,8 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
         (st = h->alloc(&a.zr, nz)) || (st = h->alloc(&a.ze, nz)) || (st = h->alloc(&a.zetot, nz)) ||
         (st = h->alloc(&a.zwrate, nz)) || (st = h->alloc(&a.zvol, nz)) || (st = h->alloc(&a.zp, nz)) ||
         (st = h->alloc(&a.cmass, ns + m.nhalo)) || (st = h->alloc(&a.cforce, ns + m.nhalo)) || (st = h->alloc(&a.sftot, ns)) ||
-        (st = h->alloc(&a.part_dtnew, nzb)) || (st = h->alloc(&a.part_badA, nzb)) ||
-        (st = h->alloc(&a.part_dvov, nzbc)) || (st = h->alloc(&a.part_badC, nzbc)) ||
-        (st = h->alloc(&a.fin_part, 2 * kFinBlocks)) || (st = h->alloc(&a.fin_bad, 2 * kFinBlocks)) ||
-        (st = h->alloc(&a.fin_ticket, 1)) || (st = h->alloc(&a.ctl, 1)))
+        (st = h->alloc(&a.cyc_red, 4)) || (st = h->alloc(&a.fin_ticket, 1)) || (st = h->alloc(&a.ctl, 1)))
         return st;
-    a.npartA = (int32_t)nzb;
-    a.npartC = (int32_t)nzbc;
     a.cmass_f = reinterpret_cast<float*>(a.cmass);
     a.cforce_f = reinterpret_cast<float2*>(a.cforce);
     a.sftot_f = reinterpret_cast<float2*>(a.sftot);
@@ -336,6 +329,14 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
     ctl.done = (p.cstop <= 0 || !(0. < p.tstop)) ? 1 : 0;
     ctl.stop_at = INT_MAX;
 
+    // the cycle reductions' starting values: minimum from 1e99, maximum
+    // from 1e-99 (keys of positive doubles are their bits), no bad sides
+    long long cyc_red_init[4] = {0, 0, 0, 0};
+    {
+        const double lo = 1.e99, hi = 1.e-99;
+        std::memcpy(&cyc_red_init[0], &lo, 8);
+        std::memcpy(&cyc_red_init[1], &hi, 8);
+    }
     cudaStream_t s = h->stream;
     auto up = [&](void* dst, const void* src, size_t bytes) {
         return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
@@ -348,7 +349,8 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
         (e = up(a.pu[0], pu.data(), np * 16)) || (e = up(a.zm, zm.data(), nz * 8)) ||
         (e = up(a.zr, zr.data(), nz * 8)) || (e = up(a.ze, ze.data(), nz * 8)) ||
         (e = up(a.zetot, zetot.data(), nz * 8)) || (e = up(a.zwrate, zwrate.data(), nz * 8)) ||
-        (e = up(a.zvol, m.zvol.data(), nz * 8)) || (e = up(a.ctl, &ctl, sizeof(Ctl))))
+        (e = up(a.zvol, m.zvol.data(), nz * 8)) || (e = up(a.ctl, &ctl, sizeof(Ctl))) ||
+        (e = up(a.cyc_red, cyc_red_init, sizeof(cyc_red_init))))
         return fail(PNT_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
     if ((e = cudaMemsetAsync(a.zp, 0, nz * 8, s)) || (e = cudaMemsetAsync(a.fin_ticket, 0, 4, s)) ||
         (e = cudaMemsetAsync(mask + np, 0, 4, s)) ||

@@ -70,16 +70,19 @@ struct DevArrays {
     float* cmass_f;
     float2* cforce_f;
     float2* sftot_f;
-    // per-block partial reductions (npartA entries for pass A, npartC for C)
+    // batched meshes: per-tile partial reductions (npartA entries for pass
+    // A, npartC for C)
     int32_t npartA, npartC;
     double* part_dtnew;
     int32_t* part_badA;
     double* part_dvov;
     int32_t* part_badC;
-    // the finalize blocks' results (kFinBlocks each of dt, dvov / bad
-    // counts) and the ticket that picks the last block
-    double* fin_part;
-    int32_t* fin_bad;
+    // one mesh: the cycle's reductions, combined by every CTA of passes A
+    // and C with atomics ([0] minimum zone dt and [1] maximum |dV/V0| as
+    // order-preserving keys (dkey), [2] / [3] inverted sides in A / C), and
+    // the ticket that picks pass C's last CTA, which ends the cycle and
+    // resets them
+    long long* cyc_red;
     uint32_t* fin_ticket;
     Ctl* ctl;
     // learned closure (precision = learned): parameter image and the corner
@@ -93,7 +96,7 @@ struct DevArrays {
     int32_t* closure_nrec;
     int32_t closure_grid;   // CTAs of the persistent closure pass
     int32_t gridC;          // CTAs of the persistent pass C (pass_c_staged.cuh)
-    // multi-piece runs: the finalize step writes this piece's [dtnew,
+    // multi-piece runs: pass C's last CTA writes this piece's [dtnew,
     // -dvovmax, inverted sides in A, in C] here instead of ending the cycle
     // (nullptr for a single piece)
     double* piece_red;
@@ -109,7 +112,6 @@ inline int64_t zone_blocks(int32_t numz, int threads = kZoneThreads) {
 // Events a cycle records when timed: before pass A, after A, after the
 // closure pass (right after A when there is none), after B, C, finalize.
 constexpr int kNumEvents = 6;
-constexpr int kFinBlocks = 64;   // blocks of the finalize reduction
 constexpr int kNumKernels = 5;   // A, B, C, finalize, closure pass
 
 // Phases of a cycle: the corner forces (pass A and the learned closure
@@ -145,8 +147,6 @@ cudaError_t prepare_learned_kernels();
 // write a.gridC partials.
 cudaError_t prepare_pass_c(bool mixed, bool quads, int32_t numz, int nsm, int32_t* grid);
 void launch_pass_c(const DevArrays& a, const HydroConst& c, bool mixed, cudaStream_t stream);
-// The finalize step shared by both cycles (nA / nC partials of passes A / C).
-void launch_finalize(const DevArrays& a, const HydroConst& c, int nA, int nC, cudaStream_t stream);
 
 // Device state of a pnt_hydro for the closure harvest (closure.cu).
 struct HydroAccess {

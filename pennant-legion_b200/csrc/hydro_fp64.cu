@@ -1,6 +1,6 @@
 // hydro_fp64.cu -- the plain FP64 hydro cycle on sm_100a (one mesh).
 //
-// One cycle of Hydro::doCycle (Hydro.cc:342-983) runs as four kernels:
+// One cycle of Hydro::doCycle (Hydro.cc:342-983) runs as three kernels:
 //
 //   pass A  zone pass, predictor: advPosHalf, calcCtrs, calcVols,
 //           calcSurfVecs, calcEdgeLen, calcCharLen, calcRho, calcCrnrMass,
@@ -11,9 +11,11 @@
 //           point->corner CSR in ascending side order (no float atomics),
 //           applyFixedBC, calcAccel, advPosFull
 //   pass C  zone pass, corrector: calcCtrs, calcVols, calcWork,
-//           calcWorkRate, calcEnergy, calcRho, calcDvol (block maximum)
-//   finalize  calcDt, checkBadSides, time/cycle update and the next
-//           cycle's calcGlobalDt (Driver.cc:213-245), all on the device
+//           calcWorkRate, calcEnergy, calcRho, calcDvol (block maximum);
+//           its last CTA then runs calcDt, checkBadSides, the time/cycle
+//           update and the next cycle's calcGlobalDt (Driver.cc:213-245)
+// Passes A and C add their blocks' dt minimum, dV/V maximum and inverted
+// sides to the cycle's reductions with atomics (exact in any order).
 //
 // Pass A runs one thread per zone (pass_a_zone_thread): the zone's sides
 // in the reference's side order, each zone-level quantity (centre, sums,
@@ -63,9 +65,7 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_PASS_A_ZT_MIN_BLOCKS) pass
         }
     }
     const int nbad = tiles::block_isum<kZoneThreadsZT>(bad);
-    if (blockIdx.x >= (unsigned)a.npartA) return;   // partials are sized for this grid
-    block_fold<true, kZoneThreadsZT>(zdthyd, a.part_dtnew + blockIdx.x);
-    if (threadIdx.x == 0) a.part_badA[blockIdx.x] = nbad;
+    block_to_cycle<true, kZoneThreadsZT>(a.cyc_red, zdthyd, nbad);
 }
 
 __global__ void __launch_bounds__(kPointThreads) pass_b(DevArrays a, HydroConst c) {
@@ -74,89 +74,6 @@ __global__ void __launch_bounds__(kPointThreads) pass_b(DevArrays a, HydroConst 
     const int64_t p = (int64_t)blockIdx.x * kPointThreads + threadIdx.x;
     if (p >= a.nump) return;
     pass_b_point(a, c, ctl->cycle & 1, ctl->dt, p);
-}
-
-// finalize: kFinBlocks blocks reduce slices of the pass A / pass C
-// partials; the last block to finish (ticket counter) reduces the blocks'
-// results and ends the cycle.  Minimum, maximum and integer sums are exact
-// in any order, so the result does not depend on which block is last.
-constexpr int kFinThreads = 512;
-
-__device__ __forceinline__ void fin_block_reduce(double& dtn, double& dvm, int& badA, int& badC) {
-    __shared__ double sdt[kFinThreads / 32], sdv[kFinThreads / 32];
-    __shared__ int sba[kFinThreads / 32], sbc[kFinThreads / 32];
-    for (int o = 16; o > 0; o >>= 1) {
-        dtn = dmin(dtn, __shfl_xor_sync(kFull, dtn, o));
-        const double w = __shfl_xor_sync(kFull, dvm, o);
-        dvm = (w > dvm) ? w : dvm;
-        badA += __shfl_xor_sync(kFull, badA, o);
-        badC += __shfl_xor_sync(kFull, badC, o);
-    }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) { sdt[warp] = dtn; sdv[warp] = dvm; sba[warp] = badA; sbc[warp] = badC; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int i = 1; i < kFinThreads / 32; ++i) {
-            dtn = dmin(dtn, sdt[i]);
-            dvm = (sdv[i] > dvm) ? sdv[i] : dvm;
-        }
-        badA = 0;
-        badC = 0;
-        for (int i = 0; i < kFinThreads / 32; ++i) { badA += sba[i]; badC += sbc[i]; }
-    }
-    __syncthreads();   // the shared slots are reused by the last block
-}
-
-__global__ void __launch_bounds__(kFinThreads) finalize(DevArrays a, HydroConst c, int nblocksA, int nblocksC) {
-    Ctl* ctl = a.ctl;
-    if (skip_cycle(ctl)) return;
-    double dtn = 1.e99, dvm = 1.e-99;
-    int badA = 0, badC = 0;
-    const int stride = gridDim.x * kFinThreads;
-    for (int i = blockIdx.x * kFinThreads + threadIdx.x; i < nblocksA; i += stride) {
-        dtn = dmin(dtn, a.part_dtnew[i]);
-        badA += a.part_badA[i];
-    }
-    for (int i = blockIdx.x * kFinThreads + threadIdx.x; i < nblocksC; i += stride) {
-        const double v = a.part_dvov[i];
-        dvm = (v > dvm) ? v : dvm;
-        badC += a.part_badC[i];
-    }
-    fin_block_reduce(dtn, dvm, badA, badC);
-    __shared__ bool last;
-    if (threadIdx.x == 0) {
-        a.fin_part[blockIdx.x] = dtn;
-        a.fin_part[kFinBlocks + blockIdx.x] = dvm;
-        a.fin_bad[blockIdx.x] = badA;
-        a.fin_bad[kFinBlocks + blockIdx.x] = badC;
-        __threadfence();
-        last = atomicAdd(a.fin_ticket, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    dtn = 1.e99;
-    dvm = 1.e-99;
-    badA = badC = 0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += kFinThreads) {
-        dtn = dmin(dtn, __ldcg(a.fin_part + i));
-        const double v = __ldcg(a.fin_part + kFinBlocks + i);
-        dvm = (v > dvm) ? v : dvm;
-        badA += __ldcg(a.fin_bad + i);
-        badC += __ldcg(a.fin_bad + kFinBlocks + i);
-    }
-    fin_block_reduce(dtn, dvm, badA, badC);
-    if (threadIdx.x == 0) {
-        *a.fin_ticket = 0u;
-        if (a.piece_red) {   // a piece: the caller reduces over pieces, then piece_finish
-            a.piece_red[0] = dtn;
-            a.piece_red[1] = -dvm;
-            a.piece_red[2] = (double)badA;
-            a.piece_red[3] = (double)badC;
-        } else {
-            finish_cycle(ctl, c, dtn, dvm, badA, badC);
-        }
-    }
 }
 
 // Multi-piece runs: the corner values the neighbours need, and the end of
@@ -198,10 +115,9 @@ cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStrea
     if (phases & kPhaseAdvance) {
         pass_b<<<pb, kPointThreads, 0, stream>>>(a, c);
         if (ev) cudaEventRecord(ev[3], stream);
-        launch_pass_c(a, c, false, stream);
+        launch_pass_c(a, c, false, stream);   // its last CTA ends the cycle
         if (ev) cudaEventRecord(ev[4], stream);
-        finalize<<<kFinBlocks, kFinThreads, 0, stream>>>(a, c, zba, a.gridC);
-        if (ev) cudaEventRecord(ev[5], stream);
+        if (ev) cudaEventRecord(ev[5], stream);   // no separate finalize step
     }
     return cudaGetLastError();
 }
@@ -215,8 +131,5 @@ void launch_piece_finish(const DevArrays& a, const HydroConst& c, cudaStream_t s
     piece_finish<<<1, 1, 0, stream>>>(a, c);
 }
 
-void launch_finalize(const DevArrays& a, const HydroConst& c, int nA, int nC, cudaStream_t stream) {
-    finalize<<<kFinBlocks, kFinThreads, 0, stream>>>(a, c, nA, nC);
-}
 
 }  // namespace pnt

@@ -66,10 +66,10 @@ __device__ __forceinline__ bool skip_cycle(const Ctl* ctl) {
     return ctl->done || ctl->cycle >= ctl->stop_at;
 }
 
-// Block-wide min (dt) / max (dvov) in the reference fold semantics, and a
-// count.  Writes one partial per block.
+// Block-wide min (dt) / max (dvov) in the reference fold semantics; the
+// result is valid in thread 0.
 template <bool kMin, int kThreads>
-__device__ __forceinline__ void block_fold(double v, double* out) {
+__device__ __forceinline__ double block_fold_value(double v) {
     __shared__ double red[kThreads / 32];
     for (int o = 16; o > 0; o >>= 1) {
         const double w = __shfl_xor_sync(kFull, v, o);
@@ -78,10 +78,44 @@ __device__ __forceinline__ void block_fold(double v, double* out) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) red[warp] = v;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double r = red[0];
+    double r = red[0];
+    if (threadIdx.x == 0)
         for (int i = 1; i < kThreads / 32; ++i) r = kMin ? dmin(r, red[i]) : ((red[i] > r) ? red[i] : r);
-        *out = r;
+    return r;
+}
+
+// The same, written to *out (one partial per block).
+template <bool kMin, int kThreads>
+__device__ __forceinline__ void block_fold(double v, double* out) {
+    const double r = block_fold_value<kMin, kThreads>(v);
+    if (threadIdx.x == 0) *out = r;
+}
+
+// Order-preserving 64-bit keys of doubles: dkey(x) < dkey(y) iff x < y for
+// any two non-NaN values, so a minimum or maximum over keys with integer
+// atomics is exact in any order.
+__device__ __forceinline__ long long dkey(double d) {
+    const long long b = __double_as_longlong(d);
+    return b ^ ((b >> 63) & 0x7fffffffffffffffLL);
+}
+__device__ __forceinline__ double dkey_value(long long k) {
+    return __longlong_as_double(k ^ ((k >> 63) & 0x7fffffffffffffffLL));
+}
+
+// A block's share of the cycle reductions (one mesh): its minimum zone dt
+// (pass A) or maximum |dV/V0| (pass C) into cyc_red[0] / [1], its inverted
+// sides into [2] / [3].  A NaN result is left out, as the serial fold leaves
+// NaN out after its first value.
+template <bool kPassA, int kThreads>
+__device__ __forceinline__ void block_to_cycle(long long* cyc_red, double v, int nbad) {
+    const double r = block_fold_value<kPassA, kThreads>(v);
+    if (threadIdx.x == 0) {
+        if (r == r) {
+            if (kPassA) atomicMin(cyc_red, dkey(r));
+            else atomicMax(cyc_red + 1, dkey(r));
+        }
+        if (nbad)
+            atomicAdd(reinterpret_cast<unsigned long long*>(cyc_red + (kPassA ? 2 : 3)), (unsigned long long)nbad);
     }
 }
 
@@ -337,6 +371,35 @@ __device__ __forceinline__ void finish_cycle(Ctl* ctl, const HydroConst& c, doub
     if (dtrec < ndt) ndt = dtrec;
     ctl->dt = ndt;
     ctl->dtinv = 1. / ndt;
+}
+
+// Pass C's CTAs, after their block_to_cycle: the last one to finish
+// (ticket) takes the cycle's reductions, resets them for the next cycle and
+// ends the cycle, or, in a multi-piece run, hands this piece's values to
+// the caller (piece_red).  Called by every thread of the CTA.
+__device__ __forceinline__ void end_cycle_if_last(const DevArrays& a, const HydroConst& c) {
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(a.fin_ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    unsigned long long* r = reinterpret_cast<unsigned long long*>(a.cyc_red);
+    const double dtn = dkey_value((long long)atomicExch(r, (unsigned long long)dkey(1.e99)));
+    const double dvm = dkey_value((long long)atomicExch(r + 1, (unsigned long long)dkey(1.e-99)));
+    const int badA = (int)atomicExch(r + 2, 0ull);
+    const int badC = (int)atomicExch(r + 3, 0ull);
+    *a.fin_ticket = 0u;
+    if (a.piece_red) {
+        a.piece_red[0] = dtn;
+        a.piece_red[1] = -dvm;
+        a.piece_red[2] = (double)badA;
+        a.piece_red[3] = (double)badC;
+    } else {
+        finish_cycle(a.ctl, c, dtn, dvm, badA, badC);
+    }
 }
 
 }  // namespace fp64

@@ -28,6 +28,7 @@
 // Compiled with fast math; the accuracy of this path is stated as its L1
 // error against the FP64 run (tests/test_gpu_mixed.py).
 #include "closure_dev.cuh"
+#include "hydro_fp64_body.cuh"
 #include "hydro_dev.h"
 #include "zone_tiles.cuh"
 
@@ -504,9 +505,7 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_MIXED_ZT_MIN_BLOCKS) pass_
             if (t) atomicAdd(a.closure_counts + kCounted[threadIdx.x] * 64 + (blockIdx.x & 63), (unsigned long long)t);
         }
     }
-    if (blockIdx.x >= (unsigned)a.npartA) return;   // partials are sized for this grid
-    block_fold<true, kZoneThreadsZT>(zdthyd, a.part_dtnew + blockIdx.x);
-    if (threadIdx.x == 0) a.part_badA[blockIdx.x] = nbad;
+    fp64::block_to_cycle<true, kZoneThreadsZT>(a.cyc_red, zdthyd, nbad);
 }
 
 // ---------------------------------------------------------------------
@@ -720,10 +719,9 @@ cudaError_t launch_cycle_mixed_impl(const DevArrays& a, const HydroConst& c, cud
     if (phases & kPhaseAdvance) {
         pass_b_mixed<<<pb, kPointThreads, 0, stream>>>(a, c);
         if (ev) cudaEventRecord(ev[3], stream);
-        launch_pass_c(a, c, true, stream);
+        launch_pass_c(a, c, true, stream);   // its last CTA ends the cycle
         if (ev) cudaEventRecord(ev[4], stream);
-        launch_finalize(a, c, zba, a.gridC, stream);
-        if (ev) cudaEventRecord(ev[5], stream);
+        if (ev) cudaEventRecord(ev[5], stream);   // no separate finalize step
     }
     return cudaGetLastError();
 }

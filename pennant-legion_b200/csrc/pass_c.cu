@@ -3,9 +3,10 @@
 // calcDvol; Hydro.cc:924-983) as the persistent staged kernel of
 // pass_c_staged.cuh, in its FP64 form (bit-identical to a serial run of the
 // reference: this file is compiled with -fmad=false) and its mixed form
-// (the mixed and learned cycles).  Each CTA writes the maximum |dV/V0| and
-// the count of inverted sides over its tiles to part_dvov / part_badC
-// [blockIdx.x]; the finalize step reduces the gridC partials.
+// (the mixed and learned cycles).  Each CTA adds the maximum |dV/V0| and
+// the count of inverted sides over its tiles to the cycle's reductions; the
+// last CTA to finish ends the cycle (calcDt, checkBadSides, time/cycle, the
+// next calcGlobalDt), so a cycle needs no separate finalize launch.
 #include "hydro_fp64_body.cuh"
 #include "pass_c_staged.cuh"
 
@@ -20,8 +21,8 @@ __global__ void __launch_bounds__(stagedc::kTile) pass_c_staged(DevArrays a, Hyd
     int nbad = 0;
     stagedc::pass_c_tiles<kQuads, kMixed>(a, c, smem_c, dvm, nbad);
     const int nb = tiles::block_isum<stagedc::kTile>(nbad);
-    fp64::block_fold<false, stagedc::kTile>(dvm, a.part_dvov + blockIdx.x);
-    if (threadIdx.x == 0) a.part_badC[blockIdx.x] = nb;
+    fp64::block_to_cycle<false, stagedc::kTile>(a.cyc_red, dvm, nb);
+    fp64::end_cycle_if_last(a, c);
 }
 
 using Kernel = void (*)(DevArrays, HydroConst);
