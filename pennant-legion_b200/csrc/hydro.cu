@@ -5,6 +5,10 @@
 #include "hydro_dev.h"
 #include "pnt_internal.h"
 
+#ifndef PNT_CLOSURE_CTAS_PER_SM
+#define PNT_CLOSURE_CTAS_PER_SM 3
+#endif
+
 #include <algorithm>
 #include <chrono>
 #include <climits>
@@ -765,7 +769,9 @@ pnt_status pnt_hydro_set_closure(pnt_hydro* h, const pnt_closure* c, int32_t mod
         h->a.closure_rec = rec;
         h->a.closure_zhdr = hdr;
         h->a.closure_nrec = nrec;
-        h->a.closure_grid = 3 * nsm;   // 3 x 128 TMEM columns and 3 x 54 KB shared memory per SM
+        // 128 TMEM columns and 54 KB of shared memory per CTA; 3 per SM (4, at
+        // 64 registers, measured slower: more CTAs pay the image setup)
+        h->a.closure_grid = PNT_CLOSURE_CTAS_PER_SM * nsm;
     }
     // the image lives in this object: a copy of the closure's, with the mode
     uint8_t* img = const_cast<uint8_t*>(h->a.closure_img);

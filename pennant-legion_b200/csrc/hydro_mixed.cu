@@ -564,7 +564,10 @@ __global__ void __launch_bounds__(kPointThreads) pass_b_mixed(DevArrays a, Hydro
 // which only touch the recorded zone's own sides: no two records write the
 // same side, so the update is deterministic without atomics.
 // ---------------------------------------------------------------------
-__global__ void __launch_bounds__(kMlpRows, 3) closure_pass(DevArrays a, HydroConst c) {
+#ifndef PNT_CLOSURE_MIN_BLOCKS
+#define PNT_CLOSURE_MIN_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(kMlpRows, PNT_CLOSURE_MIN_BLOCKS) closure_pass(DevArrays a, HydroConst c) {
     if (skip_cycle(a.ctl)) return;
     const int nrec = *a.closure_nrec;
     if (blockIdx.x == 0 && threadIdx.x == 0 && nrec)
