@@ -226,7 +226,8 @@ pnt_status pnt_hydro_get_scalars(pnt_hydro* hydro, pnt_scalars* out);
  * Driver.cc:117-168): runs `ncycles` cycles launching each pass separately
  * with CUDA events around it and writes the mean milliseconds of pass i to
  * kernel_ms[i] for i < nkernels (0 pass A zone predictor, 1 pass B point
- * update, 2 pass C zone corrector, 3 finalize, 4 the learned cycle's closure
+ * update, 2 pass C zone corrector, which also ends the cycle, 3 a separate
+ * end-of-cycle step (none any more: about 0), 4 the learned cycle's closure
  * pass, 0 for the other cycles). */
 pnt_status pnt_hydro_time_kernels(pnt_hydro* hydro, int32_t ncycles, double* kernel_ms,
                                   int32_t nkernels);

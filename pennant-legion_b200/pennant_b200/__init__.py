@@ -361,7 +361,8 @@ class Hydro:
         check(lib.pnt_hydro_enqueue(self.h, ncycles))
 
     def time_kernels(self, ncycles: int) -> list:
-        """Mean ms of passes A, B, C, finalize and the closure pass over `ncycles`
+        """Mean ms of passes A, B, C (which ends the cycle), a separate
+        end-of-cycle step (none: about 0) and the closure pass over `ncycles`
         (these cycles advance the run)."""
         out = (C.c_double * 5)()
         check(lib.pnt_hydro_time_kernels(self.h, ncycles, out, 5))
