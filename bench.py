@@ -494,7 +494,7 @@ def main():
         full["1920"] = full_run(1920)
 
     hbm, peak_kind = measured_peaks()
-    names = ["A", "B", "C", "finalize", "closure"]
+    names = ["A", "B", "C", "end_of_cycle", "closure"]   # end_of_cycle: folded into C, ~0
     kms_head = res[args.precision]["kernel_ms"]
     dom = int(np.argmax(kms_head[:3]))
     if args.precision in ("mixed", "learned"):
@@ -548,12 +548,14 @@ def main():
     if rank == 0:
         paths = {
             "learned": "learned closure + mixed precision: the 14-64-64-4 BF16 network (tcgen05) in place of QCS "
-                       "on compressing corners within its range, plain QCS elsewhere; FP32 side geometry and "
-                       "TTS/QCS forces, FP64 point kinematics, volumes, EOS, work and dt",
-            "mixed": "mixed precision: FP32 edge/corner geometry and TTS/QCS side forces, FP64 point kinematics, "
-                     "volumes, EOS, work and dt; plain QCS",
+                       "on compressing corners within its range, plain QCS elsewhere; FP32 side geometry, "
+                       "TTS/QCS forces, sound speed and zone dt, FP64 point kinematics, volumes, pressure, "
+                       "work and the dt reduction",
+            "mixed": "mixed precision: FP32 edge/corner geometry, TTS/QCS side forces, sound speed and zone dt, "
+                     "FP64 point kinematics, volumes, pressure, work and the dt reduction; plain QCS",
             "fp64": "plain FP64 (bitwise parity path)"}
-        launches = 5 if args.precision == "learned" else 4
+        # passes A, B, C (which ends the cycle), and the closure pass
+        launches = 4 if args.precision == "learned" else 3
         others = {p: {"value": res[p]["value"], "ms_per_step": res[p]["ms"] / args.steps,
                       "kernel_ms": dict(zip(names, res[p]["kernel_ms"]))} for p in order if p != args.precision}
         result = {
