@@ -357,7 +357,7 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
         (e = up(a.cyc_red, cyc_red_init, sizeof(cyc_red_init))))
         return fail(PNT_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
     if ((e = cudaMemsetAsync(a.zp, 0, nz * 8, s)) || (e = cudaMemsetAsync(a.fin_ticket, 0, 4, s)) ||
-        (e = cudaMemsetAsync(mask + np, 0, 4, s)) ||
+        (e = cudaMemsetAsync(mask + np, 0, 4, s)) ||   // pad: pass C copies whole 32-bit mask words
         (e = cudaMemsetAsync(a.px[1], 0, np * 16, s)) ||
         (e = cudaMemsetAsync(a.pu[1], 0, np * 16, s)))
         return fail(PNT_ERR_CUDA, "memset: %s", cudaGetErrorString(e));
