@@ -55,11 +55,11 @@ DEFAULT_DECK = os.path.join(PKG, "decks", "sedov1920.pnt")
 DEFAULT_CLOSURE = os.path.join(PKG, "closure", "qcs_mlp.bin")
 MLP_FLOP_PER_ROW = 2 * (16 * 64 + 64 * 64 + 64 * 16)   # tensor-core MMA shapes, padded
 # DRAM bytes (read + write) of one pass A launch per zone, from the ncu
-# capture of profiles/pass_a_closure_sedov1024.md (1,048,576 zones; the
+# capture of profiles/pass_a_pass_c_sedov1024.md (1,048,576 zones; the
 # bench scales them by its zone count)
-PASS_A_TRAFFIC_PER_ZONE = {"learned": (126.038e6 + 98.280e6) / 1048576,
-                           "mixed": (125.964e6 + 86.100e6) / 1048576,
-                           "fp64": (125.949e6 + 128.223e6) / 1048576}
+PASS_A_TRAFFIC_PER_ZONE = {"learned": (125.963e6 + 92.962e6) / 1048576,
+                           "mixed": (125.960e6 + 84.336e6) / 1048576,
+                           "fp64": (125.973e6 + 130.137e6) / 1048576}
 
 
 def algorithmic_bytes(nump, nums, numz):
