@@ -57,8 +57,10 @@ struct pnt_hydro {
     // host copies needed by the output writers
     std::vector<int32_t> znump, mapsp1;
     int32_t nump = 0, numz = 0, nums = 0;
-    // captured CUDA graph of graph_cycles cycles
+    // captured CUDA graphs of graph_cycles cycles and of one cycle (the
+    // single steps of pnt_hydro_cycle)
     cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph1 = nullptr;
     int graph_cycles = 0;
     // the cycle of the selected precision
     cudaError_t (*launch)(const DevArrays&, const HydroConst&, cudaStream_t, cudaEvent_t*, int) = launch_cycle_fp64;
@@ -78,6 +80,7 @@ struct pnt_hydro {
     ~pnt_hydro() {
         DeviceGuard dg(device);
         if (graph) cudaGraphExecDestroy(graph);
+        if (graph1) cudaGraphExecDestroy(graph1);
         for (void* p : allocs) cudaFree(p);
         if (ctl_host) cudaFreeHost(ctl_host);
         if (stream) cudaStreamDestroy(stream);
@@ -113,6 +116,27 @@ struct pnt_hydro {
         for (int i = 0; i < n; ++i) {
             const cudaError_t e = launch(a, hc, stream, nullptr, kPhaseAll);
             if (e != cudaSuccess) return fail(PNT_ERR_CUDA, "cycle launch: %s", cudaGetErrorString(e));
+        }
+        return PNT_OK;
+    }
+
+    // One cycle as a graph: one launch per step instead of one per kernel.
+    pnt_status ensure_graph1() {
+        if (graph1) return PNT_OK;
+        if (pnt_status st = check_ready()) return st;
+        cudaGraph_t g = nullptr;
+        CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t e = launch(a, hc, stream, nullptr, kPhaseAll);
+        const cudaError_t e2 = cudaStreamEndCapture(stream, &g);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return fail(PNT_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+        }
+        const cudaError_t e3 = cudaGraphInstantiate(&graph1, g, 0);
+        cudaGraphDestroy(g);
+        if (e3 != cudaSuccess) {
+            graph1 = nullptr;
+            return fail(PNT_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e3));
         }
         return PNT_OK;
     }
@@ -443,8 +467,10 @@ void pnt_hydro_destroy(pnt_hydro* h) { delete h; }
 pnt_status pnt_hydro_cycle(pnt_hydro* h, pnt_scalars* out) {
     if (!h) return fail(PNT_ERR_INVALID_ARG, "null argument");
     DeviceGuard dg(h->device);
-    pnt_status st = h->launch_cycles(1);
-    if (!st) st = h->fetch_ctl();
+    pnt_status st = h->ensure_graph1();
+    if (st) return st;
+    CUDA_TRY(cudaGraphLaunch(h->graph1, h->stream));
+    st = h->fetch_ctl();
     if (st) return st;
     h->scalars(out);
     if (h->ctl_host->status) return fail(h->ctl_host->status, "%d negative side volumes on cycle %d",
@@ -779,6 +805,10 @@ pnt_status pnt_hydro_set_closure(pnt_hydro* h, const pnt_closure* c, int32_t mod
     CUDA_TRY(cudaMemcpyAsync(img, pnt::closure_image(c), kImgBytes, cudaMemcpyDeviceToDevice, h->stream));
     CUDA_TRY(cudaMemcpyAsync(img + kImgThr + 12, &fmode, sizeof(float), cudaMemcpyHostToDevice, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (h->graph1) {   // the captured cycle holds the old DevArrays
+        cudaGraphExecDestroy(h->graph1);
+        h->graph1 = nullptr;
+    }
     if (h->graph) {   // the captured cycles hold the old DevArrays
         cudaGraphExecDestroy(h->graph);
         h->graph = nullptr;
