@@ -1,9 +1,11 @@
-"""Mixed-precision cycle (FP32 side forces, FP64 kinematics/work/dt) against
-the FP64 cycle, which is itself bit-identical to the CPU oracle.
+"""Mixed-precision cycle (FP32 side forces, sound speed and zone dt; FP64
+kinematics, pressure, work and the dt reduction) against the FP64 cycle,
+which is itself bit-identical to the CPU oracle.
 
 Every case states its relative L1 errors (sum |a - b| / sum |b|) of density,
-specific energy and point velocity; the bound asserted is the north star's
-1e-3 relative L1 density error, applied to all three fields.
+specific energy and point velocity; the bound asserted is the accuracy
+target of the reduced-precision paths, 1e-3 relative L1 density error,
+applied to all three fields.
 """
 import numpy as np
 import pytest
