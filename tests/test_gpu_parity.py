@@ -2,7 +2,7 @@
 
 The FP64 path is built to reproduce a serial run of the reference bit for
 bit: every state field and the dt sequence are compared with exact equality
-after every cycle.  The north-star bound is 1e-11 relative per field after
+after every cycle.  The accuracy bound of the FP64 path is 1e-11 relative per field after
 the run; bitwise equality is the stronger claim tested here, and the
 fingerprint test measures the relative error explicitly.
 """
@@ -20,7 +20,7 @@ import pennant_b200 as pb
 pytestmark = pytest.mark.gpu
 
 STATE = ("px", "pu", "zr", "ze", "zp", "zetot", "zvol", "zwrate")
-REL_TOL = 1e-11   # north-star bound for the FP64 path
+REL_TOL = 1e-11   # accuracy bound of the FP64 path
 
 
 def make_pair(path=None, text=None, **overrides):
