@@ -91,3 +91,21 @@ def test_pieces_match_the_single_piece_run_bitwise(case):
             assert f[k].tobytes() == f1[k][z].tobytes(), (case, r, k)
         for k in POINT:
             assert f[k].tobytes() == f1[k][info["gpoint"]].tobytes(), (case, r, k)
+
+
+def test_a_piece_refuses_whole_cycles_and_a_mesh_the_piece_calls():
+    """Whole cycles on a piece (no exchange) and piece steps on a mesh object
+    are state errors, not silent wrong answers."""
+    d = pb.Deck(text=sedov(8, tstop=0.01))
+    m = pb.Mesh(deck=d)
+    h = pb.Hydro(m.piece(2, 0), d.params())
+    for call in (h.cycle, lambda: h.run(), lambda: h.enqueue(1), lambda: h.time_cycles(1)):
+        with pytest.raises(pb.PntError) as e:
+            call()
+        assert e.value.status == pb.PNT_ERR_STATE
+    h.close()
+    whole = pb.Hydro(m, d.params())
+    with pytest.raises(pb.PntError) as e:
+        pb.check(pb.lib.pnt_hydro_piece_forces(whole.h))
+    assert e.value.status == pb.PNT_ERR_STATE
+    whole.close()
