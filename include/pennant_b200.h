@@ -311,8 +311,8 @@ typedef struct pnt_batch pnt_batch;
 pnt_status pnt_batch_create(const pnt_mesh* const* meshes, const pnt_params* params, int32_t n,
                             int32_t device, pnt_batch** out);
 void pnt_batch_destroy(pnt_batch* batch);
-/* Work-list shape: zones per tile (multiple of 64) and CTAs per SM of the
- * persistent zone passes.  Results do not depend on it. */
+/* Work-list shape: zones per tile of the zone passes (multiple of 64) and
+ * CTAs per SM of the persistent point pass.  Results do not depend on it. */
 pnt_status pnt_batch_set_shape(pnt_batch* batch, int32_t zones_per_tile, int32_t ctas_per_sm);
 pnt_status pnt_batch_get_shape(pnt_batch* batch, int32_t* zones_per_tile, int32_t* ctas_per_sm);
 /* Autotuner: times each candidate shape on `trial_cycles` cycles of this

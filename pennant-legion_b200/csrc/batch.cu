@@ -10,10 +10,11 @@
 // (pass A: pass_a_zone_thread of hydro_fp64_body.cuh, one thread per zone;
 // pass C: the staged corrector of pass_c_staged.cuh), so every instance is
 // bit-identical to its own single-mesh run; tiles only change which CTA
-// does the work.  The batch
-// cycle is captured in a CUDA graph.  Tile size and CTAs per SM are picked
-// by pnt_batch_tune, which times candidate shapes on the run's own cycles
-// (the results do not depend on the shape).
+// does the work.  Pass A runs one CTA per zone tile; passes B and C are
+// persistent.  The batch cycle is captured in a CUDA graph.  The tile size
+// (passes A and C) and the point pass's CTAs per SM are picked by
+// pnt_batch_tune, which times candidate shapes on the run's own cycles (the
+// results do not depend on the shape).
 //
 // Compiled with -fmad=false (FP64 parity).
 #include "hydro_fp64_body.cuh"
@@ -58,13 +59,16 @@ constexpr int kZonesPerIter = 64;           // zone tiles are whole multiples of
 
 __device__ __forceinline__ bool inst_skip(const Ctl& ctl) { return ctl.done || ctl.cycle >= ctl.stop_at; }
 
-// Pass A: one thread per zone (pass_a_zone_thread), 128 zones per step
-// through the tile; one partial per tile.
+// Pass A: one CTA per tile (no persistent loop: its state would cost the
+// zone body registers), one thread per zone (pass_a_zone_thread), 128 zones
+// per step through the tile; one partial per tile.
 __global__ void __launch_bounds__(kBatchZT, 3) batch_pass_a(BatchDev b) {
-    for (int t = blockIdx.x; t < b.nztiles; t += gridDim.x) {
+    {
+        const int t = blockIdx.x;
+        if (t >= b.nztiles) return;   // no tiles left: the grid is one idle CTA
         const Tile tile = b.ztiles[t];
         const Ctl& ctl = b.ctls[tile.inst];
-        if (inst_skip(ctl)) continue;   // uniform over the CTA
+        if (inst_skip(ctl)) return;   // uniform over the CTA
         const HydroConst& c = b.consts[tile.inst];
         const int cur = ctl.cycle & 1;
         const double dt = ctl.dt;
@@ -87,7 +91,6 @@ __global__ void __launch_bounds__(kBatchZT, 3) batch_pass_a(BatchDev b) {
         nbad = tiles::block_isum<kBatchZT>(nbad);
         block_fold<true, kBatchZT>(fold, b.a.part_dtnew + t);
         if (threadIdx.x == 0) b.a.part_badA[t] = nbad;
-        __syncthreads();   // the reductions' shared slots are reused by the next tile
     }
 }
 
@@ -308,11 +311,10 @@ struct pnt_batch {
     }
 
     cudaError_t launch_cycle(cudaEvent_t* ev = nullptr) {
-        const int grid_z = std::max(1, std::min(b.nztiles, nsm * shape.ctas_per_sm));
-        const int grid_p = std::max(1, std::min(b.nptiles, nsm * 4));
+        const int grid_p = std::max(1, std::min(b.nptiles, nsm * shape.ctas_per_sm));
         const int grid_f = (ninst * 32 + kBatchThreads - 1) / kBatchThreads;
         if (ev) cudaEventRecord(ev[0], stream);
-        batch_pass_a<<<grid_z, kBatchZT, 0, stream>>>(b);
+        batch_pass_a<<<std::max(1, b.nztiles), kBatchZT, 0, stream>>>(b);
         if (ev) cudaEventRecord(ev[1], stream);
         batch_point_pass<<<grid_p, kBatchThreads, 0, stream>>>(b);
         if (ev) cudaEventRecord(ev[2], stream);
