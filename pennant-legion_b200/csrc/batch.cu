@@ -62,6 +62,9 @@ __device__ __forceinline__ bool inst_skip(const Ctl& ctl) { return ctl.done || c
 // Pass A: one CTA per tile (no persistent loop: its state would cost the
 // zone body registers), one thread per zone (pass_a_zone_thread), 128 zones
 // per step through the tile; one partial per tile.
+// kAllQuads: every instance's zones are quads at sides 4z..4z+3, so only
+// the 4-sided body is compiled (fewer registers than the general form).
+template <bool kAllQuads>
 __global__ void __launch_bounds__(kBatchZT, 3) batch_pass_a(BatchDev b) {
     {
         const int t = blockIdx.x;
@@ -78,7 +81,7 @@ __global__ void __launch_bounds__(kBatchZT, 3) batch_pass_a(BatchDev b) {
             const int64_t z = (int64_t)zb + threadIdx.x;
             if (z >= tile.end) continue;
             double v = 1.e99;
-            if (tile.quads) {
+            if (kAllQuads || tile.quads) {
                 pass_a_zone_thread<4>(b.a, c, cur, dt, z, 4 * z, v, nbad);
             } else {
                 const int n = b.a.znump[z];
@@ -216,6 +219,7 @@ struct pnt_batch {
     std::vector<int64_t> zoff, poff, soff;      // instance offsets (host)
     std::vector<int32_t> nz, np, ns;
     std::vector<int32_t> quads;
+    bool all_quads = false;                      // every instance: quads at sides 4z..4z+3
     Ctl* ctl_host = nullptr;                     // pinned [ninst]
     int* running_dev = nullptr;
     int* running_host = nullptr;                 // pinned
@@ -314,7 +318,8 @@ struct pnt_batch {
         const int grid_p = std::max(1, std::min(b.nptiles, nsm * shape.ctas_per_sm));
         const int grid_f = (ninst * 32 + kBatchThreads - 1) / kBatchThreads;
         if (ev) cudaEventRecord(ev[0], stream);
-        batch_pass_a<<<std::max(1, b.nztiles), kBatchZT, 0, stream>>>(b);
+        if (all_quads) batch_pass_a<true><<<std::max(1, b.nztiles), kBatchZT, 0, stream>>>(b);
+        else batch_pass_a<false><<<std::max(1, b.nztiles), kBatchZT, 0, stream>>>(b);
         if (ev) cudaEventRecord(ev[1], stream);
         batch_point_pass<<<grid_p, kBatchThreads, 0, stream>>>(b);
         if (ev) cudaEventRecord(ev[2], stream);
@@ -497,6 +502,7 @@ pnt_status pnt_batch_create(const pnt_mesh* const* meshes, const pnt_params* par
             NP += m.nump;
             NS += m.nums;
         }
+        bt->all_quads = std::all_of(bt->quads.begin(), bt->quads.end(), [](int32_t q) { return q != 0; });
         if (NZ > INT32_MAX || NP > INT32_MAX || NS > INT32_MAX) {
             delete bt;
             return fail(PNT_ERR_UNSUPPORTED, "batch exceeds int32 indexing");
