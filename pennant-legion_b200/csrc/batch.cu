@@ -100,6 +100,9 @@ __global__ void __launch_bounds__(kBatchZT, 3) batch_pass_a(BatchDev b) {
 // Pass C: the staged corrector of pass_c_staged.cuh, one stage, its
 // kTile zones per step through the tile (copies issued, waited for,
 // computed); one partial per tile.
+// kAllQuads as in batch_pass_a; quad tiles load the next step's point
+// indices while the current step's copies are in flight.
+template <bool kAllQuads>
 __global__ void __launch_bounds__(stagedc::kTile) batch_pass_c(BatchDev b) {
     extern __shared__ __align__(16) unsigned char smem_c[];
     const int th = threadIdx.x;
@@ -112,19 +115,22 @@ __global__ void __launch_bounds__(stagedc::kTile) batch_pass_c(BatchDev b) {
         const double dt = ctl.dt, dtinv = ctl.dtinv;
         double dvm = 1.e-99;
         int nbad = 0;
+        const bool quads = kAllQuads || tile.quads;
+        tiles::ZoneIdx nix{};
+        if (quads && (int64_t)tile.beg + th < tile.end) nix = tiles::load_idx<true>(b.a, (int64_t)tile.beg + th);
         for (int zb = tile.beg; zb < tile.end; zb += stagedc::kTile) {
             const int64_t z = (int64_t)zb + th;
             const bool zok = z < tile.end;
             if (zok) {
-                const tiles::ZoneIdx ix =
-                    tile.quads ? tiles::load_idx<true>(b.a, z) : tiles::load_idx<false>(b.a, z);
+                const tiles::ZoneIdx ix = quads ? nix : tiles::load_idx<false>(b.a, z);
                 stagedc::issue(b.a, cur, smem_c, th, z, ix);
             }
             tiles::commit();
+            if (quads && z + stagedc::kTile < tile.end) nix = tiles::load_idx<true>(b.a, z + stagedc::kTile);
             tiles::wait_groups<0>();
             if (zok) {
-                const double d = tile.quads ? stagedc::zone<true, false>(b.a, c, smem_c, th, z, dt, dtinv, nbad)
-                                            : stagedc::zone<false, false>(b.a, c, smem_c, th, z, dt, dtinv, nbad);
+                const double d = quads ? stagedc::zone<true, false>(b.a, c, smem_c, th, z, dt, dtinv, nbad)
+                                       : stagedc::zone<false, false>(b.a, c, smem_c, th, z, dt, dtinv, nbad);
                 dvm = (d > dvm) ? d : dvm;
             }
         }
@@ -323,7 +329,9 @@ struct pnt_batch {
         if (ev) cudaEventRecord(ev[1], stream);
         batch_point_pass<<<grid_p, kBatchThreads, 0, stream>>>(b);
         if (ev) cudaEventRecord(ev[2], stream);
-        batch_pass_c<<<std::max(1, std::min(b.nztiles, grid_c)), stagedc::kTile, stagedc::kSmemBytes, stream>>>(b);
+        const int gc = std::max(1, std::min(b.nztiles, grid_c));
+        if (all_quads) batch_pass_c<true><<<gc, stagedc::kTile, stagedc::kSmemBytes, stream>>>(b);
+        else batch_pass_c<false><<<gc, stagedc::kTile, stagedc::kSmemBytes, stream>>>(b);
         if (ev) cudaEventRecord(ev[3], stream);
         batch_finalize<<<grid_f, kBatchThreads, 0, stream>>>(b);
         if (ev) cudaEventRecord(ev[4], stream);
@@ -585,10 +593,14 @@ pnt_status pnt_batch_create(const pnt_mesh* const* meshes, const pnt_params* par
         if (e == cudaSuccess) e = cudaMemset(d_mask + NP, 0, 4);   // pass C copies 32-bit mask words
         if (e == cudaSuccess) {
             // the staged pass C: its shared-memory limit and resident CTAs per SM
-            e = cudaFuncSetAttribute(batch_pass_c, cudaFuncAttributeMaxDynamicSharedMemorySize, stagedc::kSmemBytes);
+            e = cudaFuncSetAttribute(batch_pass_c<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, stagedc::kSmemBytes);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(batch_pass_c<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         stagedc::kSmemBytes);
             int occ = 0;
             if (e == cudaSuccess)
-                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pass_c, stagedc::kTile, stagedc::kSmemBytes);
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pass_c<false>, stagedc::kTile,
+                                                                  stagedc::kSmemBytes);
             if (e == cudaSuccess && occ < 1) e = cudaErrorInvalidConfiguration;
             bt->grid_c = bt->nsm * std::max(occ, 1);
         }
