@@ -435,6 +435,26 @@ pnt_status pnt_hydro_closure_counts(pnt_hydro* hydro, uint64_t* counts, int32_t 
 pnt_status pnt_hydro_write_xy(pnt_hydro* hydro, const char* path);
 pnt_status pnt_hydro_write_gold(pnt_hydro* hydro, const char* basename);
 
+/* numpcs pieces of one mesh stepped together by the library: the
+ * reference's Mesh(inp, numpcs) on one node (Mesh.cc:211-241), without
+ * Legion.  Piece q (pnt_mesh_piece) runs on devices[q % ndevices] (device 0
+ * when ndevices is 0).  Every cycle the halo corners move by peer copies on
+ * the receiving piece's stream after the sending piece's pack, and the four
+ * per-piece scalars are reduced on the host; results are bit-identical to
+ * the single-piece run.  pnt_pieces_download gathers a point or zone field
+ * of the whole mesh in reference order; pnt_pieces_write_xy writes the
+ * reference's .xy file (WriteXY.cc:28-52). */
+typedef struct pnt_pieces pnt_pieces;
+pnt_status pnt_pieces_create(const pnt_mesh* mesh, const pnt_params* params, int32_t npieces,
+                             const int32_t* devices, int32_t ndevices, pnt_pieces** out);
+pnt_status pnt_pieces_set_closure(pnt_pieces* pieces, const pnt_closure* closure, int32_t mode);
+pnt_status pnt_pieces_cycle(pnt_pieces* pieces, pnt_scalars* out);
+pnt_status pnt_pieces_run(pnt_pieces* pieces, int32_t max_cycles, pnt_report_fn report, void* user,
+                          pnt_scalars* out);
+pnt_status pnt_pieces_download(pnt_pieces* pieces, int32_t field, void* dst, size_t bytes);
+pnt_status pnt_pieces_write_xy(pnt_pieces* pieces, const char* path);
+void pnt_pieces_destroy(pnt_pieces* pieces);
+
 #ifdef __cplusplus
 }
 #endif

@@ -864,6 +864,15 @@ pnt_status pnt_hydro_copy_state(pnt_hydro* dst, const pnt_hydro* src) {
 }  // extern "C"
 
 namespace pnt {
+
+pnt_status write_xy_file(const char* path, const std::vector<double>& zr, const std::vector<double>& ze,
+                         const std::vector<double>& zp) {
+    return write_xy(path, zr, ze, zp);
+}
+
+}  // namespace pnt
+
+namespace pnt {
 bool hydro_access(pnt_hydro* h, HydroAccess* out) {
     if (!h || !out) return false;
     out->a = h->a;

@@ -48,9 +48,35 @@ int main(int argc, char** argv) {
     try {
         printf("********************\nRunning PENNANT (B200)\n********************\n\n");
         pnt::InputFile inp(filename);
-        pnt::Mesh mesh(&inp, numpcs);
+        pnt::Mesh mesh(&inp);
         printf("--- Mesh Information ---\nPoints:  %d\nZones:   %d\nSides:   %d\n------------------------\n",
                mesh.nump, mesh.numz, mesh.nums);
+        if (numpcs > 1) {
+            // Mesh(inp, numpcs): the pieces stepped together on this GPU
+            pnt_params prm;
+            pnt::check(pnt_params_from_deck(inp.handle(), &prm));
+            pnt_pieces* ps = nullptr;
+            pnt::check(pnt_pieces_create(mesh.handle(), &prm, numpcs, &device, 1, &ps));
+            pnt_scalars s{};
+            const auto t0 = std::chrono::steady_clock::now();
+            const pnt_status st = pnt_pieces_run(ps, 0, report, nullptr, &s);
+            const auto t1 = std::chrono::steady_clock::now();
+            if (st == PNT_ERR_BADSIDES) {
+                fprintf(stderr, "Error: %d negative side volumes on cycle %d\nExiting...\n", s.nbad, s.cycle);
+                pnt_pieces_destroy(ps);
+                return 1;
+            }
+            pnt::check(st);
+            const double wall = std::chrono::duration<double, std::micro>(t1 - t0).count();
+            printf("\nRun complete (%d pieces)\ncycle = %6d,        cstop = %8d\ntime = %14.6g, tstop = %8.6g\n\n",
+                   numpcs, s.cycle, prm.cstop, s.time, prm.tstop);
+            printf("************************************\nhydro cycle run time= %14.8g us\n"
+                   "************************************\n",
+                   wall);
+            pnt::check(pnt_pieces_write_xy(ps, (probname + ".xy").c_str()));
+            pnt_pieces_destroy(ps);
+            return 0;
+        }
         pnt::Hydro hydro(&inp, &mesh, device);
         pnt_scalars s{};
         const auto t0 = std::chrono::steady_clock::now();

@@ -57,10 +57,10 @@ private:
 
 class Mesh {
 public:
-    // numpcs: pieces of the reference's domain decomposition; this build
-    // runs one piece per GPU (numpcs must be 1).
+    // The whole mesh (one piece); its pieces are pnt_mesh_piece meshes, and
+    // pnt_pieces steps numpcs of them together (the `pennant -n` path).
     Mesh(const InputFile* inp, int numpcs = 1) {
-        if (numpcs != 1) throw Error(PNT_ERR_UNSUPPORTED, "multi-piece meshes are not built (numpcs must be 1)");
+        if (numpcs != 1) throw Error(PNT_ERR_UNSUPPORTED, "build the pieces with pnt_mesh_piece / pnt_pieces_create");
         check(pnt_mesh_generate(inp->handle(), &mesh_));
         pnt_mesh_desc d;
         check(pnt_mesh_describe(mesh_, &d));

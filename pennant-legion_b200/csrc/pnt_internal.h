@@ -64,6 +64,10 @@ pnt_status finish_mesh(Mesh& m);
 // the contiguous zone range [numz*piece/npieces, numz*(piece+1)/npieces).
 pnt_status make_piece(const Mesh& g, int npieces, int piece, Mesh& out);
 
+// The reference's .xy writer (WriteXY.cc:28-52) for zone fields in global
+// order (hydro.cu).
+pnt_status write_xy_file(const char* path, const std::vector<double>& zr, const std::vector<double>& ze,
+                         const std::vector<double>& zp);
 // The closure's device parameter image and device (closure.cu).
 const uint8_t* closure_image(const pnt_closure* c);
 int closure_device(const pnt_closure* c);

@@ -184,6 +184,13 @@ def _load():
         "pnt_hydro_set_closure": (i32, [vp, vp, i32]),
         "pnt_hydro_closure_counts": (i32, [vp, C.POINTER(C.c_uint64), i32]),
         "pnt_hydro_write_xy": (i32, [vp, C.c_char_p]),
+        "pnt_pieces_create": (i32, [vp, C.POINTER(Params), i32, C.POINTER(i32), i32, pp]),
+        "pnt_pieces_set_closure": (i32, [vp, vp, i32]),
+        "pnt_pieces_cycle": (i32, [vp, C.POINTER(Scalars)]),
+        "pnt_pieces_run": (i32, [vp, i32, REPORT_FN, vp, C.POINTER(Scalars)]),
+        "pnt_pieces_download": (i32, [vp, i32, vp, sz]),
+        "pnt_pieces_write_xy": (i32, [vp, C.c_char_p]),
+        "pnt_pieces_destroy": (None, [vp]),
         "pnt_hydro_write_gold": (i32, [vp, C.c_char_p]),
     }
     for name, (res, args) in sig.items():
@@ -489,6 +496,49 @@ class Batch:
         out = np.empty(shape, dtype=np.float64)
         check(lib.pnt_batch_download(self.h, i, FIELDS[name], out.ctypes.data, out.nbytes))
         return out
+
+
+class Pieces:
+    """numpcs pieces of one mesh stepped together by the library (peer
+    copies between the pieces' devices, host reductions): bit-identical to
+    one Hydro over the whole mesh."""
+
+    def __init__(self, mesh: Mesh, params: Params, npieces: int, devices=(0,)):
+        h = C.c_void_p()
+        devs = (C.c_int32 * len(devices))(*devices)
+        check(lib.pnt_pieces_create(mesh.h, C.byref(params), npieces, devs, len(devices), C.byref(h)))
+        self.h = h
+        self.mesh = mesh
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.pnt_pieces_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_closure(self, closure: "Closure", mode: int = 0) -> None:
+        check(lib.pnt_pieces_set_closure(self.h, closure.h, mode))
+
+    def cycle(self) -> dict:
+        s = Scalars()
+        check(lib.pnt_pieces_cycle(self.h, C.byref(s)))
+        return s.as_dict()
+
+    def run(self, max_cycles: int = 0) -> dict:
+        s = Scalars()
+        check(lib.pnt_pieces_run(self.h, max_cycles, REPORT_FN(), None, C.byref(s)))
+        return s.as_dict()
+
+    def download(self, name: str) -> np.ndarray:
+        shape = (self.mesh.nump, 2) if name in _POINT2 else (self.mesh.numz,)
+        out = np.empty(shape, dtype=np.float64)
+        check(lib.pnt_pieces_download(self.h, FIELDS[name], out.ctypes.data, out.nbytes))
+        return out
+
+    def write_xy(self, path: str) -> None:
+        check(lib.pnt_pieces_write_xy(self.h, _b(path)))
 
 
 class Closure:

@@ -109,3 +109,24 @@ def test_a_piece_refuses_whole_cycles_and_a_mesh_the_piece_calls():
         pb.check(pb.lib.pnt_hydro_piece_forces(whole.h))
     assert e.value.status == pb.PNT_ERR_STATE
     whole.close()
+
+
+@pytest.mark.parametrize("case,npieces", [("sedov-fp64", 2), ("sedov-fp64-3", 3), ("noh-pie-fp64", 4),
+                                          ("sedov-mixed", 3), ("sedov-learned", 2)])
+def test_native_pieces_match_the_single_piece_run_bitwise(case, npieces, tmp_path):
+    """pnt_pieces (one process; peer copies, host reductions), gathered back
+    to the whole mesh: equal to the single-piece run bit for bit."""
+    text, precision, _ = CASES[case]
+    s1, f1 = single(text, precision)
+    d = _deck(text, precision)
+    m = pb.Mesh(deck=d)
+    ps = pb.Pieces(m, d.params(), npieces, devices=(0,))
+    if precision == "learned":
+        ps.set_closure(pb.Closure(path=CLOSURE))
+    s = ps.run()
+    assert s["cycle"] == s1["cycle"] and s["time"] == s1["time"] and s["done"] == 1, (case, s, s1)
+    for k in ZONE + POINT:
+        assert ps.download(k).tobytes() == f1[k].tobytes(), (case, k)
+    ps.write_xy(str(tmp_path / "p.xy"))
+    assert (tmp_path / "p.xy").stat().st_size > 0
+    ps.close()
