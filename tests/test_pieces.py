@@ -156,3 +156,19 @@ def test_halo_exchange_over_gloo(world, mixed):
     mp.start_processes(_exchange_rank, args=(world, _free_port(), mixed, out), nprocs=world, join=True,
                        start_method="spawn")
     assert sorted(out.keys()) == list(range(world))
+
+
+def test_pieces_driver_arguments_and_no_device():
+    """pnt_pieces_create: fewer than two pieces is an argument error; without
+    a GPU it fails cleanly (no device), after building the pieces on the
+    host."""
+    import torch
+    m = pb.Mesh(deck=pb.Deck(text=sedov(6)))
+    d = pb.Deck(text=sedov(6))
+    with pytest.raises(pb.PntError) as e:
+        pb.Pieces(m, d.params(), 1)
+    assert e.value.status == pb.PNT_ERR_INVALID_ARG
+    if not torch.cuda.is_available():
+        with pytest.raises(pb.PntError) as e:
+            pb.Pieces(m, d.params(), 2)
+        assert e.value.status == pb.PNT_ERR_NO_DEVICE
