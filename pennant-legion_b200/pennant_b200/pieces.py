@@ -54,7 +54,9 @@ class HaloExchange:
     through host copies."""
 
     def __init__(self, info: dict, cmass_bytes: int, cforce_bytes: int, foff: int, group=None):
-        self.nbr = [int(q) for q in info["nbr"]]
+        # pieces are numbered by rank within the group; point-to-point
+        # operations address global ranks
+        self.nbr = [int(q) if group is None else dist.get_global_rank(group, int(q)) for q in info["nbr"]]
         self.send_off = [int(v) for v in info["send_off"]]
         self.recv_off = [int(v) for v in info["recv_off"]]
         self.cmb, self.cfb, self.foff = cmass_bytes, cforce_bytes, foff
