@@ -435,6 +435,13 @@ pnt_status pnt_hydro_closure_counts(pnt_hydro* hydro, uint64_t* counts, int32_t 
 pnt_status pnt_hydro_write_xy(pnt_hydro* hydro, const char* path);
 pnt_status pnt_hydro_write_gold(pnt_hydro* hydro, const char* basename);
 
+/* The analogue of the reference's NAN_CHECK accessors (MyLegion.hh:29-206):
+ * scans the current point positions and velocities and the zone fields
+ * (PNT_FIELD_PX .. PNT_FIELD_ZWRATE) on the device for NaN or Inf.  *field
+ * = the first such field in that order and *index = the smallest point or
+ * zone index holding one, or -1 and -1 when every value is finite. */
+pnt_status pnt_hydro_check_finite(pnt_hydro* hydro, int32_t* field, int64_t* index);
+
 /* numpcs pieces of one mesh stepped together by the library: the
  * reference's Mesh(inp, numpcs) on one node (Mesh.cc:211-241), without
  * Legion.  Piece q (pnt_mesh_piece) runs on devices[q % ndevices] (device 0

@@ -70,6 +70,7 @@ struct pnt_hydro {
     // multi-piece runs (a hydro object over a piece mesh): the send lists,
     // the send buffer (corner masses, then corner forces at send_foff) and
     // the per-corner byte sizes of the cycle's precision
+    unsigned long long* scan = nullptr;   // pnt_hydro_check_finite's results
     bool piece = false;
     int32_t nsend = 0, nhalo = 0;
     int32_t* send_side = nullptr;
@@ -673,6 +674,37 @@ pnt_status pnt_hydro_piece_finish(pnt_hydro* h) {
     DeviceGuard dg(h->device);
     launch_piece_finish(h->a, h->hc, h->stream);
     CUDA_TRY(cudaGetLastError());
+    return PNT_OK;
+}
+
+pnt_status pnt_hydro_check_finite(pnt_hydro* h, int32_t* field, int64_t* index) {
+    if (!h || !field || !index) return fail(PNT_ERR_INVALID_ARG, "null argument");
+    DeviceGuard dg(h->device);
+    pnt_status st = h->fetch_ctl();
+    if (st) return st;
+    static const int32_t kFields[] = {PNT_FIELD_PX, PNT_FIELD_PU, PNT_FIELD_ZR, PNT_FIELD_ZE, PNT_FIELD_ZP,
+                                      PNT_FIELD_ZM, PNT_FIELD_ZETOT, PNT_FIELD_ZVOL, PNT_FIELD_ZWRATE};
+    constexpr int kN = (int)(sizeof(kFields) / sizeof(kFields[0]));
+    if (!h->scan && (st = h->alloc(&h->scan, kN))) return st;
+    CUDA_TRY(cudaMemsetAsync(h->scan, 0xff, kN * sizeof(unsigned long long), h->stream));
+    for (int i = 0; i < kN; ++i) {
+        const FieldInfo fi = field_info(h, kFields[i], h->ctl_host->cycle & 1);
+        launch_find_nonfinite(static_cast<const double*>(fi.dev), (int64_t)(fi.bytes / 8), h->scan + i, h->stream);
+    }
+    CUDA_TRY(cudaGetLastError());
+    unsigned long long first[kN];
+    CUDA_TRY(cudaMemcpyAsync(first, h->scan, sizeof(first), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    *field = -1;
+    *index = -1;
+    for (int i = 0; i < kN; ++i) {
+        if (first[i] != ~0ull) {
+            *field = kFields[i];
+            const bool point = kFields[i] == PNT_FIELD_PX || kFields[i] == PNT_FIELD_PU;
+            *index = (int64_t)(point ? first[i] / 2 : first[i]);
+            break;
+        }
+    }
     return PNT_OK;
 }
 

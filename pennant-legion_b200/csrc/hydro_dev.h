@@ -138,6 +138,9 @@ cudaError_t launch_cycle_learned(const DevArrays& a, const HydroConst& c, cudaSt
 void launch_piece_pack(const DevArrays& a, const int32_t* send_side, int32_t nsend, unsigned char* send,
                        size_t foff, bool mixed, cudaStream_t stream);
 void launch_piece_finish(const DevArrays& a, const HydroConst& c, cudaStream_t stream);
+// The index of the first non-finite value of a[0 .. n) into *first (an
+// atomic minimum; *first must start at ULLONG_MAX).
+void launch_find_nonfinite(const double* a, int64_t n, unsigned long long* first, cudaStream_t stream);
 // Raises the learned pass A's dynamic shared-memory limit on the current device.
 cudaError_t prepare_learned_kernels();
 // Pass C of the FP64 (mixed = false) or mixed/learned cycle (pass_c.cu):

@@ -33,6 +33,8 @@
 // batched kernels); this file is compiled with -fmad=false, so the results
 // match a serial CPU run of the reference bit for bit.
 #include "hydro_fp64_body.cuh"
+
+#include <algorithm>
 #include "zone_tiles.cuh"
 
 namespace pnt {
@@ -93,6 +95,19 @@ __global__ void piece_pack(DevArrays a, const int32_t* __restrict__ send_side, i
     }
 }
 
+// The first non-finite element of a[0 .. n): its index into *first by
+// atomic minimum (a thread's indices grow along its grid-stride loop, so it
+// stops at its first).
+__global__ void find_nonfinite(const double* __restrict__ a, int64_t n, unsigned long long* first) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        if (!isfinite(__ldg(a + i))) {
+            atomicMin(first, (unsigned long long)i);
+            return;
+        }
+    }
+}
+
 __global__ void piece_finish(DevArrays a, HydroConst c) {
     Ctl* ctl = a.ctl;
     if (skip_cycle(ctl)) return;
@@ -125,6 +140,12 @@ cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStrea
 void launch_piece_pack(const DevArrays& a, const int32_t* send_side, int32_t nsend, unsigned char* send,
                        size_t foff, bool mixed, cudaStream_t stream) {
     if (nsend > 0) piece_pack<<<(nsend + 255) / 256, 256, 0, stream>>>(a, send_side, nsend, send, foff, mixed);
+}
+
+void launch_find_nonfinite(const double* a, int64_t n, unsigned long long* first, cudaStream_t stream) {
+    if (n <= 0) return;
+    const int64_t blocks = std::min<int64_t>((n + 255) / 256, 148 * 8);
+    find_nonfinite<<<(int)blocks, 256, 0, stream>>>(a, n, first);
 }
 
 void launch_piece_finish(const DevArrays& a, const HydroConst& c, cudaStream_t stream) {

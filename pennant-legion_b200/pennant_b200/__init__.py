@@ -153,6 +153,7 @@ def _load():
         "pnt_hydro_upload": (i32, [vp, i32, vp, sz]),
         "pnt_hydro_device_ptr": (i32, [vp, i32, pp]),
         "pnt_hydro_stream": (i32, [vp, pp]),
+        "pnt_hydro_check_finite": (i32, [vp, C.POINTER(i32), C.POINTER(C.c_int64)]),
         "pnt_hydro_piece_buffers": (i32, [vp, C.POINTER(PieceBuffers)]),
         "pnt_hydro_piece_forces": (i32, [vp]),
         "pnt_hydro_piece_advance": (i32, [vp]),
@@ -417,6 +418,15 @@ class Hydro:
         p = C.c_void_p()
         check(lib.pnt_hydro_stream(self.h, C.byref(p)))
         return p.value or 0
+
+    def check_finite(self):
+        """(field name, index) of the first NaN/Inf in the state, or (None, -1)."""
+        f, i = C.c_int32(), C.c_int64()
+        check(lib.pnt_hydro_check_finite(self.h, C.byref(f), C.byref(i)))
+        if f.value < 0:
+            return None, -1
+        name = next(k for k, v in FIELDS.items() if v == f.value)
+        return name, i.value
 
     def set_closure(self, closure: "Closure", mode: int = 0) -> None:
         """Learned cycle: 0 the network, 1 no force on its corners, 2 plain QCS there."""

@@ -198,3 +198,22 @@ def test_copy_state_restarts_bitwise():
     other = pb.Hydro(pb.Mesh(deck=pb.Deck(path=golden("sedovsmall.pnt"))), d.params())
     with pytest.raises(pb.PntError):
         other.copy_state_from(src)
+
+
+def test_check_finite_finds_the_first_non_finite_value():
+    """pnt_hydro_check_finite (the NAN_CHECK analogue): none after a clean
+    run, then the first field in field order and its smallest bad index."""
+    d = pb.Deck(path=golden("sedov.pnt"))
+    h = pb.Hydro(pb.Mesh(deck=d), d.params())
+    h.run()
+    assert h.check_finite() == (None, -1)
+    ze = h.download("ze")
+    ze[90] = np.inf
+    ze[37] = np.nan
+    h.upload("ze", ze)
+    assert h.check_finite() == ("ze", 37)
+    px = h.download("px")
+    px[5, 1] = -np.inf
+    h.upload("px", px)
+    assert h.check_finite() == ("px", 5)
+    h.close()
