@@ -448,9 +448,11 @@ pnt_status pnt_hydro_check_finite(pnt_hydro* hydro, int32_t* field, int64_t* ind
  * when ndevices is 0).  Every cycle the halo corners move by peer copies on
  * the receiving piece's stream after the sending piece's pack, and the four
  * per-piece scalars are reduced on the host; results are bit-identical to
- * the single-piece run.  pnt_pieces_download gathers a point or zone field
- * of the whole mesh in reference order; pnt_pieces_write_xy writes the
- * reference's .xy file (WriteXY.cc:28-52). */
+ * the single-piece run.  A cycle that fails part way (a CUDA error) leaves
+ * the pieces out of step: later cycles return PNT_ERR_STATE.
+ * pnt_pieces_download gathers a point or zone field of the whole mesh in
+ * reference order; pnt_pieces_write_xy writes the reference's .xy file
+ * (WriteXY.cc:28-52). */
 typedef struct pnt_pieces pnt_pieces;
 pnt_status pnt_pieces_create(const pnt_mesh* mesh, const pnt_params* params, int32_t npieces,
                              const int32_t* devices, int32_t ndevices, pnt_pieces** out);

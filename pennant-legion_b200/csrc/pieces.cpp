@@ -65,6 +65,8 @@ struct pnt_pieces {
     pnt_params params{};
     int32_t numz = 0, nump = 0;
     double* red_host = nullptr;   // pinned [npieces][4]
+    // a cycle that failed part way leaves some pieces a phase ahead of others
+    bool broken = false;
 
     ~pnt_pieces() {
         for (Piece& q : p) {
@@ -210,7 +212,11 @@ pnt_status pnt_pieces_create(const pnt_mesh* mesh, const pnt_params* params, int
 
 pnt_status pnt_pieces_cycle(pnt_pieces* ps, pnt_scalars* out) {
     if (!ps) return pnt::fail(PNT_ERR_INVALID_ARG, "null argument");
-    if (pnt_status st = ps->cycle()) return st;
+    if (ps->broken) return pnt::fail(PNT_ERR_STATE, "an earlier cycle of these pieces failed part way");
+    if (pnt_status st = ps->cycle()) {
+        ps->broken = true;
+        return st;
+    }
     pnt_scalars s{};
     if (pnt_status st = pnt_hydro_get_scalars(ps->p[0].hydro, &s)) return st;
     if (out) *out = s;
