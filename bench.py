@@ -80,18 +80,75 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks, power and throttle reasons sampled during the timed region:
+    NVML polled every 10 ms from a thread (a 100 ms window still gets ~10
+    samples), else `nvidia-smi -lms 200`.  Reads only; changes nothing."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, gpu_index: str):
+    def __init__(self, gpu_index: str, period_s: float = 0.01):
         self.gpu = gpu_index
+        self.period = period_s
         self.proc = None
         self.path = None
+        self.thread = None
+        self.rows = []          # (sm MHz, max sm MHz, power W, set of reasons)
+        self.stop = None
+
+    def _nvml_open(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+        except Exception:
+            return None
+        try:
+            h = (nv.nvmlDeviceGetHandleByUUID(self.gpu) if self.gpu.startswith(("GPU-", "MIG-"))
+                 else nv.nvmlDeviceGetHandleByIndex(int(self.gpu)))
+            reasons_fn = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons",
+                                 getattr(nv, "nvmlDeviceGetCurrentClocksThrottleReasons", None))
+            bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+            smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            # one trial read of every query the thread makes: any failure
+            # falls back to nvidia-smi rather than an empty record
+            nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            nv.nvmlDeviceGetPowerUsage(h)
+            if reasons_fn is None:
+                raise RuntimeError("NVML without a clock-event reasons query")
+            reasons_fn(h)
+            return nv, h, reasons_fn, bits, smax
+        except Exception:
+            try:
+                nv.nvmlShutdown()
+            except Exception:
+                pass
+            return None
+
+    def _poll(self, nv, h, reasons_fn, bits, smax):
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1e3
+                r = reasons_fn(h)
+                self.rows.append((float(sm), float(smax), pw,
+                                  {n for n, b in zip(self.REASONS, bits) if r & b}))
+            except Exception:
+                pass
+            self.stop.wait(self.period)
 
     def __enter__(self):
+        opened = self._nvml_open()
+        if opened:
+            import threading
+            self.stop = threading.Event()
+            self.nv = opened[0]
+            self.thread = threading.Thread(target=self._poll, args=opened, daemon=True)
+            self.thread.start()
+            time.sleep(0.05)
+            return self
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
@@ -104,6 +161,13 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
+        if self.thread:
+            self.stop.set()
+            self.thread.join(timeout=5)
+            try:
+                self.nv.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -111,17 +175,10 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self):
-        if not self.path or not os.path.exists(self.path):
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+    def _smi_rows(self):
         rows = []
-        for line in open(self.path):
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
-        os.unlink(self.path)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        if not self.path or not os.path.exists(self.path):
+            return rows
 
         def num(x):
             try:
@@ -129,13 +186,24 @@ class ClockSampler:
             except ValueError:
                 return None
 
-        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
-        smax = [num(r[2]) for r in rows if num(r[2]) is not None]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
-        pw = [num(r[3]) for r in rows if num(r[3]) is not None]
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None}
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9 and num(parts[1]) is not None:
+                rows.append((num(parts[1]), num(parts[2]), num(parts[3]),
+                             {n for i, n in enumerate(self.REASONS) if parts[5 + i].lower().startswith("active")}))
+        os.unlink(self.path)
+        return rows
+
+    def summary(self):
+        rows = self.rows if self.thread else self._smi_rows()
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        smax = [r[1] for r in rows if r[1] is not None]
+        pw = [r[2] for r in rows if r[2] is not None]
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(set().union(*(r[3] for r in rows))), "samples": len(rows),
+                "sampler": "nvml 10 ms" if self.thread else "nvidia-smi 200 ms",
+                "power_w_max": max(pw) if pw else None}
 
 
 def host_cores():
