@@ -422,6 +422,13 @@ pnt_status pnt_closure_gradient(pnt_closure* closure, const void* x, const float
 /* The network on n raw input rows (device feats [n][14] -> out [n][4]),
  * the tcgen05 inference of the learned cycle. */
 pnt_status pnt_closure_forward(const pnt_closure* closure, const float* feats, int64_t n, float* out);
+/* The bounded device-side wait the tensor-core kernels use for their MMA
+ * completions, run on its own on `device`: one mbarrier polled at most
+ * `limit` (1 .. 2^20) times, completed first by the waiting thread
+ * (arrive = 1) or by nothing (arrive = 0).  PNT_OK when the wait completed,
+ * PNT_ERR_TIMEOUT when it ran out; the device stays usable either way.  It
+ * exercises the timeout path of those kernels without a fault. */
+pnt_status pnt_closure_wait_probe(int32_t device, int32_t arrive, int32_t limit);
 /* Gives a precision-learned hydro object its copy of the closure.  mode 0:
  * the network; 1: no force on the network's corners (ablation); 2: plain
  * QCS on them (isolates the classification). */

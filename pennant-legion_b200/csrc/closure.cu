@@ -679,6 +679,20 @@ __global__ void __launch_bounds__(kMlpRows, 1) closure_forward_kernel(const uint
         for (int i = 0; i < 4; ++i) out[r * 4 + i] = y[i];
 }
 
+// The bounded wait of the tensor-core kernels on its own: one mbarrier of
+// arrival count 1 that this thread completes first (arrive = 1) or that
+// nothing completes (arrive = 0).  The wait ends either way, after at most
+// `limit` polls; *timed_out records which.  No tensor-core work is in
+// flight, so giving up leaves nothing behind.
+__global__ void __launch_bounds__(32, 1) bounded_wait_probe(int arrive, int limit, int* timed_out) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    const uint32_t mbar = smem_addr(&bar);
+    mbar_init(mbar, 1);
+    if (arrive) mbar_arrive(mbar);
+    *timed_out = mbar_wait(mbar, 0, limit) ? 0 : 1;
+}
+
 }  // namespace
 }  // namespace pnt
 
@@ -1018,6 +1032,32 @@ pnt_status pnt_closure_gradient(pnt_closure* c, const void* x, const float* t, i
     pnt_status st = c->step(x, t, n, 0, n, 0.f, false, grad, &l);
     if (st) return st;
     if (loss) *loss = l;
+    return PNT_OK;
+}
+
+pnt_status pnt_closure_wait_probe(int32_t device, int32_t arrive, int32_t limit) {
+    if ((arrive != 0 && arrive != 1) || limit < 1 || limit > (1 << 20))
+        return fail(PNT_ERR_INVALID_ARG, "arrive must be 0 or 1 and limit in 1 .. 2^20");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return fail(PNT_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev) return fail(PNT_ERR_INVALID_ARG, "device %d out of range", device);
+    DeviceGuard dg(device);
+    int* d = nullptr;
+    CUDA_TRY(cudaMalloc(&d, sizeof(int)));
+    cudaError_t e = cudaMemset(d, 0xff, sizeof(int));
+    if (e == cudaSuccess) {
+        bounded_wait_probe<<<1, 32>>>(arrive, limit, d);
+        e = cudaGetLastError();
+    }
+    int h = -1;
+    if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(PNT_ERR_CUDA, "bounded wait probe: %s", cudaGetErrorString(e));
+    if (h != 0 && h != 1) return fail(PNT_ERR_CUDA, "bounded wait probe wrote %d", h);
+    if (h) return fail(PNT_ERR_TIMEOUT, "the bounded wait ran out after %d polls", limit);
     return PNT_OK;
 }
 

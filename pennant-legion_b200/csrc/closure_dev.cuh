@@ -216,9 +216,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait: false if the phase did not complete within the limit.
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-    for (int i = 0; i < (1 << 20); ++i)
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+// Bounded wait: false if the phase did not complete within `limit` polls.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, int limit = 1 << 20) {
+    for (int i = 0; i < limit; ++i)
         if (mbar_try_wait(mbar, parity)) return true;
     return false;
 }

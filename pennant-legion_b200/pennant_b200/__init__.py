@@ -182,6 +182,7 @@ def _load():
         "pnt_closure_train": (i32, [vp, vp, vp, C.c_int64, C.c_int64, i32, i32, C.c_float, vp]),
         "pnt_closure_gradient": (i32, [vp, vp, vp, C.c_int64, vp, C.POINTER(C.c_float)]),
         "pnt_closure_forward": (i32, [vp, vp, C.c_int64, vp]),
+        "pnt_closure_wait_probe": (i32, [i32, i32, i32]),
         "pnt_hydro_set_closure": (i32, [vp, vp, i32]),
         "pnt_hydro_closure_counts": (i32, [vp, C.POINTER(C.c_uint64), i32]),
         "pnt_hydro_write_xy": (i32, [vp, C.c_char_p]),

@@ -69,3 +69,12 @@ def test_hydro_create_without_device_fails_loudly():
     with pytest.raises(pb.PntError) as e:
         pb.Hydro(m, d.params())
     assert e.value.status == pb.PNT_ERR_NO_DEVICE
+
+
+def test_wait_probe_arguments_and_no_device():
+    """pnt_closure_wait_probe: bad arguments are rejected before any device
+    work; without a device it fails with PNT_ERR_NO_DEVICE."""
+    for arrive, limit in ((2, 10), (-1, 10), (0, 0), (1, (1 << 20) + 1)):
+        assert pb.lib.pnt_closure_wait_probe(0, arrive, limit) == pb.PNT_ERR_INVALID_ARG
+    if not _has_device():
+        assert pb.lib.pnt_closure_wait_probe(0, 0, 10) == pb.PNT_ERR_NO_DEVICE

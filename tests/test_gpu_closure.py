@@ -207,3 +207,23 @@ def test_learned_cycle_accuracy_and_ablation():
     assert res["network"][2]["mlp"] > 0
     assert er_net <= 1e-3
     assert res["no force"][0] > 2 * er_net   # the network carries the force it replaces
+
+
+def test_bounded_wait_runs_out_with_a_status_and_the_device_stays_usable():
+    """The tensor-core kernels' bounded mbarrier wait, on its own: a barrier
+    nothing completes gives PNT_ERR_TIMEOUT after the poll limit (no trap, no
+    hang); one the thread completes gives PNT_OK; tensor-core inference
+    still runs correctly afterwards."""
+    for limit in (1, 64, 4096):
+        with pytest.raises(pb.PntError) as e:
+            pb.check(pb.lib.pnt_closure_wait_probe(0, 0, limit))
+        assert e.value.status == pb.PNT_ERR_TIMEOUT
+        pb.check(pb.lib.pnt_closure_wait_probe(0, 1, limit))
+    c, p, norm, rng = random_closure(3)
+    feats = (rng.normal(size=(256, 14)) * norm[14:28] + norm[:14]).astype(np.float32)
+    ft = torch.from_numpy(feats).to(DEV)
+    out = torch.full((256, 4), float("nan"), dtype=torch.float32, device=DEV)
+    c.forward(ft.data_ptr(), 256, out.data_ptr())
+    yn, _ = co.forward(p, co.normalise(feats, norm), bf16_round=True)
+    yo = yn * norm[32:36] + norm[28:32]
+    assert np.abs(out.cpu().numpy() - yo).max() <= 2e-2 * np.abs(yo).max()
