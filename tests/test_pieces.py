@@ -6,7 +6,9 @@ hold is that (1) the pieces cover the zones exactly once, (2) a piece holds
 every point its zones touch, (3) each local point's corner list, local and
 halo slots, is the global corner list in global side order, and (4) the
 exchange fills every halo slot with the owning piece's value, so the
-corner sums at shared points equal the single-piece sums bit for bit."""
+corner sums at shared points equal the single-piece sums bit for bit.
+A rank lost between steps ends its neighbour's next exchange with an error,
+not a wait without end."""
 import os
 import socket
 import sys
@@ -172,3 +174,47 @@ def test_pieces_driver_arguments_and_no_device():
         with pytest.raises(pb.PntError) as e:
             pb.Pieces(m, d.params(), 2)
         assert e.value.status == pb.PNT_ERR_NO_DEVICE
+
+
+def _lost_rank(rank, world, port, mode, out):
+    import time
+    import torch
+    import torch.distributed as dist
+    from pennant_b200.pieces import HaloExchange, reduce_scalars
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=5))
+    m = pb.Mesh(deck=pb.Deck(text=sedov(8)))
+    info = m.piece(world, rank).piece_info()
+    if rank == 1:
+        # this rank leaves between steps (exits, or stays alive and never
+        # takes the next step): no exchange, no reduction
+        if mode == "stall":
+            time.sleep(12)
+        out[rank] = "left"
+        return
+    nsend, nhalo = int(info["send_off"][-1]), int(info["nhalo"])
+    send = torch.zeros(16 + nsend * 24, dtype=torch.uint8)
+    t0 = time.monotonic()
+    for step in (lambda: HaloExchange(info, 8, 16, 16 + nsend * 8).exchange(
+                     send, torch.zeros(nhalo * 8, dtype=torch.uint8), torch.zeros(nhalo * 16, dtype=torch.uint8)),
+                 lambda: reduce_scalars(torch.zeros(4, dtype=torch.float64))):
+        try:
+            step()
+            out[rank] = "no error"
+            return
+        except RuntimeError as e:
+            out[rank] = ("error", time.monotonic() - t0, str(e)[:200])
+            break
+
+
+@pytest.mark.parametrize("mode", ["exit", "stall"])
+def test_a_lost_rank_ends_the_exchange_with_an_error(mode):
+    """A rank that leaves between steps: its neighbour's next exchange ends
+    with an error (the closed connection, or the process group's 5 s
+    timeout) instead of waiting for good."""
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    mp.start_processes(_lost_rank, args=(2, _free_port(), mode, out), nprocs=2, join=True, start_method="spawn")
+    assert out[1] == "left"
+    assert out[0][0] == "error", out[0]
+    assert out[0][1] < 11, out[0]
