@@ -257,7 +257,8 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world,
         "steps": len(times), "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": os.path.basename(args.deck), "zones": numz, "path": "cpu-openmp-port"},
+        "config": {"workload": f"{os.path.basename(args.deck)} ({numz} zones, {o.nums} sides, {o.nump} points)",
+                   "zones": numz, "path": "cpu-openmp-port"},
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{len(times)} cycles of {os.path.basename(args.deck)} after {args.warmup} "
                                    f"warm-up cycles; oracle restating the reference's *OMPTask loops "
