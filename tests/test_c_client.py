@@ -1,0 +1,89 @@
+"""The drop-in boundary from plain C: a C99 program (no C++, no Python)
+includes include/pennant_b200.h, links libpennant_b200.so and drives the
+host-side half of the API -- the deck (InputFile), the mesh (Mesh + GenMesh),
+the parameters, a piece of the mesh -- then asks for a Hydro object, which
+without a GPU must fail with PNT_ERR_NO_DEVICE rather than fall back to
+anything.  Its output is compared with the same calls made through the
+Python binding."""
+import os
+import subprocess
+
+import pytest
+
+from conftest import ROOT, golden
+import pennant_b200 as pb
+
+C_SOURCE = r"""
+#include <stdio.h>
+#include <stdlib.h>
+#include "pennant_b200.h"
+
+#define CHECK(x) do { pnt_status s_ = (x); if (s_ != PNT_OK) { \
+    fprintf(stderr, "%s: %s (%s)\n", #x, pnt_status_string(s_), pnt_last_error()); return 2; } } while (0)
+
+int main(int argc, char** argv) {
+    pnt_deck* deck = NULL;
+    pnt_mesh* mesh = NULL;
+    pnt_mesh* piece = NULL;
+    pnt_mesh_desc md;
+    pnt_piece_desc pd;
+    pnt_params prm;
+    pnt_hydro* hydro = NULL;
+    pnt_status st;
+    if (argc != 2) return 1;
+    if (pnt_abi_version() != PNT_ABI_VERSION) return 3;
+    CHECK(pnt_deck_load(argv[1], &deck));
+    CHECK(pnt_mesh_generate(deck, &mesh));
+    CHECK(pnt_mesh_describe(mesh, &md));
+    CHECK(pnt_params_from_deck(deck, &prm));
+    printf("mesh %d %d %d\n", md.numz, md.nums, md.nump);
+    printf("params %d %.17g %.17g %.17g %.17g %d %d\n", prm.cstop, prm.tstop, prm.dtinit, prm.q1, prm.alfa,
+           prm.nbcx, prm.nbcy);
+    CHECK(pnt_mesh_piece(mesh, 2, 1, &piece));
+    CHECK(pnt_mesh_piece_describe(piece, &pd));
+    printf("piece %d %d %d %d\n", pd.piece, pd.zone0, pd.nhalo, pd.nnbr);
+    st = pnt_hydro_create(mesh, &prm, 0, &hydro);
+    printf("hydro %d\n", (int)st);
+    if (hydro) pnt_hydro_destroy(hydro);
+    pnt_mesh_destroy(piece);
+    pnt_mesh_destroy(mesh);
+    pnt_deck_destroy(deck);
+    return 0;
+}
+"""
+
+
+def _has_device():
+    import ctypes
+    try:
+        rt = ctypes.CDLL("libcudart.so")
+    except OSError:
+        return False
+    n = ctypes.c_int(0)
+    return rt.cudaGetDeviceCount(ctypes.byref(n)) == 0 and n.value > 0
+
+
+@pytest.mark.skipif(_has_device(), reason="checks the no-device answer of the C boundary")
+def test_plain_c_client_against_the_python_binding(tmp_path):
+    src = tmp_path / "client.c"
+    src.write_text(C_SOURCE)
+    exe = tmp_path / "client"
+    pkg = os.path.dirname(pb.LIB_PATH)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I", os.path.join(ROOT, "include"),
+                    str(src), "-o", str(exe), "-L", pkg, "-lpennant_b200", f"-Wl,-rpath,{pkg}"], check=True)
+    deck_path = golden("sedov.pnt")
+    r = subprocess.run([str(exe), deck_path], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    lines = dict(line.split(" ", 1) for line in r.stdout.strip().splitlines())
+
+    d = pb.Deck(path=deck_path)
+    m = pb.Mesh(deck=d)
+    p = d.params()
+    assert lines["mesh"].split() == [str(m.numz), str(m.nums), str(m.nump)]
+    want = [p.cstop, p.tstop, p.dtinit, p.q1, p.alfa, p.nbcx, p.nbcy]
+    got = lines["params"].split()
+    assert [int(got[0])] + [float(v) for v in got[1:5]] + [int(v) for v in got[5:]] == want
+    info = m.piece(2, 1).piece_info()
+    assert lines["piece"].split() == [str(info["piece"]), str(info["zone0"]), str(info["nhalo"]),
+                                      str(len(info["nbr"]))]
+    assert int(lines["hydro"]) == pb.PNT_ERR_NO_DEVICE
