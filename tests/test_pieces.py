@@ -15,6 +15,8 @@ import sys
 
 import numpy as np
 import pytest
+from hypothesis import given, settings
+from hypothesis import strategies as st
 import torch.multiprocessing as mp
 
 from conftest import DECKS, golden
@@ -37,42 +39,61 @@ def slot_sides(info, nums, slots):
 @pytest.mark.parametrize("npieces", [2, 3, 7])
 def test_partition_covers_and_keeps_the_corner_order(npieces):
     for name, m in meshes():
-        goff, gsides = m.point_corners()
-        gmapsp1, gmapsz = m.array("mapsp1"), m.array("mapsz")
-        zone_owner = np.full(m.numz, -1)
-        infos = []
-        for q in range(npieces):
-            pm = m.piece(npieces, q)
-            info = pm.piece_info()
-            infos.append((pm, info))
-            z0 = info["zone0"]
-            assert (zone_owner[z0:z0 + pm.numz] == -1).all(), name
-            zone_owner[z0:z0 + pm.numz] = q
-            # local zones' sides are the global sides side0 .. side0 + nums
-            assert (pm.array("mapsz") + z0 == gmapsz[info["side0"]:info["side0"] + pm.nums]).all()
-            # points: exactly those the zones touch, ascending global ids
-            gp = info["gpoint"]
-            assert (np.diff(gp) > 0).all()
-            touched = np.unique(gmapsp1[info["side0"]:info["side0"] + pm.nums])
-            assert np.array_equal(touched, gp), name
-            assert (gp[pm.array("mapsp1")] == gmapsp1[info["side0"]:info["side0"] + pm.nums]).all()
-            assert np.array_equal(pm.array("px"), m.array("px")[gp])
-            # corner lists: the global list of each point, in global order
-            off, slots = pm.point_corners()
-            assert len(slots) == pm.nums + info["nhalo"]
-            sides_of_slots = slot_sides(info, pm.nums, slots)
-            for p in range(pm.nump):
-                g = gp[p]
-                assert np.array_equal(sides_of_slots[off[p]:off[p + 1]], gsides[goff[g]:goff[g + 1]]), (name, q, p)
-        assert (zone_owner >= 0).all(), name
-        # send lists of i to j = the halo slots j receives from i, same order
-        for q, (pm, info) in enumerate(infos):
-            for j, r in enumerate(info["nbr"]):
-                rpm, rinfo = infos[r]
-                k = list(rinfo["nbr"]).index(q)
-                sent = info["send_side"][info["send_off"][j]:info["send_off"][j + 1]] + info["side0"]
-                recv = rinfo["halo_side"][rinfo["recv_off"][k]:rinfo["recv_off"][k + 1]]
-                assert np.array_equal(sent, recv), (name, q, r)
+        check_partition(name, m, npieces)
+
+
+@settings(max_examples=40, deadline=None)
+@given(kind=st.sampled_from(["rect", "pie"]), nx=st.integers(1, 12), ny=st.integers(1, 12),
+       npieces=st.integers(2, 64))
+def test_partition_of_random_meshes(kind, nx, ny, npieces):
+    extra = "1.0 1.0" if kind == "rect" else "90.0 1.0"
+    m = pb.Mesh(deck=pb.Deck(text=f"cstop 1\nmeshtype {kind}\nmeshparams {nx} {ny} {extra}\n"))
+    if npieces > m.numz:
+        with pytest.raises(pb.PntError):
+            m.piece(npieces, 0)
+        return
+    check_partition(f"{kind} {nx}x{ny}", m, npieces)
+
+
+def check_partition(name, m, npieces):
+    """Invariants (1)-(3) of the module docstring and the pairing of send
+    lists with halo slots, for `m` split into npieces."""
+    goff, gsides = m.point_corners()
+    gmapsp1, gmapsz = m.array("mapsp1"), m.array("mapsz")
+    zone_owner = np.full(m.numz, -1)
+    infos = []
+    for q in range(npieces):
+        pm = m.piece(npieces, q)
+        info = pm.piece_info()
+        infos.append((pm, info))
+        z0 = info["zone0"]
+        assert (zone_owner[z0:z0 + pm.numz] == -1).all(), name
+        zone_owner[z0:z0 + pm.numz] = q
+        # local zones' sides are the global sides side0 .. side0 + nums
+        assert (pm.array("mapsz") + z0 == gmapsz[info["side0"]:info["side0"] + pm.nums]).all()
+        # points: exactly those the zones touch, ascending global ids
+        gp = info["gpoint"]
+        assert (np.diff(gp) > 0).all()
+        touched = np.unique(gmapsp1[info["side0"]:info["side0"] + pm.nums])
+        assert np.array_equal(touched, gp), name
+        assert (gp[pm.array("mapsp1")] == gmapsp1[info["side0"]:info["side0"] + pm.nums]).all()
+        assert np.array_equal(pm.array("px"), m.array("px")[gp])
+        # corner lists: the global list of each point, in global order
+        off, slots = pm.point_corners()
+        assert len(slots) == pm.nums + info["nhalo"]
+        sides_of_slots = slot_sides(info, pm.nums, slots)
+        for p in range(pm.nump):
+            g = gp[p]
+            assert np.array_equal(sides_of_slots[off[p]:off[p + 1]], gsides[goff[g]:goff[g + 1]]), (name, q, p)
+    assert (zone_owner >= 0).all(), name
+    # send lists of i to j = the halo slots j receives from i, same order
+    for q, (pm, info) in enumerate(infos):
+        for j, r in enumerate(info["nbr"]):
+            rpm, rinfo = infos[r]
+            k = list(rinfo["nbr"]).index(q)
+            sent = info["send_side"][info["send_off"][j]:info["send_off"][j + 1]] + info["side0"]
+            recv = rinfo["halo_side"][rinfo["recv_off"][k]:rinfo["recv_off"][k + 1]]
+            assert np.array_equal(sent, recv), (name, q, r)
 
 
 def test_one_piece_is_the_mesh():
