@@ -1,4 +1,4 @@
-// main.cpp -- `pennant [-n numpcs] -f deck.pnt`: the reference's command line
+// main.cpp -- `pennant [legion args] [-n numpcs] [-g gpu] [-d] -f deck.pnt`: the reference's command line
 // (main.cc:46-107) and Driver::run (Driver.cc:65-187) on the GPU library.
 //
 // Output: the reference's report lines (Driver.cc:344-345), the run summary
@@ -12,6 +12,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+
+#include <unistd.h>
 
 namespace {
 
@@ -28,12 +30,25 @@ int main(int argc, char** argv) {
     const char* filename = nullptr;
     int device = 0;
     bool warn = true;
-    for (int i = 1; i < argc;) {
+    // Legion runtime arguments lead the command line in the reference's run
+    // scripts (main.cc:53-57: -ll:*, -lg:*, -ca:*, -le:*, -dm:* with one
+    // value each); there is no runtime here, so they are skipped.
+    int i = 1;
+    while (i < argc && (!strncmp(argv[i], "-ll", 3) || !strncmp(argv[i], "-lg", 3) || !strncmp(argv[i], "-ca", 3) ||
+                        !strncmp(argv[i], "-le", 3) || !strncmp(argv[i], "-dm", 3)))
+        i += 2;
+    while (i < argc) {
         if (!strcmp(argv[i], "-f") && i + 1 < argc) { filename = argv[i + 1]; i += 2; }
         else if (!strcmp(argv[i], "-n") && i + 1 < argc) { numpcs = atoi(argv[i + 1]); i += 2; }
         else if (!strcmp(argv[i], "-g") && i + 1 < argc) { device = atoi(argv[i + 1]); i += 2; }
+        else if (!strcmp(argv[i], "-d")) {
+            // the reference spins here until a debugger clears a flag
+            // (main.cc:90-91); this build prints its pid and carries on
+            fprintf(stderr, "pennant: pid %ld (-d: attach a debugger now; no wait)\n", (long)getpid());
+            ++i;
+        }
         else {
-            if (warn) fprintf(stderr, "Usage: pennant [-n <numpcs>] [-g <gpu>] -f <filename>\n");
+            if (warn) fprintf(stderr, "Usage: pennant [legion args] [-n <numpcs>] [-g <gpu>] [-d] -f <filename>\n");
             warn = false;
             ++i;
         }

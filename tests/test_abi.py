@@ -53,6 +53,22 @@ def test_cli_binary_exists():
     assert r.returncode == 1 and "No Pennant input file" in r.stderr
 
 
+def test_cli_skips_legion_arguments_and_accepts_debug_flag(tmp_path):
+    """Run scripts of the reference put Legion runtime arguments first
+    (-ll:cpu 4 -ll:gpu 1 ...); they are skipped, -d is accepted, and the
+    deck is read and meshed before the GPU is asked for (without one, the
+    run stops there with an error)."""
+    exe = os.path.join(ROOT, "pennant-legion_b200", "pennant")
+    deck = tmp_path / "sedovsmall.pnt"      # outputs land beside the deck
+    deck.write_text(open(os.path.join(ROOT, "tests", "golden", "sedovsmall.pnt")).read())
+    r = subprocess.run([exe, "-ll:cpu", "4", "-ll:gpu", "1", "-lg:prof", "0", "-d", "-f", str(deck)],
+                       capture_output=True, text=True, timeout=120)
+    assert "Usage" not in r.stderr
+    assert "Zones:   81" in r.stdout and "Sides:   324" in r.stdout
+    if not _has_device():
+        assert r.returncode == 1 and "no CUDA device" in r.stderr
+
+
 def _has_device():
     n = ctypes.c_int(0)
     try:
