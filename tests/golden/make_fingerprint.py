@@ -6,7 +6,10 @@ The fingerprint holds, per field, the SHA-256 of the float64 array bytes
 evenly spaced indices, so a mismatch can still be measured against the 1e-11
 relative bound.
 
-Usage: python tests/golden/make_fingerprint.py <deck.pnt> <out.json>
+Usage: python tests/golden/make_fingerprint.py <deck.pnt> <out.json> [cstop]
+
+With cstop the run stops after that many cycles (a "cstop N" line is added
+to the deck text; the decks used this way have no cstop of their own).
 """
 import hashlib
 import json
@@ -41,15 +44,23 @@ def fingerprint(arrays: dict, meta: dict) -> dict:
     return out
 
 
-def main(deck: str, out_json: str) -> None:
+def main(deck: str, out_json: str, cstop: int = 0) -> None:
     t0 = time.time()
-    o = Oracle(deck)
+    if cstop:
+        text = open(deck).read()
+        if any(line.split()[:1] == ["cstop"] for line in text.splitlines()):
+            raise SystemExit(f"{deck} has a cstop of its own")
+        o = Oracle(text=text.rstrip("\n") + f"\ncstop {cstop}\n")
+    else:
+        o = Oracle(deck)
     st = o.run()
     if st:
         raise SystemExit(f"oracle failed with status {st}")
     meta = {"deck": os.path.basename(deck), "cycle": o.num("cycle"),
             "time": float(o.scalar("time")).hex(), "dt": float(o.scalar("dt")).hex(),
             "oracle_seconds": round(time.time() - t0, 1)}
+    if cstop:
+        meta["cstop"] = cstop
     fp = fingerprint({k: o.field(k) for k in FIELDS}, meta)
     with open(out_json, "w") as f:
         json.dump(fp, f, indent=0)
@@ -57,4 +68,4 @@ def main(deck: str, out_json: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1], sys.argv[2])
+    main(sys.argv[1], sys.argv[2], int(sys.argv[3]) if len(sys.argv) > 3 else 0)

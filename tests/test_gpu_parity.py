@@ -180,6 +180,25 @@ def test_sedov480_to_t1_matches_oracle_fingerprint():
     _fp_compare(fp, h, "sedov480")
 
 
+@pytest.mark.slow
+@pytest.mark.parametrize("fp_name,deck_name", [("leblanc2880x288_c400_fingerprint.json", "leblanc2880x288.pnt"),
+                                               ("sedov1920_c100_fingerprint.json", "sedov1920.pnt")])
+def test_full_size_meshes_match_oracle_fingerprints(fp_name, deck_name):
+    """The FP64 cycle on the full-size meshes of the mixed-precision and
+    learned-closure workloads (2880x288 Leblanc, 1920^2 Sedov), from the
+    deck's initial state for the fingerprint's cycles, bit for bit against
+    the oracle's final state (tests/golden/make_fingerprint.py with cstop)."""
+    fp = json.load(open(golden(fp_name)))
+    d = pb.Deck(path=deck(deck_name))
+    d.set("cstop", fp["cstop"])
+    h = pb.Hydro(pb.Mesh(deck=d), d.params())
+    s = h.run()
+    assert s["cycle"] == fp["cycle"] == fp["cstop"]
+    assert s["time"] == float.fromhex(fp["time"])
+    _fp_compare(fp, h, deck_name)
+    h.close()
+
+
 def test_copy_state_restarts_bitwise():
     """pnt_hydro_copy_state: an object restarted from another's state
     continues exactly as the source does (same fields after the same cycles),
