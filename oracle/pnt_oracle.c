@@ -1121,6 +1121,25 @@ double orc_scalar(const orc_sim* sim, const char* w) {
     if (!strcmp(w, "dtnew")) return sim->dtnew;
     if (!strcmp(w, "dvovmax")) return sim->dvovmax;
     if (!strcmp(w, "tstop")) return sim->tstop;
+    /* the deck parameters (Driver.cc:78-87, Hydro.cc:206-214,
+     * PolyGas.cc:58-59, TTS.cc:46-47, QCS.cc:84-86) */
+    if (!strcmp(w, "dtmax")) return sim->dtmax;
+    if (!strcmp(w, "dtinit")) return sim->dtinit;
+    if (!strcmp(w, "dtfac")) return sim->dtfac;
+    if (!strcmp(w, "cfl")) return sim->cfl;
+    if (!strcmp(w, "cflv")) return sim->cflv;
+    if (!strcmp(w, "rinit")) return sim->rinit;
+    if (!strcmp(w, "einit")) return sim->einit;
+    if (!strcmp(w, "rinitsub")) return sim->rinitsub;
+    if (!strcmp(w, "einitsub")) return sim->einitsub;
+    if (!strcmp(w, "uinitradial")) return sim->uinitradial;
+    if (!strcmp(w, "gamma")) return sim->pgamma;
+    if (!strcmp(w, "pgas_ssmin")) return sim->pssmin;
+    if (!strcmp(w, "alfa")) return sim->alfa;
+    if (!strcmp(w, "tts_ssmin")) return sim->tssmin;
+    if (!strcmp(w, "qgamma")) return sim->qgamma;
+    if (!strcmp(w, "q1")) return sim->q1;
+    if (!strcmp(w, "q2")) return sim->q2;
     return NAN;
 }
 

@@ -29,12 +29,15 @@ def mesh_decks(draw):
         params = f"{nx} {ny} {theta!r} {draw(extent)!r}"
     lines = [f"cstop {draw(st.integers(1, 50))}", f"meshtype {kind}", f"meshparams {params}"]
     if draw(st.booleans()):
+        lines.append(f"dtreport {draw(st.integers(1, 1000))}")
+    if draw(st.booleans()):
         lines.append(f"tstop {draw(extent)!r}")
     if draw(st.booleans()):
         a, b = sorted(draw(st.lists(extent, min_size=2, max_size=2)))
         c, d = sorted(draw(st.lists(extent, min_size=2, max_size=2)))
         lines.append(f"subregion {a!r} {b!r} {c!r} {d!r}")
-    for key in ("dtinit", "cfl", "cflv", "q1", "q2", "alfa", "ssmin", "gamma", "einitsub", "uinitradial"):
+    for key in ("dtinit", "dtmax", "dtfac", "cfl", "cflv", "q1", "q2", "qgamma", "alfa", "ssmin", "gamma", "rinit",
+                "einit", "rinitsub", "einitsub", "uinitradial"):
         if draw(st.booleans()):
             lines.append(f"{key} {draw(extent)!r}")
     for key in ("bcx", "bcy"):
@@ -74,7 +77,10 @@ def test_random_decks_build_the_same_mesh_as_the_oracle(text):
         np.testing.assert_array_equal(m.array(k), o.field(k), err_msg=f"{k}\n{text}")
     assert m.array("px").tobytes() == o.field("px").tobytes(), text
     p = d.params()
-    assert p.cstop == o.num("cstop") and p.tstop == o.scalar("tstop"), text
+    assert p.cstop == o.num("cstop") and p.dtreport == o.num("dtreport"), text
+    for k in ("tstop", "dtmax", "dtinit", "dtfac", "cfl", "cflv", "rinit", "einit", "rinitsub", "einitsub",
+              "uinitradial", "gamma", "pgas_ssmin", "alfa", "tts_ssmin", "qgamma", "q1", "q2"):
+        assert getattr(p, k) == o.scalar(k), (k, getattr(p, k), o.scalar(k), text)
     # the boundary point sets
     px = m.array("px")
     planes = [(0, v) for v in p.bcx[:p.nbcx]] + [(1, v) for v in p.bcy[:p.nbcy]]
