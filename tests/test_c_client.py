@@ -87,3 +87,78 @@ def test_plain_c_client_against_the_python_binding(tmp_path):
     assert lines["piece"].split() == [str(info["piece"]), str(info["zone0"]), str(info["nhalo"]),
                                       str(len(info["nbr"]))]
     assert int(lines["hydro"]) == pb.PNT_ERR_NO_DEVICE
+
+
+CPP_SOURCE = r"""
+#include <cstdio>
+#include "pennant.hh"
+
+int main(int argc, char** argv) {
+    if (argc != 2) return 1;
+    pnt::InputFile inp(argv[1]);
+    pnt::Mesh mesh(&inp);
+    pnt::PolyGas pgas(&inp, nullptr);
+    pnt::TTS tts(&inp, nullptr);
+    pnt::QCS qcs(&inp, nullptr);
+    std::printf("mesh %d %d %d %d\n", mesh.nump, mesh.numz, mesh.nums, mesh.numc);
+    std::printf("side %d %d %d %d %d\n", mesh.mapsp1()[5], mesh.mapsp2()[5], mesh.mapsz()[5], mesh.mapss3()[5],
+                mesh.mapss4()[5]);
+    std::printf("coef %.17g %.17g %.17g %.17g %.17g %.17g %.17g\n", pgas.gamma, pgas.ssmin, tts.alfa, tts.ssmin,
+                qcs.qgamma, qcs.q1, qcs.q2);
+    const std::vector<double> bcx = inp.getDoubleList("bcx", {}), bcy = inp.getDoubleList("bcy", {});
+    for (double b : bcx) {
+        pnt::HydroBC bc(&mesh, pnt::double2{1., 0.}, b, true);
+        std::printf("bc %d", bc.numb);
+        for (int p : bc.mapbp) std::printf(" %d", p);
+        std::printf("\n");
+    }
+    for (double b : bcy) {
+        pnt::HydroBC bc(&mesh, pnt::double2{0., 1.}, b, false);
+        std::printf("bc %d", bc.numb);
+        for (int p : bc.mapbp) std::printf(" %d", p);
+        std::printf("\n");
+    }
+    try {
+        pnt::Driver drv(&inp, "client");
+        std::printf("driver %d\n", 0);
+    } catch (const pnt::Error& e) {
+        std::printf("driver %d\n", (int)e.status);
+    }
+    return 0;
+}
+"""
+
+
+@pytest.mark.skipif(_has_device(), reason="checks the no-device answer of the C++ classes")
+def test_cpp_classes_against_the_oracle(tmp_path):
+    """The reference's class surface in C++ (pennant.hh): InputFile, Mesh
+    with its side maps, PolyGas / TTS / QCS coefficients, HydroBC boundary
+    point lists, and Driver, which without a GPU throws pnt::Error with
+    PNT_ERR_NO_DEVICE.  Coefficients and boundary lists agree with the
+    oracle's independent restatement."""
+    from oracle import Oracle
+    src = tmp_path / "client.cpp"
+    src.write_text(CPP_SOURCE)
+    exe = tmp_path / "client"
+    pkg = os.path.dirname(pb.LIB_PATH)
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    "-I", os.path.join(pkg, "csrc"), str(src), "-o", str(exe), "-L", pkg, "-lpennant_b200",
+                    f"-Wl,-rpath,{pkg}"], check=True)
+    for name in ("sedov.pnt", "leblanc.pnt", "nohsquare.pnt"):
+        deck_path = golden(name)
+        r = subprocess.run([str(exe), deck_path], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        rows = [line.split() for line in r.stdout.strip().splitlines()]
+        o = Oracle(deck_path)
+        mesh = next(r[1:] for r in rows if r[0] == "mesh")
+        assert [int(v) for v in mesh] == [o.nump, o.numz, o.nums, o.nums]
+        side = [int(v) for v in next(r[1:] for r in rows if r[0] == "side")]
+        assert side == [int(o.field(k)[5]) for k in ("mapsp1", "mapsp2", "mapsz", "mapss3", "mapss4")]
+        coef = [float(v) for v in next(r[1:] for r in rows if r[0] == "coef")]
+        assert coef == [o.scalar(k) for k in ("gamma", "pgas_ssmin", "alfa", "tts_ssmin", "qgamma", "q1", "q2")]
+        bcs = [r[1:] for r in rows if r[0] == "bc"]
+        assert len(bcs) == o.num("nbc")
+        for b, row in enumerate(bcs):
+            pts = [int(v) for v in row[1:]]
+            assert int(row[0]) == len(pts) and pts == o.field(f"bcpts{b}").tolist(), (name, b)
+        assert int(next(r[1] for r in rows if r[0] == "driver")) == pb.PNT_ERR_NO_DEVICE
