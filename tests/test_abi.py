@@ -33,6 +33,16 @@ def test_dynamic_symbol_table_has_c_linkage():
         assert s in names, s
 
 
+def test_only_the_c_abi_is_exported():
+    """Internal C++ symbols stay local (csrc/exports.map): a client's own
+    classes of the same names cannot interpose on them."""
+    out = subprocess.run(["nm", "-D", "--defined-only", pb.LIB_PATH], capture_output=True, text=True,
+                         check=True).stdout
+    names = [line.split()[-1] for line in out.splitlines() if line.strip()]
+    assert names and all(n.startswith("pnt_") for n in names), [n for n in names if not n.startswith("pnt_")]
+    assert sorted(names) == _header_symbols()
+
+
 def test_status_strings():
     for st in range(0, 10):
         assert pb.lib.pnt_status_string(st)
