@@ -546,11 +546,11 @@ pnt_status pnt_batch_create(const pnt_mesh* const* meshes, const pnt_params* par
         a.numz = (int32_t)NZ;
         a.nums = (int32_t)NS;
         a.quads = 0;
-        int32_t *d_zfirst, *d_znump, *d_mapsp1, *d_poff, *d_pcorner;
-        double* d_smf;
-        uint16_t* d_mask;
-        HydroConst* d_consts;
-        Ctl* d_ctls;
+        int32_t *d_zfirst = nullptr, *d_znump = nullptr, *d_mapsp1 = nullptr, *d_poff = nullptr, *d_pcorner = nullptr;
+        double* d_smf = nullptr;
+        uint16_t* d_mask = nullptr;
+        HydroConst* d_consts = nullptr;
+        Ctl* d_ctls = nullptr;
         if ((st = bt->alloc(&d_zfirst, NZ)) || (st = bt->alloc(&d_znump, NZ)) || (st = bt->alloc(&d_mapsp1, NS)) ||
             (st = bt->alloc(&d_smf, NS)) || (st = bt->alloc(&d_poff, NP + 1)) || (st = bt->alloc(&d_pcorner, NS)) ||
             (st = bt->alloc(&d_mask, NP + 2)) || (st = bt->alloc(&a.px[0], NP)) || (st = bt->alloc(&a.px[1], NP)) ||

@@ -86,8 +86,6 @@ __global__ void __launch_bounds__(kZoneThreads) harvest_kernel(DevArrays a, Hydr
     const double zm = zok ? a.zm[z] : 1.;
     const double zr = zok ? a.zr[z] : 1.;
     const double ze = zok ? a.ze[z] : 0.;
-    const double zwrate = zok ? a.zwrate[z] : 0.;
-    const double zvol0 = zok ? a.zvol[z] : 1.;
 
     const double dth = 0.5 * dt;
     const double2 xp = add(x0, smul(dth, u0));

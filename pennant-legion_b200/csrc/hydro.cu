@@ -298,9 +298,9 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
     a.numz = (int32_t)nz;
     a.nums = (int32_t)ns;
     a.quads = m.all_quads ? 1 : 0;
-    int32_t *zfirst, *znump, *mapsp1, *poff, *pcorner;
-    double* smf;
-    uint16_t* mask;
+    int32_t *zfirst = nullptr, *znump = nullptr, *mapsp1 = nullptr, *poff = nullptr, *pcorner = nullptr;
+    double* smf = nullptr;
+    uint16_t* mask = nullptr;
     // the persistent pass C's grid
     {
         int nsm = 148;
