@@ -43,7 +43,6 @@ __device__ __forceinline__ double2 mk(double x, double y) { return make_double2(
 __device__ __forceinline__ double2 add(double2 a, double2 b) { return mk(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 sub(double2 a, double2 b) { return mk(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 smul(double r, double2 v) { return mk(v.x * r, v.y * r); }
-__device__ __forceinline__ double2 neg(double2 a) { return mk(-a.x, -a.y); }
 __device__ __forceinline__ double dot(double2 a, double2 b) { return a.x * b.x + a.y * b.y; }
 __device__ __forceinline__ double cross(double2 a, double2 b) { return a.x * b.y - a.y * b.x; }
 __device__ __forceinline__ double2 project(double2 v, double ux, double uy) {
@@ -63,11 +62,6 @@ __device__ __forceinline__ float flen(float2 v) { return sqrtf(v.x * v.x + v.y *
 __device__ __forceinline__ float flen2(float2 v) { return v.x * v.x + v.y * v.y; }
 __device__ __forceinline__ float2 f2(double2 v) { return fk((float)v.x, (float)v.y); }
 
-__device__ __forceinline__ double shfl(double v, int src) { return __shfl_sync(kFull, v, src); }
-__device__ __forceinline__ float shflf(float v, int src) { return __shfl_sync(kFull, v, src); }
-__device__ __forceinline__ double2 shfl2(double2 v, int src) {
-    return mk(__shfl_sync(kFull, v.x, src), __shfl_sync(kFull, v.y, src));
-}
 __device__ __forceinline__ float2 shflf2(float2 v, int src) {
     return fk(__shfl_sync(kFull, v.x, src), __shfl_sync(kFull, v.y, src));
 }
