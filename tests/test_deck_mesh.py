@@ -4,8 +4,6 @@ The product's mesh builder (libpennant_b200.so, C++) and the oracle (C)
 restate GenMesh independently; connectivity, coordinates, boundary point
 sets and the point->corner CSR must agree bit for bit.
 """
-import os
-
 import numpy as np
 import pytest
 

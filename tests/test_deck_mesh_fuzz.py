@@ -5,7 +5,6 @@ deck both accept or both reject it, and when they accept, the connectivity,
 the coordinates (bitwise) and the parameters agree.  Random junk text never
 crashes the parser: it answers with a status."""
 import numpy as np
-import pytest
 from hypothesis import HealthCheck, event, given, settings
 from hypothesis import strategies as st
 

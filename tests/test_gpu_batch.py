@@ -1,7 +1,6 @@
 """Batched meshes (needs a GPU): every instance of a batch must be bit-identical
 to its own single-mesh run (itself bit-identical to the CPU oracle),
 whatever the work-list shape and after the autotuner has run."""
-import os
 import sys
 
 import numpy as np

@@ -8,7 +8,6 @@ fingerprint test measures the relative error explicitly.
 """
 import hashlib
 import json
-import os
 
 import numpy as np
 import pytest

@@ -9,7 +9,6 @@ import os
 import socket
 import sys
 
-import numpy as np
 import pytest
 import torch.multiprocessing as mp
 
