@@ -239,3 +239,30 @@ def test_a_lost_rank_ends_the_exchange_with_an_error(mode):
     assert out[1] == "left"
     assert out[0][0] == "error", out[0]
     assert out[0][1] < 11, out[0]
+
+
+def _reduce_rank(rank, world, port, out):
+    import torch
+    import torch.distributed as dist
+    from pennant_b200.pieces import reduce_scalars
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        # {dtnew, -dvovmax, inverted sides in pass A, in pass C} of this piece
+        red = torch.tensor([1e-3 * (rank + 2), -0.01 * (rank + 1), float(rank), 2.0 * rank], dtype=torch.float64)
+        reduce_scalars(red)
+        out[rank] = red.tolist()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_piece_scalars_reduce_over_gloo(world):
+    """The per-cycle scalars: minimum dtnew and -dvovmax (the maximum dV/V),
+    summed inverted-side counts, the same on every rank."""
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    mp.start_processes(_reduce_rank, args=(world, _free_port(), out), nprocs=world, join=True, start_method="spawn")
+    want = [2e-3, -0.01 * world, float(sum(range(world))), 2.0 * sum(range(world))]
+    for r in range(world):
+        assert out[r] == want, (r, out[r])
