@@ -4,6 +4,8 @@ The product's mesh builder (libpennant_b200.so, C++) and the oracle (C)
 restate GenMesh independently; connectivity, coordinates, boundary point
 sets and the point->corner CSR must agree bit for bit.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -195,3 +197,20 @@ def test_bc_point_sets_match_oracle(name):
     for b, (axis, bound) in enumerate(planes):
         mine = np.nonzero(np.abs(px[:, axis] - bound) < 1e-12)[0]
         np.testing.assert_array_equal(mine, o.field(f"bcpts{b}"))
+
+
+def test_committed_decks_are_what_make_decks_writes():
+    """The benchmark decks in the package are exactly make_decks.py's output
+    (no hand edits), and the batch workload is reproducible from its seed:
+    256 instances, N in [32, 512], E0 in [0.1, 1], gamma in [1.4, 5/3]."""
+    import sys
+    from conftest import DECKS as DECK_DIR
+    sys.path.insert(0, DECK_DIR)
+    import make_decks
+    for name, text in make_decks.DECKS.items():
+        with open(os.path.join(DECK_DIR, name)) as f:
+            assert f.read() == text, name
+    a, b = make_decks.sedov_batch(), make_decks.sedov_batch()
+    assert a == b and len(a) == 256
+    assert all(32 <= i["n"] <= 512 and 0.1 <= i["e0"] <= 1.0 and 1.4 <= i["gamma"] <= 5 / 3 for i in a)
+    assert len({i["n"] for i in a}) > 50   # uneven sizes
