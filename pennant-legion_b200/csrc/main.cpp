@@ -31,7 +31,7 @@ int main(int argc, char** argv) {
     int device = 0;
     bool warn = true;
     // Legion runtime arguments lead the command line in the reference's run
-    // scripts (main.cc:53-57: -ll:*, -lg:*, -ca:*, -le:*, -dm:* with one
+    // scripts (main.cc:52-58: -ll:*, -lg:*, -ca:*, -le:*, -dm:* with one
     // value each); there is no runtime here, so they are skipped.
     int i = 1;
     while (i < argc && (!strncmp(argv[i], "-ll", 3) || !strncmp(argv[i], "-lg", 3) || !strncmp(argv[i], "-ca", 3) ||
@@ -43,7 +43,7 @@ int main(int argc, char** argv) {
         else if (!strcmp(argv[i], "-g") && i + 1 < argc) { device = atoi(argv[i + 1]); i += 2; }
         else if (!strcmp(argv[i], "-d")) {
             // the reference spins here until a debugger clears a flag
-            // (main.cc:90-91); this build prints its pid and carries on
+            // (main.cc:92-93); this build prints its pid and carries on
             fprintf(stderr, "pennant: pid %ld (-d: attach a debugger now; no wait)\n", (long)getpid());
             ++i;
         }
