@@ -350,8 +350,10 @@ pnt_status pnt_op_calc_dt(const double* zdl, const double* zdu, const double* zs
  * PNT_OP_CALC_DT_NOALLOC_MAX_ZONES (larger numz: PNT_ERR_INVALID_ARG).
  * Runs on the calling thread's current device.  The first call on a
  * device looks up the array's address: make it before any stream capture.
- * All calls on a device share the array, so calls that overlap on the GPU
- * race; serialise them. */
+ * A device reset (cudaDeviceReset, or the end of the device's context)
+ * moves the array; the next call after it looks the address up again, so
+ * make that call before stream capture as well.  All calls on a device
+ * share the array, so calls that overlap on the GPU race; serialise them. */
 #define PNT_OP_CALC_DT_NOALLOC_MAX_ZONES 16777216
 pnt_status pnt_op_calc_dt_noalloc(const double* zdl, const double* zdu, const double* zss,
                                   const double* zvol, const double* zvol0, int64_t numz,

@@ -284,9 +284,16 @@ __device__ __forceinline__ void mlp_hidden_epilogue(uint32_t tacc, const float* 
 // t % 128).  Every thread of the CTA calls setup once, rows once per batch
 // of 256 rows, and teardown once.  smem: kMlpSmemBytes of dynamic shared
 // memory (16-byte aligned); gimg: the parameter image in global memory.
+//
+// Tensor-core waits are bounded.  Once a wait runs out on any thread, the
+// CTA agrees on it at its next barrier (__syncthreads_and) and issues no
+// further MMA, commit or TMEM load: the rows of that batch and of every
+// later one come out as zeros, and teardown waits (bounded again) for the
+// last commit issued, which covers every MMA still in flight, before it
+// frees the TMEM columns.
 struct MlpState {
     uint32_t tbase;   // TMEM columns of the two accumulators
-    uint32_t phase;   // completed mbarrier phases
+    uint32_t phase;   // commits issued (each ends one mbarrier phase)
     bool ok;          // every tensor-core wait so far completed
 };
 
@@ -309,13 +316,18 @@ __device__ __forceinline__ void closure_mlp_setup(uint8_t* smem, const uint8_t* 
 }
 
 // f: this row's raw inputs; out: its 4 outputs, denormalised (zero after a
-// wait ran out).
+// wait ran out, in this batch or an earlier one).
 __device__ __forceinline__ void closure_mlp_rows(uint8_t* smem, MlpState& st, const float* f, float* out) {
     const int t = threadIdx.x;
     const int warp = t >> 5;
     const int tile = t >> 7;
     const int row = t & 127;
     const uint32_t mbar = smem_addr(smem + kSmBar);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) out[i] = 0.f;
+    // a wait that ran out earlier on any thread: no more tensor-core work
+    st.ok = __syncthreads_and(st.ok) != 0;
+    if (!st.ok) return;
     // normalised inputs -> this row of the layer-1 A operand
     {
         const float* mean = reinterpret_cast<const float*>(smem + kImgFMean);
@@ -344,15 +356,16 @@ __device__ __forceinline__ void closure_mlp_rows(uint8_t* smem, MlpState& st, co
                       umma_idesc_bf16(128, 64), 0u);
         umma_commit(mbar);
     }
-    st.ok = mbar_wait(mbar, st.phase & 1) && st.ok;
     ++st.phase;
+    bool w = mbar_wait(mbar, (st.phase - 1) & 1);
     tc_fence_after();
     uint8_t* hrow = smem + kSmH + tile * 16384 + row * 16;
-    mlp_hidden_epilogue(tacc, reinterpret_cast<const float*>(smem + kImgB1), hrow);
+    if (w) mlp_hidden_epilogue(tacc, reinterpret_cast<const float*>(smem + kImgB1), hrow);
     fence_async_smem();
     tc_fence_before();
-    __syncthreads();
+    st.ok = __syncthreads_and(w) != 0;
     tc_fence_after();
+    if (!st.ok) return;
 
     // layer 2: [128 x 64] x [64 x 64]
     if (t == 0) {
@@ -362,14 +375,15 @@ __device__ __forceinline__ void closure_mlp_rows(uint8_t* smem, MlpState& st, co
                           umma_desc(sb + kImgW2 + kb * 2048, 1024, 128), umma_idesc_bf16(128, 64), kb > 0 ? 1u : 0u);
         umma_commit(mbar);
     }
-    st.ok = mbar_wait(mbar, st.phase & 1) && st.ok;
     ++st.phase;
+    w = mbar_wait(mbar, (st.phase - 1) & 1);
     tc_fence_after();
-    mlp_hidden_epilogue(tacc, reinterpret_cast<const float*>(smem + kImgB2), hrow);
+    if (w) mlp_hidden_epilogue(tacc, reinterpret_cast<const float*>(smem + kImgB2), hrow);
     fence_async_smem();
     tc_fence_before();
-    __syncthreads();
+    st.ok = __syncthreads_and(w) != 0;
     tc_fence_after();
+    if (!st.ok) return;
 
     // layer 3: [128 x 64] x [64 x 16] (4 outputs used)
     if (t == 0) {
@@ -379,25 +393,37 @@ __device__ __forceinline__ void closure_mlp_rows(uint8_t* smem, MlpState& st, co
                           umma_desc(sb + kImgW3 + kb * 512, 256, 128), umma_idesc_bf16(128, 16), kb > 0 ? 1u : 0u);
         umma_commit(mbar);
     }
-    st.ok = mbar_wait(mbar, st.phase & 1) && st.ok;
     ++st.phase;
+    w = mbar_wait(mbar, (st.phase - 1) & 1);
     tc_fence_after();
-    float y[4];
-    tmem_ld4(tacc, y);
-    const float* b3 = reinterpret_cast<const float*>(smem + kImgB3);
-    const float* tmean = reinterpret_cast<const float*>(smem + kImgTMean);
-    const float* tstd = reinterpret_cast<const float*>(smem + kImgTStd);
+    if (w) {
+        float y[4];
+        tmem_ld4(tacc, y);
+        const float* b3 = reinterpret_cast<const float*>(smem + kImgB3);
+        const float* tmean = reinterpret_cast<const float*>(smem + kImgTMean);
+        const float* tstd = reinterpret_cast<const float*>(smem + kImgTStd);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) out[i] = st.ok ? (y[i] + b3[i]) * tstd[i] + tmean[i] : 0.f;
+        for (int i = 0; i < 4; ++i) out[i] = (y[i] + b3[i]) * tstd[i] + tmean[i];
+    }
+    // this thread's view; the next batch's (or teardown's) barrier makes it
+    // the CTA's
+    st.ok = w;
     // the next batch's layer-1 MMA overwrites these accumulators after the
     // barrier that follows its input writes
     tc_fence_before();
 }
 
-// Returns false on every thread if any tensor-core wait ran out.
-__device__ __forceinline__ bool closure_mlp_teardown(MlpState& st) {
+// Frees the TMEM columns.  After a wait that ran out, first waits (bounded)
+// for the last commit issued, so no MMA still writes the columns; returns
+// false on every thread if any tensor-core wait ran out.
+__device__ __forceinline__ bool closure_mlp_teardown(uint8_t* smem, MlpState& st) {
     tc_fence_before();
     const bool ok = __syncthreads_and(st.ok) != 0;
+    if (!ok && st.phase > 0) {
+        mbar_wait(smem_addr(smem + kSmBar), (st.phase - 1) & 1);
+        tc_fence_before();
+        __syncthreads();
+    }
     if ((threadIdx.x >> 5) == 0) {
         tc_fence_after();
         tmem_dealloc(st.tbase, kTmemCols);
@@ -411,7 +437,7 @@ __device__ __forceinline__ bool closure_mlp_block(uint8_t* smem, const uint8_t* 
     MlpState st;
     closure_mlp_setup(smem, gimg, st);
     closure_mlp_rows(smem, st, f, out);
-    return closure_mlp_teardown(st);
+    return closure_mlp_teardown(smem, st);
 }
 
 }  // namespace pnt

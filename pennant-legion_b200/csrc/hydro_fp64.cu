@@ -19,11 +19,14 @@
 //
 // Pass A runs one thread per zone (pass_a_zone_thread): the zone's sides
 // in the reference's side order, each zone-level quantity (centre, sums,
-// EOS) formed once, 4-way independent corner work for latency hiding, no
-// shuffles; 168 registers, 3 blocks of 128 per SM (13% faster than four
-// lanes per zone at a developed 1024^2 Sedov state;
-// it is bound by the ~50 correctly rounded FP64 divisions and square roots
-// of a zone).  Pass C is the persistent staged kernel of pass_c.cu (one
+// EOS) formed once, no shuffles, scheduled so the side arrays die early;
+// 128 registers, 4 blocks of 128 per SM.  It is bound by its ~2400
+// instructions per zone, a third of them the correctly rounded FP64
+// divisions and square roots; quotients whose IEEE result is fixed without
+// the division (zero over a finite non-zero divisor, division by one, the
+// zkur square root of a corner without compression) skip it, which a
+// quiescent region (zero velocities and pressure) hits on most corners.
+// Pass C is the persistent staged kernel of pass_c.cu (one
 // thread per zone, inputs gathered into shared memory by asynchronous
 // copies); the batched kernels run the same two bodies.  1/elen is formed
 // once per side and shared with the neighbouring corner; QCS terms the
@@ -37,13 +40,17 @@
 #include <algorithm>
 #include "zone_tiles.cuh"
 
+#ifndef PNT_PF_WAVES
+#define PNT_PF_WAVES 0
+#endif
+
 namespace pnt {
 namespace {
 
 using namespace fp64;
 
 #ifndef PNT_PASS_A_ZT_MIN_BLOCKS
-#define PNT_PASS_A_ZT_MIN_BLOCKS 3
+#define PNT_PASS_A_ZT_MIN_BLOCKS 4
 #endif
 constexpr int kZoneThreadsZT = 128;   // one zone per thread
 
@@ -54,6 +61,16 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_PASS_A_ZT_MIN_BLOCKS) pass
     const int64_t z = (int64_t)blockIdx.x * kZoneThreadsZT + threadIdx.x;
     double zdthyd = 1.e99;
     int bad = 0;
+#if PNT_PF_WAVES
+    if (kQuads) {
+        // warm L2 for the block that runs PNT_PF_WAVES resident waves later
+        const int64_t zf0 = ((int64_t)blockIdx.x + (int64_t)PNT_PF_WAVES * 148 * PNT_PASS_A_ZT_MIN_BLOCKS) * kZoneThreadsZT;
+        const int64_t zf = zf0 + threadIdx.x;
+        const bool ok = zf < a.numz;
+        const int4 pf = ok ? __ldg(reinterpret_cast<const int4*>(a.mapsp1) + zf) : make_int4(0, 0, 0, 0);
+        tiles::prefetch_zone_block(a, ctl->cycle & 1, zf0, pf, ok);
+    }
+#endif
     if (z < a.numz) {
         const int cur = ctl->cycle & 1;
         const double dt = ctl->dt;

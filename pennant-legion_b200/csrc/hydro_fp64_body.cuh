@@ -43,6 +43,27 @@ __device__ __forceinline__ double2 project(double2 v, double ux, double uy) {
 __device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }
 __device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }
 
+// x / y, with the division left out where IEEE 754 fixes its result without
+// it: a zero dividend over a finite non-zero divisor gives a zero whose sign
+// is the XOR of the operands' signs, which is exactly x * y; a divisor of 1
+// gives x (NaN dividends excepted, whose payload a division may change).
+// Every other case is the correctly rounded division.  In a quiescent part
+// of the mesh (zero velocities, zero pressure) most of the QCS quotients
+// take the first two branches.
+__device__ __forceinline__ double xdiv(double x, double y) {
+    if (x == 0.0 && fabs(y) < __longlong_as_double(0x7ff0000000000000LL) && y != 0.0) return x * y;
+    if (y == 1.0 && x == x) return x;
+    return x / y;
+}
+#ifndef PNT_FP64_XDIV
+#define PNT_FP64_XDIV 1
+#endif
+#if PNT_FP64_XDIV
+#define PNT_QDIV(x, y) xdiv((x), (y))
+#else
+#define PNT_QDIV(x, y) ((x) / (y))
+#endif
+
 __device__ __forceinline__ double shfl(double v, int src) { return __shfl_sync(kFull, v, src); }
 __device__ __forceinline__ double2 shfl2(double2 v, int src) {
     return mk(__shfl_sync(kFull, v.x, src), __shfl_sync(kFull, v.y, src));
@@ -121,11 +142,82 @@ __device__ __forceinline__ void block_to_cycle(long long* cyc_red, double v, int
 
 
 // ---------------------------------------------------------------------
+// Pass A, one corner of the QCS (QCS.cc:116-380), shared by the zone
+// bodies below: corner k at point k, its side k and the previous side pk.
+// Returns the two terms of setForce's side sum the corner contributes:
+// A = cw (cqe2 + ccos cqe1) to side k and B = cw (cqe1 + ccos cqe2) to side
+// pk, so sfq[k] = (A_k + B_nk) / elen[k] in the reference's order.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ void qcs_corner(const HydroConst& c, double2 up0, double2 upp, double2 upn, double2 xq0,
+                                           double2 xq1, double2 xq3, double2 zxp, double2 zuc, double de1,
+                                           double de2, double rinv_pk, double rinv_k, double zss, double zrp,
+                                           double2& A, double2& B) {
+    const double2 up1 = smul(0.5, add(up0, upn));
+    const double2 up2 = zuc, xq2 = zxp;
+    const double2 up3 = smul(0.5, add(upp, up0));
+    const double cvolume = 0.5 * cross(sub(xq2, xq0), sub(xq3, xq1));
+    const double2 v1 = sub(xq3, xq0);
+    const double2 v2 = sub(xq1, xq0);
+    const double minelen = dmin(de1, de2);
+    const double ccos = ((minelen < 1.e-12) ? 0. : PNT_QDIV(4. * dot(v1, v2), de1 * de2));
+    const double cdiv = PNT_QDIV(cross(sub(up2, up0), sub(xq3, xq1)) - cross(sub(up3, up1), sub(xq2, xq0)),
+                                 2.0 * cvolume);
+    double evol = 0., du = 0.;
+    if (cdiv < 0.0) {
+        const double2 dxx1 = smul(0.5, sub(sub(add(xq1, xq2), xq0), xq3));
+        const double2 dxx2 = smul(0.5, sub(sub(add(xq2, xq3), xq0), xq1));
+        const double dx1 = length(dxx1);
+        const double dx2 = length(dxx2);
+        const double2 duav = smul(0.25, add(add(add(up0, up1), up2), up3));
+        const double test1 = fabs(dot(dxx1, duav) * dx2);
+        const double test2 = fabs(dot(dxx2, duav) * dx1);
+        const double num = (test1 > test2 ? dx1 : dx2);
+        const double den = (test1 > test2 ? dx2 : dx1);
+        const double r = num / den;
+        evol = sqrt(4.0 * cvolume * r);
+        evol = dmin(evol, 2.0 * minelen);
+        const double dv1 = length2(sub(sub(add(up1, up2), up0), up3));
+        const double dv2 = length2(sub(sub(add(up2, up3), up0), up1));
+        du = sqrt(dmax(dv1, dv2));
+    }
+    double crmu = 0.;
+    if (!(cdiv > 0.0)) {
+        const double ztmp2 = c.q2 * 0.25 * c.gammap1 * du;
+        const double ztmp1 = c.q1 * zss;
+#if PNT_FP64_XDIV
+        // no compression (evol = du = 0): zkur = ztmp2 + sqrt(ztmp2^2 +
+        // ztmp1^2) with ztmp2 a zero is a finite zkur >= +0 when |ztmp1| <
+        // 1e150, and with |zrp| < 1e150 too, (zkur zrp) evol is a zero with
+        // the sign of zrp: exactly zrp * 0
+        if (!(cdiv < 0.0) && ztmp2 == 0.0 && fabs(ztmp1) < 1.e150 && fabs(zrp) < 1.e150) {
+            crmu = zrp * 0.0;
+        } else
+#endif
+        {
+            const double zkur = ztmp2 + sqrt(ztmp2 * ztmp2 + ztmp1 * ztmp1);
+            crmu = zkur * zrp * evol;
+        }
+    }
+    const double2 t1 = smul(crmu, sub(up0, upp));
+    const double2 cqe1 = mk(t1.x * rinv_pk, t1.y * rinv_pk);   // / elen[s]
+    const double2 t2 = smul(crmu, sub(upn, up0));
+    const double2 cqe2 = mk(t2.x * rinv_k, t2.y * rinv_k);     // / elen[s2]
+    const double csin2 = 1.0 - ccos * ccos;
+    const double cw = ((csin2 < 1.e-4) ? 0. : PNT_QDIV(cvolume, csin2));
+    const double cc = ((csin2 < 1.e-4) ? 0. : ccos);
+    A = smul(cw, add(cqe2, smul(cc, cqe1)));
+    B = smul(cw, add(cqe1, smul(cc, cqe2)));
+}
+
+// ---------------------------------------------------------------------
 // Pass A, one thread per zone of N sides (N = 3 or 4, static so the side
-// arrays stay in registers): the arithmetic of pass_a_zone, side by side in
-// the zone's side order, so zone sums keep the reference's serial order and
-// every zone-level quantity is formed once.  nbad counts the zone's
-// inverted sides (checkBadSides counts sides, Mesh.cc:1531-1550).
+// arrays stay in registers): the zone's sides in its side order, so zone
+// sums keep the reference's serial order and every zone-level quantity is
+// formed once.  Scheduled for few live registers: the PolyGas and TTS side
+// forces and setVelDiff are formed before the QCS corner loop (so smf, the
+// side areas and zdl die early), the corners are taken in order and each
+// side is finished as soon as its second corner is known.  nbad counts the
+// zone's inverted sides (checkBadSides counts sides, Mesh.cc:1531-1550).
 // ---------------------------------------------------------------------
 template <int N>
 __device__ __forceinline__ void pass_a_zone_thread(const DevArrays& a, const HydroConst& c, int cur, double dt,
@@ -176,7 +268,7 @@ __device__ __forceinline__ void pass_a_zone_thread(const DevArrays& a, const Hyd
     const double p = c.gm1 * zr * e;
     const double pre = c.gm1 * e;
     const double per = c.gm1 * zr;
-    const double q = (per * p) / (zr * zr);
+    const double q = PNT_QDIV(per * p, zr * zr);
     const double minv = 1. / zm;
     const double csqd = dmax(c.ssmin2, pre + q);
     const double zss = sqrt(csqd);
@@ -185,7 +277,7 @@ __device__ __forceinline__ void pass_a_zone_thread(const DevArrays& a, const Hyd
     const double denom = 1. + 0.5 * per * dv;
     const double src = zwrate * dth * minv;
     const double zrp = zm / zvolp;
-    const double zp = p + (per * src - zr * bulk * dv) / denom;
+    const double zp = p + PNT_QDIV(per * src - zr * bulk * dv, denom);
     a.zp[z] = zp;
     // calcCrnrMass (Hydro.cc:1083-1117)
 #pragma unroll
@@ -193,7 +285,41 @@ __device__ __forceinline__ void pass_a_zone_thread(const DevArrays& a, const Hyd
         const int pk = (k == 0) ? N - 1 : k - 1;
         a.cmass[s0 + k] = zrp * zareap * 0.5 * (mf[k] + mf[pk]);
     }
-    // QCS::setCornerDiv / setQCnForce (QCS.cc:116-327), corner k at point k
+    // PolyGas::calcForce (PolyGas.cc:164-184) and TTS::calcForce (TTS.cc:55-104)
+    double2 ex[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) ex[k] = smul(0.5, add(xp[k], xp[(k + 1 == N) ? 0 : k + 1]));
+    double sstmp = dmax(zss, c.tts_ssmin);
+    sstmp = c.alfa * sstmp * sstmp;
+    double2 sfp[N], sft[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const double2 ssurf = rotateCCW(sub(ex[k], zxp));
+        const double2 fp = smul(-zp, ssurf);
+        const double vfacinv = zareap / sa[k];
+        const double srho = zrp * mf[k] * vfacinv;
+        const double sdp = sstmp * (srho - zrp);
+        sfp[k] = fp;
+        sft[k] = smul(-sdp, ssurf);
+    }
+    // QCS::setVelDiff (QCS.cc:384-448) and calcDtNew (Hydro.cc:1591-1619)
+    {
+        double ztmp = 0.;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const int nk = (k + 1 == N) ? 0 : k + 1;
+            const double2 dxs = sub(xp[nk], xp[k]);
+            const double2 dus = sub(u0[nk], u0[k]);
+            double dux = dot(dus, dxs);
+            dux = (elen[k] > 0. ? PNT_QDIV(fabs(dux), elen[k]) : 0.);
+            ztmp = dmax(ztmp, dux);
+        }
+        const double zdu = c.q1 * zss + 2. * c.q2 * ztmp;
+        const double cdu = dmax(zdu, dmax(zss, 1.e-99));
+        zdthyd = zdl * c.cfl / cdu;
+    }
+    // QCS::setCornerDiv / setQCnForce / setForce (QCS.cc:116-380), corner k at
+    // point k; side k is finished once corner k + 1 is known
     double zux = __dadd_rn(0.0, u0[0].x * rn), zuy = __dadd_rn(0.0, u0[0].y * rn);
 #pragma unroll
     for (int k = 1; k < N; ++k) {
@@ -201,102 +327,31 @@ __device__ __forceinline__ void pass_a_zone_thread(const DevArrays& a, const Hyd
         zuy = zuy + u0[k].y * rn;
     }
     const double2 zuc = mk(zux, zuy);
-    double2 ex[N];
-#pragma unroll
-    for (int k = 0; k < N; ++k) ex[k] = smul(0.5, add(xp[k], xp[(k + 1 == N) ? 0 : k + 1]));
-    double cw[N], cc[N];
-    double2 cqe1[N], cqe2[N];
+    double2 B0 = mk(0., 0.), Aprev = mk(0., 0.), ftot0 = mk(0., 0.), fprev = mk(0., 0.);
+    // side j's sfq from fs = A_j + B_(j+1): sftot, ftot, and the corner force
+    // ftot[j] - ftot[j-1] (Hydro.cc:1159-1193; side 0's after the loop)
+    auto finish_side = [&](int j, double2 fs) {
+        const double2 sfq = mk(fs.x * rinv[j], fs.y * rinv[j]);
+        const double2 sfpq = add(sfp[j], sfq);
+        const double2 ftot = add(sfpq, sft[j]);
+        a.sftot[s0 + j] = sfpq;
+        if (j == 0) ftot0 = ftot;
+        else a.cforce[s0 + j] = sub(ftot, fprev);
+        fprev = ftot;
+    };
 #pragma unroll
     for (int k = 0; k < N; ++k) {
         const int pk = (k == 0) ? N - 1 : k - 1;
         const int nk = (k + 1 == N) ? 0 : k + 1;
-        const double2 up0 = u0[k], xq0 = xp[k];
-        const double2 upp = u0[pk];
-        const double2 up1 = smul(0.5, add(up0, u0[nk]));
-        const double2 xq1 = ex[k];
-        const double2 up2 = zuc, xq2 = zxp;
-        const double2 up3 = smul(0.5, add(upp, up0));
-        const double2 xq3 = ex[pk];
-        const double cvolume = 0.5 * cross(sub(xq2, xq0), sub(xq3, xq1));
-        const double2 v1 = sub(xq3, xq0);
-        const double2 v2 = sub(xq1, xq0);
-        const double de1 = elen[pk], de2 = elen[k];
-        const double minelen = dmin(de1, de2);
-        double ccos = ((minelen < 1.e-12) ? 0. : 4. * dot(v1, v2) / (de1 * de2));
-        const double cdiv = (cross(sub(up2, up0), sub(xq3, xq1)) - cross(sub(up3, up1), sub(xq2, xq0))) /
-                            (2.0 * cvolume);
-        double evol = 0., du = 0.;
-        if (cdiv < 0.0) {
-            const double2 dxx1 = smul(0.5, sub(sub(add(xq1, xq2), xq0), xq3));
-            const double2 dxx2 = smul(0.5, sub(sub(add(xq2, xq3), xq0), xq1));
-            const double dx1 = length(dxx1);
-            const double dx2 = length(dxx2);
-            const double2 duav = smul(0.25, add(add(add(up0, up1), up2), up3));
-            const double test1 = fabs(dot(dxx1, duav) * dx2);
-            const double test2 = fabs(dot(dxx2, duav) * dx1);
-            const double num = (test1 > test2 ? dx1 : dx2);
-            const double den = (test1 > test2 ? dx2 : dx1);
-            const double r = num / den;
-            evol = sqrt(4.0 * cvolume * r);
-            evol = dmin(evol, 2.0 * minelen);
-            const double dv1 = length2(sub(sub(add(up1, up2), up0), up3));
-            const double dv2 = length2(sub(sub(add(up2, up3), up0), up1));
-            du = sqrt(dmax(dv1, dv2));
-        }
-        double crmu = 0.;
-        if (!(cdiv > 0.0)) {
-            const double ztmp2 = c.q2 * 0.25 * c.gammap1 * du;
-            const double ztmp1 = c.q1 * zss;
-            const double zkur = ztmp2 + sqrt(ztmp2 * ztmp2 + ztmp1 * ztmp1);
-            crmu = zkur * zrp * evol;
-        }
-        const double2 t1 = smul(crmu, sub(up0, upp));
-        cqe1[k] = mk(t1.x * rinv[pk], t1.y * rinv[pk]);   // / elen[s]
-        const double2 t2 = smul(crmu, sub(u0[nk], up0));
-        cqe2[k] = mk(t2.x * rinv[k], t2.y * rinv[k]);     // / elen[s2]
-        // QCS::setForce (QCS.cc:331-380) corner weights
-        const double csin2 = 1.0 - ccos * ccos;
-        cw[k] = ((csin2 < 1.e-4) ? 0. : cvolume / csin2);
-        cc[k] = ((csin2 < 1.e-4) ? 0. : ccos);
+        double2 A, B;
+        qcs_corner(c, u0[k], u0[pk], u0[nk], xp[k], ex[k], ex[pk], zxp, zuc, elen[pk], elen[k], rinv[pk], rinv[k],
+                   zss, zrp, A, B);
+        if (k == 0) B0 = B;
+        else finish_side(k - 1, add(Aprev, B));
+        Aprev = A;
     }
-    // side forces: PolyGas::calcForce (PolyGas.cc:164-184), TTS::calcForce
-    // (TTS.cc:55-104), QCS sfq, and the side part of sumCrnrForce
-    // (Hydro.cc:1159-1193)
-    double sstmp = dmax(zss, c.tts_ssmin);
-    sstmp = c.alfa * sstmp * sstmp;
-    double2 ftot[N];
-#pragma unroll
-    for (int k = 0; k < N; ++k) {
-        const int nk = (k + 1 == N) ? 0 : k + 1;
-        const double2 ssurf = rotateCCW(sub(ex[k], zxp));
-        const double2 sfp = smul(-zp, ssurf);
-        const double vfacinv = zareap / sa[k];
-        const double srho = zrp * mf[k] * vfacinv;
-        const double sdp = sstmp * (srho - zrp);
-        const double2 sft = smul(-sdp, ssurf);
-        const double2 fs = add(smul(cw[k], add(cqe2[k], smul(cc[k], cqe1[k]))),
-                               smul(cw[nk], add(cqe1[nk], smul(cc[nk], cqe2[nk]))));
-        const double2 sfq = mk(fs.x * rinv[k], fs.y * rinv[k]);
-        const double2 sfpq = add(sfp, sfq);
-        ftot[k] = add(sfpq, sft);
-        a.sftot[s0 + k] = sfpq;
-    }
-#pragma unroll
-    for (int k = 0; k < N; ++k) a.cforce[s0 + k] = sub(ftot[k], ftot[(k == 0) ? N - 1 : k - 1]);
-    // QCS::setVelDiff (QCS.cc:384-448) and calcDtNew (Hydro.cc:1591-1619)
-    double ztmp = 0.;
-#pragma unroll
-    for (int k = 0; k < N; ++k) {
-        const int nk = (k + 1 == N) ? 0 : k + 1;
-        const double2 dxs = sub(xp[nk], xp[k]);
-        const double2 dus = sub(u0[nk], u0[k]);
-        double dux = dot(dus, dxs);
-        dux = (elen[k] > 0. ? fabs(dux) / elen[k] : 0.);
-        ztmp = dmax(ztmp, dux);
-    }
-    const double zdu = c.q1 * zss + 2. * c.q2 * ztmp;
-    const double cdu = dmax(zdu, dmax(zss, 1.e-99));
-    zdthyd = zdl * c.cfl / cdu;
+    finish_side(N - 1, add(Aprev, B0));
+    a.cforce[s0] = sub(ftot0, fprev);
 }
 
 // ---------------------------------------------------------------------

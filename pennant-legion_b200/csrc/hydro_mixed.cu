@@ -34,6 +34,10 @@
 
 #include <cuda_runtime.h>
 
+#ifndef PNT_PF_WAVES
+#define PNT_PF_WAVES 0
+#endif
+
 namespace pnt {
 namespace {
 
@@ -471,6 +475,16 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_MIXED_ZT_MIN_BLOCKS) pass_
     __shared__ double2 s_sfp[4 * kZoneThreadsZT];
     __shared__ float2 s_sft[4 * kZoneThreadsZT];
     const SideSpill sp{s_sfp, s_sft, (int)threadIdx.x};
+#if PNT_PF_WAVES
+    if (kQuads) {
+        // warm L2 for the block that runs PNT_PF_WAVES resident waves later
+        const int64_t zf0 = ((int64_t)blockIdx.x + (int64_t)PNT_PF_WAVES * 148 * PNT_MIXED_ZT_MIN_BLOCKS) * kZoneThreadsZT;
+        const int64_t zf = zf0 + threadIdx.x;
+        const bool ok = zf < a.numz;
+        const int4 pf = ok ? __ldg(reinterpret_cast<const int4*>(a.mapsp1) + zf) : make_int4(0, 0, 0, 0);
+        tiles::prefetch_zone_block(a, ctl->cycle & 1, zf0, pf, ok);
+    }
+#endif
     if (z < a.numz) {
         const int cur = ctl->cycle & 1;
         const double dt = ctl->dt;
@@ -684,7 +698,7 @@ __global__ void __launch_bounds__(kMlpRows, PNT_CLOSURE_MIN_BLOCKS) closure_pass
             a.sftot[sd] = mk(sf.x + (double)ds.x, sf.y + (double)ds.y);
         }
     }
-    const bool ok = closure_mlp_teardown(st);
+    const bool ok = closure_mlp_teardown(smem, st);
     if (threadIdx.x == 0 && !ok) atomicAdd(a.closure_counts + kClassErr * 64, 1ull);
     if (threadIdx.x < 3 && ccount[threadIdx.x]) {
         const int q = threadIdx.x == 0 ? kClassMlp : (threadIdx.x == 1 ? kClassFallback : kClassOod);

@@ -8,6 +8,7 @@
 #include "pennant_b200.h"
 #include "pnt_internal.h"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -159,7 +160,11 @@ extern "C" pnt_status pnt_op_calc_dt(const double* zdl, const double* zdu, const
 // streams, or different host threads on one device) race on it and must be
 // serialised by the caller.  The first call on each device looks up the
 // array's device address (cudaGetSymbolAddress); make that first call
-// before any stream capture.
+// before any stream capture.  The address is kept per device together with
+// the identity of the device's CUDA context: after cudaDeviceReset (or any
+// other end of the context) the array lives in a new context, and the next
+// call looks the address up again -- make that call before stream capture
+// too.
 // ---------------------------------------------------------------------
 namespace {
 
@@ -171,6 +176,38 @@ static __device__ __align__(256) double g_dt_scratch[2 * kNoAllocMaxBlocks];
 
 std::mutex g_scratch_mu;
 void* g_scratch_addr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};
+
+// The unique id of the calling thread's current CUDA context (cuCtxGetId,
+// reached through the runtime's driver entry-point query, so the library
+// needs no link to libcuda), or 0 when it cannot be had.  Called with
+// g_scratch_mu held.
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        looked_up = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        cudaGetLastError();
+    }
+    if (!get_current || !get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 
 // Device address of g_dt_scratch on the current device.  In host code the
 // symbol name is only a host-side stand-in, never a device address.
@@ -183,7 +220,10 @@ pnt_status noalloc_scratch(double** out) {
     }
     if (dev < 0 || dev >= kMaxDevices) return fail(PNT_ERR_UNSUPPORTED, "device ordinal %d >= %d", dev, kMaxDevices);
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
+    // the runtime makes the device's primary context current at its first
+    // call; the id is taken after cudaGetSymbolAddress on a first look-up
+    unsigned long long ctx = g_scratch_addr[dev] ? current_context_id() : 0;
+    if (!g_scratch_addr[dev] || (ctx != 0 && ctx != g_scratch_ctx[dev])) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_dt_scratch);
         if (e != cudaSuccess || !p) {
@@ -192,6 +232,7 @@ pnt_status noalloc_scratch(double** out) {
                         cudaGetErrorString(e));
         }
         g_scratch_addr[dev] = p;
+        g_scratch_ctx[dev] = current_context_id();
     }
     *out = static_cast<double*>(g_scratch_addr[dev]);
     return PNT_OK;

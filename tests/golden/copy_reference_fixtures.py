@@ -4,7 +4,9 @@ Source: StanfordLegion/pennant-legion test/ (decks of every problem and the
 one known-answer output set, test/sedov/sedov.{xy,geo,zr,ze,zp}).  The files
 are copied byte for byte; the test suite reads only these copies.
 
-Usage: python tests/golden/copy_reference_fixtures.py [reference_root]
+Usage: python tests/golden/copy_reference_fixtures.py REFERENCE_ROOT
+
+(REFERENCE_ROOT is the checked-out StanfordLegion/pennant-legion tree.)
 """
 import os
 import shutil
@@ -24,4 +26,6 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(__doc__)
+    main(sys.argv[1])

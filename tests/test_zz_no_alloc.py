@@ -10,6 +10,8 @@ bit -- including on back-to-back calls, since every call reuses that array.
 
 This file is named to be collected last.
 """
+import ctypes
+
 import numpy as np
 import pytest
 import torch
@@ -57,3 +59,36 @@ def test_noalloc_rejects_sizes_beyond_its_limit():
                                        out.data_ptr(), None)
     assert st == pb.PNT_ERR_INVALID_ARG
     assert b"no-allocation limit" in pb.lib.pnt_last_error()
+
+
+def test_noalloc_takes_nothing_from_the_device_memory_pool():
+    """The allocating entry point takes its partials from the device's default
+    stream-ordered pool (cudaMallocAsync); the no-allocation one must leave
+    the pool's high-water mark where it was.  Inputs and outputs are
+    allocated before the mark is reset."""
+    rt = ctypes.CDLL("libcudart.so.12")   # the runtime torch has loaded
+    used_mem_high = ctypes.c_int(8)       # cudaMemPoolAttrUsedMemHigh
+    pool = ctypes.c_void_p()
+    assert rt.cudaDeviceGetDefaultMemPool(ctypes.byref(pool), ctypes.c_int(torch.cuda.current_device())) == 0
+
+    def high():
+        v = ctypes.c_uint64(0)
+        assert rt.cudaMemPoolGetAttribute(pool, used_mem_high, ctypes.byref(v)) == 0
+        return v.value
+
+    dev = _inputs(3_000_017, 4)
+    out = torch.zeros(3, dtype=torch.float64, device="cuda")
+    args = [t.data_ptr() for t in dev] + [dev[0].numel(), 0.6, 0.1, 2e-3, out.data_ptr(),
+                                          torch.cuda.current_stream().cuda_stream]
+    torch.cuda.synchronize()
+    zero = ctypes.c_uint64(0)
+    assert rt.cudaMemPoolSetAttribute(pool, used_mem_high, ctypes.byref(zero)) == 0
+    before = high()
+    for _ in range(2):
+        pb.check(pb.lib.pnt_op_calc_dt_noalloc(*args))
+    torch.cuda.synchronize()
+    assert high() == before
+    # the control: the allocating entry point does move the mark
+    pb.check(pb.lib.pnt_op_calc_dt(*args))
+    torch.cuda.synchronize()
+    assert high() > before
