@@ -2,27 +2,28 @@
 """Benchmark of the hydro cycle: zone-cycles/s on the 1920^2 Sedov deck.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--precision learned|mixed|fp64] [--full-run]
+                  [--precision learned|mixed|fp64] [--no-full-run]
 
 A step is one hydro cycle (Hydro::doCycle plus the Driver's dt update) over
 the whole mesh.  Every path is timed from the same state: the plain FP64
-cycle run to cycle --start-cycles (30000, t ~ 0.06: a developed blast whose
-shock spans the mesh; the first cycles of the deck have almost no
-compressing corners and would flatter the learned closure) and copied into
-each path's object.  `value` is device-timed throughput with the state
-resident in HBM (CUDA events on the library's stream around K
-graph-replayed cycles, barrier + synchronize on both sides, max over
-ranks).  With N > 1 (torchrun, one rank per GPU) each rank runs an
-independent replica (the single-mesh path has no multi-GPU decomposition):
-scaling is weak.
+cycle run from the deck's initial state to cycle --start-cycles (30000,
+t ~ 0.197: a developed blast whose shock has crossed a third of the mesh;
+the first cycles of the deck have almost no compressing corners and would
+flatter the learned closure) and copied into each path's object.  `value`
+is device-timed throughput with the state resident in HBM (CUDA events on
+the library's stream around K graph-replayed cycles, barrier + synchronize
+on both sides, max over ranks).  With N > 1 (torchrun, one rank per GPU)
+each rank runs an independent replica (weak scaling).
 
 The headline path is the learned cycle: the mixed-precision cycle (FP32
 side geometry, TTS and QCS forces; FP64 point kinematics, volumes, EOS,
 work and dt) with the learned closure in place of QCS on its corners.  The
-plain FP64 cycle and the mixed cycle with the plain QCS are timed beside it,
-and the headline path's relative L1 errors against the FP64 cycle are
-reported after the timed window and over whole runs to t = 1 (480^2 by
-default; 1920^2 as well with --full-run).
+plain FP64 cycle and the mixed cycle with the plain QCS are timed beside it.
+The metric's accuracy condition is measured in the same run: after the
+timed windows the FP64 run continues to t = 1, the learned and mixed cycles
+run the deck from its initial state to t = 1, and the line's `accuracy`
+holds their relative L1 errors in density, energy and speed against the
+FP64 run, with the closure's fallback fraction (--no-full-run skips this).
 
 `e2e` runs the same K cycles through the C ABI from host buffers: state
 uploaded from pinned host memory, one pnt_hydro_cycle call per step (each
@@ -257,8 +258,8 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world,
         "steps": len(times), "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{os.path.basename(args.deck)} ({numz} zones, {o.nums} sides, {o.nump} points)",
-                   "zones": numz, "path": "cpu-openmp-port"},
+        "config": workload_config(args.deck, numz, o.nums, o.nump, world),
+        "details": {"path": "cpu-openmp-port"},
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{len(times)} cycles of {os.path.basename(args.deck)} after {args.warmup} "
                                    f"warm-up cycles; oracle restating the reference's *OMPTask loops "
@@ -267,6 +268,13 @@ def run_reference(args, rank, world):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def workload_config(deck, numz, nums, nump, world):
+    """The `config` object of the line, identical in both arms."""
+    return {"workload": f"{os.path.basename(deck)} ({numz} zones, {nums} sides, {nump} points)",
+            "cycles_per_step": 1, "parallelism": f"replicas x{world}",
+            "l2": "working set > 1 GB per GPU >> 126 MB L2 (no flush needed)"}
 
 
 def l1_rel(a, b):
@@ -405,7 +413,8 @@ def main():
                     help="path of the headline value; the plain FP64 cycle is always timed beside it")
     ap.add_argument("--closure", default=DEFAULT_CLOSURE)
     ap.add_argument("--start-cycles", type=int, default=30000)
-    ap.add_argument("--full-run", action="store_true", help="also run 1920^2 to t = 1 with each path")
+    ap.add_argument("--no-full-run", action="store_true",
+                    help="skip the whole runs of the deck to t = 1 with each path (the accuracy record)")
     ap.add_argument("--no-full-480", action="store_true",
                     help="skip the 480^2 whole runs (short profiling runs)")
     ap.add_argument("--workload", default="sedov1920", choices=["sedov1920", "leblanc", "batch"],
@@ -511,11 +520,13 @@ def main():
             raise SystemExit(f"run stopped early: {s}")
         return max_over_ranks(ms), clocks
 
-    # the common start state: the FP64 cycle to cycle --start-cycles
+    # the common start state: the FP64 cycle to cycle --start-cycles (this
+    # object is the FP64 whole run: it continues to t = 1 after the windows)
     t0 = time.perf_counter()
-    base = make("fp64", cstop=args.start_cycles)
-    s0 = base.run()
-    start = {"cycle": s0["cycle"], "time": s0["time"], "setup_s": time.perf_counter() - t0,
+    base = make("fp64")
+    s0 = base.run(max_cycles=args.start_cycles)
+    t_base = time.perf_counter() - t0
+    start = {"cycle": s0["cycle"], "time": s0["time"], "setup_s": t_base,
              "note": "plain FP64 run from the deck's initial state, copied into every timed path"}
 
     order = [args.precision] + [p for p in ("fp64", "mixed") if p != args.precision]
@@ -529,38 +540,95 @@ def main():
         kms = h.time_kernels(10)
         res[p] = {"ms": ms, "clocks": clocks, "kernel_ms": kms, "counts": cnt,
                   "value": world * numz * args.steps / (ms / 1e3)}
-    base.close()
     head = heads[args.precision]
     window_err = {p: errors(heads[p], heads["fp64"]) for p in order if p != "fp64"}
     for p in order:
         if p != args.precision:
             heads[p].close()
 
-    # whole runs to t = 1 against the FP64 cycle: 480^2 always, 1920^2 with --full-run
-    def full_run(n):
-        text = sedov(n, tstop=1.0)
-        ref = make("fp64", text=text)
+    # end to end through the C ABI with pinned host buffers
+    fields = ["px", "pu", "zr", "ze", "zm", "zetot", "zwrate", "zvol"]
+    host = {}
+    for k in fields:
+        arr = head.download(k)
+        pin = torch.empty(arr.shape, dtype=torch.float64, pin_memory=True).numpy()
+        pin[...] = arr
+        host[k] = pin
+    outs = {k: torch.empty(head._shape(k), dtype=torch.float64, pin_memory=True).numpy()
+            for k in ("zr", "ze", "zp", "px", "pu")}
+    barrier_sync()
+    t0 = time.perf_counter()
+    for k in fields:
+        pb.check(pb.lib.pnt_hydro_upload(head.h, pb.FIELDS[k], host[k].ctypes.data, host[k].nbytes))
+    for _ in range(args.steps):
+        head.cycle()
+    for k, arr in outs.items():
+        pb.check(pb.lib.pnt_hydro_download(head.h, pb.FIELDS[k], arr.ctypes.data, arr.nbytes))
+    barrier_sync()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    h2d = sum(a.nbytes for a in host.values())
+    d2h = sum(a.nbytes for a in outs.values()) + 72 * args.steps
+    head.close()
+
+    def whole_run(p, text=None):
+        h = make(p, text=text)
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        ref.run()
-        out = {"fp64": {"wall_s": time.perf_counter() - t1, "cycles": ref.scalars()["cycle"]}}
+        h.run()
+        return h, time.perf_counter() - t1
+
+    def compare(p, h, ref, wall):
+        out = {"wall_s": wall, "cycles": h.scalars()["cycle"], "time": h.scalars()["time"],
+               "l1_rel_err_vs_fp64": errors(h, ref)}
+        if p == "learned":
+            c = h.closure_counts()
+            out["corner_fractions"] = fractions(c)
+            out["fallback_fraction"] = (c["fallback"] + c["ood"]) / max(c["mlp"] + c["fallback"] + c["ood"], 1)
+            out["wait_timeouts"] = c["error"]
+        return out
+
+    # whole runs to t = 1 against the FP64 cycle: 480^2, and the metric's
+    # 1920^2 (the FP64 one continues the start-state run)
+    def full_run_480():
+        text = sedov(480, tstop=1.0)
+        ref, wall = whole_run("fp64", text)
+        out = {"fp64": {"wall_s": wall, "cycles": ref.scalars()["cycle"]}}
         for p in order:
-            if p == "fp64":
-                continue
-            h = make(p, text=text)
-            torch.cuda.synchronize()
-            t1 = time.perf_counter()
-            h.run()
-            out[p] = {"wall_s": time.perf_counter() - t1, "l1_rel_err_vs_fp64": errors(h, ref)}
-            if p == "learned":
-                out[p]["corner_fractions"] = fractions(h.closure_counts())
-            h.close()
+            if p != "fp64":
+                h, wall = whole_run(p, text)
+                out[p] = compare(p, h, ref, wall)
+                h.close()
         ref.close()
         return out
 
-    full = {} if args.no_full_480 else {"480": full_run(480)}
-    if args.full_run:
-        full["1920"] = full_run(1920)
+    full = {} if args.no_full_480 else {"480": full_run_480()}
+    accuracy = None
+    if not args.no_full_run:
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        base.run()
+        wall = t_base + time.perf_counter() - t1
+        f1920 = {"fp64": {"wall_s": wall, "cycles": base.scalars()["cycle"], "time": base.scalars()["time"],
+                          "value": numz * base.scalars()["cycle"] / wall}}
+        for p in order:
+            if p != "fp64":
+                h, wall = whole_run(p)
+                f1920[p] = compare(p, h, base, wall)
+                f1920[p]["value"] = numz * f1920[p]["cycles"] / wall
+                h.close()
+        full["1920"] = f1920
+        hp = f1920[args.precision] if args.precision != "fp64" else None
+        if hp:
+            err = hp["l1_rel_err_vs_fp64"]
+            accuracy = {"mesh": f"{os.path.basename(args.deck)} to t = {hp['time']:.6g} from its initial state",
+                        "l1_rel_err_vs_fp64": {"rho": err["zr"], "e": err["ze"], "u": err["u"]},
+                        "bound": 1e-3, "within_bound": max(err["zr"], err["ze"], err["u"]) <= 1e-3,
+                        "cycles": hp["cycles"], "cycles_fp64": f1920["fp64"]["cycles"],
+                        "whole_run_speedup_vs_fp64": f1920["fp64"]["wall_s"] / hp["wall_s"]}
+            if "fallback_fraction" in hp:
+                accuracy["fallback_fraction"] = hp["fallback_fraction"]
+                accuracy["wait_timeouts"] = hp["wait_timeouts"]
+    base.close()
 
     hbm, peak_kind = measured_peaks()
     names = ["A", "B", "C", "end_of_cycle", "closure"]   # the order of pnt_hydro_time_kernels
@@ -599,30 +667,6 @@ def main():
             "tensor_tflops": (4 * zones_per_cycle * MLP_FLOP_PER_ROW) / (cl_ms / 1e3) / 1e12 if cl_ms > 0 else None,
             "wait_timeouts": cnt["error"], "weights": os.path.relpath(args.closure, ROOT)}
 
-    # end to end through the C ABI with pinned host buffers
-    fields = ["px", "pu", "zr", "ze", "zm", "zetot", "zwrate", "zvol"]
-    host = {}
-    for k in fields:
-        arr = head.download(k)
-        pin = torch.empty(arr.shape, dtype=torch.float64, pin_memory=True).numpy()
-        pin[...] = arr
-        host[k] = pin
-    outs = {k: torch.empty(head._shape(k), dtype=torch.float64, pin_memory=True).numpy()
-            for k in ("zr", "ze", "zp", "px", "pu")}
-    barrier_sync()
-    t0 = time.perf_counter()
-    for k in fields:
-        pb.check(pb.lib.pnt_hydro_upload(head.h, pb.FIELDS[k], host[k].ctypes.data, host[k].nbytes))
-    for _ in range(args.steps):
-        head.cycle()
-    for k, arr in outs.items():
-        pb.check(pb.lib.pnt_hydro_download(head.h, pb.FIELDS[k], arr.ctypes.data, arr.nbytes))
-    barrier_sync()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
-    h2d = sum(a.nbytes for a in host.values())
-    d2h = sum(a.nbytes for a in outs.values()) + 72 * args.steps
-    head.close()
-
     result = None
     if rank == 0:
         paths = {
@@ -643,15 +687,13 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": {"learned": "bf16+f32+f64", "mixed": "f32+f64", "fp64": "f64"}[args.precision],
             "data": "synthetic",
-            "config": {"workload": f"{os.path.basename(args.deck)} ({numz} zones, {nums} sides, {nump} points)",
-                       "path": paths[args.precision], "cycles_per_step": 1, "parallelism": f"replicas x{world}",
-                       "start_state": start,
-                       "l2": "working set > 1 GB per GPU >> 126 MB L2 (no flush needed)",
-                       "others": others,
-                       "speedup_vs_fp64": res[args.precision]["value"] / res["fp64"]["value"],
-                       "l1_rel_err_vs_fp64_window": window_err,
-                       "full_runs_to_t1": full,
-                       "closure": closure_info},
+            "config": workload_config(args.deck, numz, nums, nump, world),
+            "accuracy": accuracy,
+            "details": {"path": paths[args.precision], "start_state": start, "others": others,
+                        "speedup_vs_fp64": res[args.precision]["value"] / res["fp64"]["value"],
+                        "l1_rel_err_vs_fp64_window": window_err,
+                        "full_runs_to_t1": full,
+                        "closure": closure_info},
             "roofline": {"bound": "hbm", "kernel": f"pass {names[dom]} ({args.precision})", "achieved": ach_dom,
                          "peak": hbm, "unit": "GB/s", "frac": ach_dom / hbm, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": per_launch[names[dom]], "launch_ms": kms_head[dom],

@@ -40,10 +40,6 @@
 #include <algorithm>
 #include "zone_tiles.cuh"
 
-#ifndef PNT_PF_WAVES
-#define PNT_PF_WAVES 0
-#endif
-
 namespace pnt {
 namespace {
 
@@ -61,16 +57,6 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_PASS_A_ZT_MIN_BLOCKS) pass
     const int64_t z = (int64_t)blockIdx.x * kZoneThreadsZT + threadIdx.x;
     double zdthyd = 1.e99;
     int bad = 0;
-#if PNT_PF_WAVES
-    if (kQuads) {
-        // warm L2 for the block that runs PNT_PF_WAVES resident waves later
-        const int64_t zf0 = ((int64_t)blockIdx.x + (int64_t)PNT_PF_WAVES * 148 * PNT_PASS_A_ZT_MIN_BLOCKS) * kZoneThreadsZT;
-        const int64_t zf = zf0 + threadIdx.x;
-        const bool ok = zf < a.numz;
-        const int4 pf = ok ? __ldg(reinterpret_cast<const int4*>(a.mapsp1) + zf) : make_int4(0, 0, 0, 0);
-        tiles::prefetch_zone_block(a, ctl->cycle & 1, zf0, pf, ok);
-    }
-#endif
     if (z < a.numz) {
         const int cur = ctl->cycle & 1;
         const double dt = ctl->dt;

@@ -34,10 +34,6 @@
 
 #include <cuda_runtime.h>
 
-#ifndef PNT_PF_WAVES
-#define PNT_PF_WAVES 0
-#endif
-
 namespace pnt {
 namespace {
 
@@ -475,16 +471,6 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_MIXED_ZT_MIN_BLOCKS) pass_
     __shared__ double2 s_sfp[4 * kZoneThreadsZT];
     __shared__ float2 s_sft[4 * kZoneThreadsZT];
     const SideSpill sp{s_sfp, s_sft, (int)threadIdx.x};
-#if PNT_PF_WAVES
-    if (kQuads) {
-        // warm L2 for the block that runs PNT_PF_WAVES resident waves later
-        const int64_t zf0 = ((int64_t)blockIdx.x + (int64_t)PNT_PF_WAVES * 148 * PNT_MIXED_ZT_MIN_BLOCKS) * kZoneThreadsZT;
-        const int64_t zf = zf0 + threadIdx.x;
-        const bool ok = zf < a.numz;
-        const int4 pf = ok ? __ldg(reinterpret_cast<const int4*>(a.mapsp1) + zf) : make_int4(0, 0, 0, 0);
-        tiles::prefetch_zone_block(a, ctl->cycle & 1, zf0, pf, ok);
-    }
-#endif
     if (z < a.numz) {
         const int cur = ctl->cycle & 1;
         const double dt = ctl->dt;

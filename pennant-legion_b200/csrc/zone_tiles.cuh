@@ -136,41 +136,6 @@ inline cudaError_t prepare(K k, int threads, int smem_bytes, int32_t numz, int n
     return cudaSuccess;
 }
 
-// L2 warm-up of a later zone's pass A inputs (quad meshes): the zone's four
-// points (position and velocity of the current buffer), and, one line per
-// thread for the first 72 threads, the 128 B lines of the zone fields and
-// side mass fractions of the 128-zone block starting at zf0.  Fire and
-// forget: prefetches hold no registers and fault on no address (every
-// address here is in its array).
-__device__ __forceinline__ void prefetch_l2(const void* p) {
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-}
-__device__ __forceinline__ void prefetch_zone_block(const DevArrays& a, int cur, int64_t zf0, int4 pf, bool pf_ok) {
-    if (pf_ok) {
-        prefetch_l2(a.px[cur] + pf.x);
-        prefetch_l2(a.px[cur] + pf.y);
-        prefetch_l2(a.px[cur] + pf.z);
-        prefetch_l2(a.px[cur] + pf.w);
-        prefetch_l2(a.pu[cur] + pf.x);
-        prefetch_l2(a.pu[cur] + pf.y);
-        prefetch_l2(a.pu[cur] + pf.z);
-        prefetch_l2(a.pu[cur] + pf.w);
-    }
-    const int t = threadIdx.x;
-    const int64_t nz = a.numz;
-    if (t < 40) {
-        const int64_t z = zf0 + 16 * (t & 7);
-        if (z < nz) {
-            const int f = t >> 3;
-            const double* arr = f == 0 ? a.zm : f == 1 ? a.zr : f == 2 ? a.ze : f == 3 ? a.zwrate : a.zvol;
-            prefetch_l2(arr + z);
-        }
-    } else if (t < 72) {
-        const int64_t z = zf0 + 4 * (t - 40);
-        if (z < nz) prefetch_l2(a.smf + 4 * z);
-    }
-}
-
 // Block sum of a per-thread count (called by every thread of the block).
 template <int kThreads>
 __device__ __forceinline__ int block_isum(int v) {

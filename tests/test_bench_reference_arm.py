@@ -31,6 +31,8 @@ def test_reference_arm_prints_one_contract_line():
     assert d["higher_is_better"] is True and d["n_gpus"] == 1 and d["steps"] == 1 and d["warmup"] == 3
     assert d["value"] > 0 and d["ms_per_step"] > 0
     assert d["config"]["workload"].startswith("sedov1920.pnt (3686400 zones")
+    # the same config object as the GPU arm's line
+    assert d["config"] == bench.workload_config(bench.DEFAULT_DECK, 3686400, 14745600, 3690241, 1)
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"]
     e = d["e2e"]
