@@ -203,6 +203,26 @@ pnt_status generate_mesh(const Deck& d, Mesh& m) {
 // ---------------------------------------------------------------------
 // Mesh::init derived data (Mesh.cc:610-623) and validation.
 // ---------------------------------------------------------------------
+
+// The zones-per-row count nzx when the mesh is numbered as genPointsRect /
+// genZonesRect / genSidesRect number a rect mesh (GenMesh.cc:790-829,
+// 898-930, 987-1100: zones row-major, points nzx + 1 a row, side 4z + k of
+// zone (i, j) starting at point (i, j), (i+1, j), (i+1, j+1), (i, j+1)),
+// else 0.  The row-tile passes (row_tiles.cuh) rely on exactly this.
+int32_t rect_columns(const Mesh& m, bool quads) {
+    if (!quads || m.npieces != 1 || m.numz < 1) return 0;
+    const int64_t npx = m.mapsp1[3];   // zone 0's left side starts at point (0, 1)
+    const int64_t nzx = npx - 1, nz = m.numz;
+    if (nzx < 1 || nz % nzx != 0 || (int64_t)m.nump != (nz / nzx + 1) * npx) return 0;
+    static const int di[4] = {0, 1, 1, 0}, dj[4] = {0, 0, 1, 1};
+    for (int64_t z = 0; z < nz; ++z) {
+        const int64_t zi = z % nzx, zj = z / nzx;
+        for (int k = 0; k < 4; ++k)
+            if (m.mapsp1[4 * z + k] != (zj + dj[k]) * npx + zi + di[k]) return 0;
+    }
+    return (int32_t)nzx;
+}
+
 pnt_status finish_mesh(Mesh& m) {
     const int64_t np = m.nump, nz = m.numz, ns = m.nums;
     if (np <= 0 || nz <= 0 || ns <= 0) return fail(PNT_ERR_INVALID_ARG, "empty mesh");
@@ -238,6 +258,7 @@ pnt_status finish_mesh(Mesh& m) {
         if (m.mapsp2[t] != m.mapsp1[m.mapss4[t]])
             return fail(PNT_ERR_INVALID_ARG, "mapsp2[%lld] != mapsp1[mapss4[%lld]]", (long long)t, (long long)t);
     m.all_quads = quads;
+    m.rect_nzx = rect_columns(m, quads);
 
     // Point -> corner CSR, ascending side order inside each point.
     m.poff.assign(np + 1, 0);

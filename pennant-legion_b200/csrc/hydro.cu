@@ -298,6 +298,7 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
     a.numz = (int32_t)nz;
     a.nums = (int32_t)ns;
     a.quads = m.all_quads ? 1 : 0;
+    a.rect_nzx = m.rect_nzx;
     int32_t *zfirst = nullptr, *znump = nullptr, *mapsp1 = nullptr, *poff = nullptr, *pcorner = nullptr;
     double* smf = nullptr;
     uint16_t* mask = nullptr;
@@ -305,18 +306,22 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
     {
         int nsm = 148;
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
-        const cudaError_t e = prepare_pass_c(p.precision != PNT_PREC_FP64, a.quads != 0, a.numz, nsm, &a.gridC);
+        cudaError_t e = prepare_pass_c(p.precision != PNT_PREC_FP64, a.quads != 0, a.rect_nzx, a.numz, nsm, &a.gridC);
         if (e != cudaSuccess) return fail(PNT_ERR_CUDA, "pass C setup: %s", cudaGetErrorString(e));
+        if (a.rect_nzx > 0 && p.precision != PNT_PREC_FP64) {
+            e = prepare_pass_a_rows_mixed(p.precision == PNT_PREC_LEARNED, a.rect_nzx, a.numz, nsm, &a.gridA);
+            if (e != cudaSuccess) return fail(PNT_ERR_CUDA, "pass A setup: %s", cudaGetErrorString(e));
+        }
     }
     pnt_status st = PNT_OK;
     if ((st = h->alloc(&zfirst, nz)) || (st = h->alloc(&znump, nz)) || (st = h->alloc(&mapsp1, ns)) ||
         (st = h->alloc(&smf, ns)) || (st = h->alloc(&poff, np + 1)) || (st = h->alloc(&pcorner, m.pcorner.size())) ||
         (st = h->alloc(&mask, np + 2)) || (st = h->alloc(&a.px[0], np)) || (st = h->alloc(&a.px[1], np)) ||
-        (st = h->alloc(&a.pu[0], np)) || (st = h->alloc(&a.pu[1], np)) || (st = h->alloc(&a.zm, nz)) ||
-        (st = h->alloc(&a.zr, nz)) || (st = h->alloc(&a.ze, nz)) || (st = h->alloc(&a.zetot, nz)) ||
-        (st = h->alloc(&a.zwrate, nz)) || (st = h->alloc(&a.zvol, nz)) || (st = h->alloc(&a.zp, nz)) ||
+        (st = h->alloc(&a.pu[0], np)) || (st = h->alloc(&a.pu[1], np)) || (st = h->alloc(&a.zm, nz + 2)) ||
+        (st = h->alloc(&a.zr, nz + 2)) || (st = h->alloc(&a.ze, nz + 2)) || (st = h->alloc(&a.zetot, nz + 2)) ||
+        (st = h->alloc(&a.zwrate, nz + 2)) || (st = h->alloc(&a.zvol, nz + 2)) || (st = h->alloc(&a.zp, nz + 2)) ||
         (st = h->alloc(&a.cmass, ns + m.nhalo)) || (st = h->alloc(&a.cforce, ns + m.nhalo)) || (st = h->alloc(&a.sftot, ns)) ||
-        (st = h->alloc(&a.cyc_red, 4)) || (st = h->alloc(&a.fin_ticket, 1)) || (st = h->alloc(&a.ctl, 1)))
+        (st = h->alloc(&a.cyc_red, 5)) || (st = h->alloc(&a.fin_ticket, 1)) || (st = h->alloc(&a.ctl, 1)))
         return st;
     a.cmass_f = reinterpret_cast<float*>(a.cmass);
     a.cforce_f = reinterpret_cast<float2*>(a.cforce);
@@ -360,7 +365,7 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
 
     // the cycle reductions' starting values: minimum from 1e99, maximum
     // from 1e-99 (keys of positive doubles are their bits), no bad sides
-    long long cyc_red_init[4] = {0, 0, 0, 0};
+    long long cyc_red_init[5] = {0, 0, 0, 0, 0};
     {
         const double lo = 1.e99, hi = 1.e-99;
         std::memcpy(&cyc_red_init[0], &lo, 8);
@@ -465,6 +470,16 @@ pnt_status pnt_hydro_create(const pnt_mesh* mesh, const pnt_params* params, int3
 
 void pnt_hydro_destroy(pnt_hydro* h) { delete h; }
 
+namespace {
+// The status of a run the device ended: inverted sides, or a bounded wait
+// of a kernel that ran out.
+pnt_status run_failure(const Ctl& c) {
+    if (c.status == PNT_ERR_TIMEOUT)
+        return fail(PNT_ERR_TIMEOUT, "a bounded device-side wait ran out on cycle %d", c.cycle);
+    return fail(c.status, "%d negative side volumes on cycle %d", c.nbad, c.cycle);
+}
+}  // namespace
+
 pnt_status pnt_hydro_cycle(pnt_hydro* h, pnt_scalars* out) {
     if (!h) return fail(PNT_ERR_INVALID_ARG, "null argument");
     DeviceGuard dg(h->device);
@@ -474,8 +489,7 @@ pnt_status pnt_hydro_cycle(pnt_hydro* h, pnt_scalars* out) {
     st = h->fetch_ctl();
     if (st) return st;
     h->scalars(out);
-    if (h->ctl_host->status) return fail(h->ctl_host->status, "%d negative side volumes on cycle %d",
-                                         h->ctl_host->nbad, h->ctl_host->cycle);
+    if (h->ctl_host->status) return run_failure(*h->ctl_host);
     return PNT_OK;
 }
 
@@ -512,8 +526,7 @@ pnt_status pnt_hydro_run(pnt_hydro* h, int32_t max_cycles, pnt_report_fn report,
     if (!st) st = h->set_stop_at(INT_MAX);
     if (st) return st;
     h->scalars(out);
-    if (h->ctl_host->status) return fail(h->ctl_host->status, "%d negative side volumes on cycle %d",
-                                         h->ctl_host->nbad, h->ctl_host->cycle);
+    if (h->ctl_host->status) return run_failure(*h->ctl_host);
     return PNT_OK;
 }
 

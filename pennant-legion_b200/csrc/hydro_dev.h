@@ -46,6 +46,7 @@ struct HydroConst {
 struct DevArrays {
     int32_t nump, numz, nums;
     int32_t quads;               // all zones are quads at sides 4z..4z+3
+    int32_t rect_nzx;            // > 0: numbered as the rect generator does, nzx zones a row (row_tiles.cuh)
     const int32_t* zfirst;       // [numz]
     const int32_t* znump;        // [numz]
     const int32_t* mapsp1;       // [nums]
@@ -81,7 +82,7 @@ struct DevArrays {
     // and C with atomics ([0] minimum zone dt and [1] maximum |dV/V0| as
     // order-preserving keys (dkey), [2] / [3] inverted sides in A / C), and
     // the ticket that picks pass C's last CTA, which ends the cycle and
-    // resets them
+    // resets them; [4] is set when a bounded wait of a kernel ran out
     long long* cyc_red;
     uint32_t* fin_ticket;
     Ctl* ctl;
@@ -96,6 +97,7 @@ struct DevArrays {
     int32_t* closure_nrec;
     int32_t closure_grid;   // CTAs of the persistent closure pass
     int32_t gridC;          // CTAs of the persistent pass C (pass_c_staged.cuh)
+    int32_t gridA;          // CTAs of the persistent row-tile mixed/learned pass A (rect meshes)
     // multi-piece runs: pass C's last CTA writes this piece's [dtnew,
     // -dvovmax, inverted sides in A, in C] here instead of ending the cycle
     // (nullptr for a single piece)
@@ -148,8 +150,12 @@ cudaError_t prepare_learned_kernels();
 // device and returns its persistent grid (resident CTAs per SM x nsm, at
 // most one per tile); launch_pass_c launches it with a.gridC CTAs, which
 // write a.gridC partials.
-cudaError_t prepare_pass_c(bool mixed, bool quads, int32_t numz, int nsm, int32_t* grid);
+cudaError_t prepare_pass_c(bool mixed, bool quads, int32_t rect_nzx, int32_t numz, int nsm, int32_t* grid);
 void launch_pass_c(const DevArrays& a, const HydroConst& c, bool mixed, cudaStream_t stream);
+// The row-tile pass A of the mixed or learned cycle (hydro_mixed.cu): raises
+// the kernel's shared-memory limit on the current device and returns its
+// persistent grid.
+cudaError_t prepare_pass_a_rows_mixed(bool learned, int32_t rect_nzx, int32_t numz, int nsm, int32_t* grid);
 
 // Device state of a pnt_hydro for the closure harvest (closure.cu).
 struct HydroAccess {

@@ -219,23 +219,39 @@ __device__ __forceinline__ void qcs_corner(const HydroConst& c, double2 up0, dou
 // side is finished as soon as its second corner is known.  nbad counts the
 // zone's inverted sides (checkBadSides counts sides, Mesh.cc:1531-1550).
 // ---------------------------------------------------------------------
-template <int N>
-__device__ __forceinline__ void pass_a_zone_thread(const DevArrays& a, const HydroConst& c, int cur, double dt,
+// Pass A's inputs of one zone gathered from global memory: the position
+// and velocity of each side's first point (current buffer), the side mass
+// fractions and the zone fields.  The row-tile kernels read the same
+// values from shared memory through an accessor of the same shape.
+struct GlobalZoneIn {
+    const DevArrays& a;
+    int cur;
+    int64_t z, s0;
+    __device__ __forceinline__ int32_t p(int k) const { return __ldg(a.mapsp1 + s0 + k); }
+    __device__ __forceinline__ double2 x0(int k) const { return a.px[cur][p(k)]; }
+    __device__ __forceinline__ double2 u0(int k) const { return a.pu[cur][p(k)]; }
+    __device__ __forceinline__ double mf(int k) const { return __ldg(a.smf + s0 + k); }
+    __device__ __forceinline__ double zm() const { return a.zm[z]; }
+    __device__ __forceinline__ double zr() const { return a.zr[z]; }
+    __device__ __forceinline__ double ze() const { return a.ze[z]; }
+    __device__ __forceinline__ double zwrate() const { return a.zwrate[z]; }
+    __device__ __forceinline__ double zvol() const { return a.zvol[z]; }
+};
+
+template <int N, typename In>
+__device__ __forceinline__ void pass_a_zone_thread(const DevArrays& a, const HydroConst& c, const In& in, double dt,
                                                    int64_t z, int64_t s0, double& zdthyd, int& nbad) {
-    const double2* __restrict__ px0 = a.px[cur];
-    const double2* __restrict__ pu0 = a.pu[cur];
     double2 xp[N], u0[N];
     double mf[N];
     const double dth = 0.5 * dt;
 #pragma unroll
     for (int k = 0; k < N; ++k) {
-        const int32_t p = __ldg(a.mapsp1 + s0 + k);
-        const double2 x0 = px0[p];
-        u0[k] = pu0[p];
-        mf[k] = __ldg(a.smf + s0 + k);
+        const double2 x0 = in.x0(k);
+        u0[k] = in.u0(k);
+        mf[k] = in.mf(k);
         xp[k] = add(x0, smul(dth, u0[k]));   // advPosHalf (Hydro.cc:986-1006)
     }
-    const double zm = a.zm[z], zr = a.zr[z], ze = a.ze[z], zwrate = a.zwrate[z], zvol0 = a.zvol[z];
+    const double zm = in.zm(), zr = in.zr(), ze = in.ze(), zwrate = in.zwrate(), zvol0 = in.zvol();
     const double rn = 1. / (double)N;
     // calcCtrs (Mesh.cc:797-837)
     double zx = __dadd_rn(0.0, xp[0].x * rn), zy = __dadd_rn(0.0, xp[0].y * rn);
@@ -354,6 +370,14 @@ __device__ __forceinline__ void pass_a_zone_thread(const DevArrays& a, const Hyd
     a.cforce[s0] = sub(ftot0, fprev);
 }
 
+// The same zone with its inputs gathered from global memory.
+template <int N>
+__device__ __forceinline__ void pass_a_zone_thread(const DevArrays& a, const HydroConst& c, int cur, double dt,
+                                                   int64_t z, int64_t s0, double& zdthyd, int& nbad) {
+    const GlobalZoneIn in{a, cur, z, s0};
+    pass_a_zone_thread<N>(a, c, in, dt, z, s0, zdthyd, nbad);
+}
+
 // ---------------------------------------------------------------------
 // Pass B, one point
 // ---------------------------------------------------------------------
@@ -447,6 +471,11 @@ __device__ __forceinline__ void end_cycle_if_last(const DevArrays& a, const Hydr
     const int badA = (int)atomicExch(r + 2, 0ull);
     const int badC = (int)atomicExch(r + 3, 0ull);
     *a.fin_ticket = 0u;
+    if (!a.piece_red && *(volatile unsigned long long*)(r + 4)) {   // a bounded wait ran out this cycle
+        a.ctl->status = 6;                                           // PNT_ERR_TIMEOUT
+        a.ctl->done = 1;
+        return;
+    }
     if (a.piece_red) {
         a.piece_red[0] = dtn;
         a.piece_red[1] = -dvm;

@@ -30,6 +30,7 @@
 #include "closure_dev.cuh"
 #include "hydro_fp64_body.cuh"
 #include "hydro_dev.h"
+#include "row_tiles.cuh"
 #include "zone_tiles.cuh"
 
 #include <cuda_runtime.h>
@@ -186,12 +187,12 @@ struct SideSpill {
 
 // nbad counts the zone's inverted sides; cnt[3]: its corners without
 // compression, in the dead zone, in an acute zone (learned cycle).
-template <int N, bool kLearned>
-__device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const HydroConst& c, int cur, double dt,
-                                                  int64_t z, int64_t s0, double& zdthyd, int& nbad, int* cnt,
-                                                  const SideSpill& sp) {
-    const double2* __restrict__ px0 = a.px[cur];
-    const double2* __restrict__ pu0 = a.pu[cur];
+// in: the zone's inputs (fp64::GlobalZoneIn, or a row tile's shared-memory
+// stage).
+template <int N, bool kLearned, typename In>
+__device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const HydroConst& c, const In& in, int cur,
+                                                  double dt, int64_t z, int64_t s0, double& zdthyd, int& nbad,
+                                                  int* cnt, const SideSpill& sp) {
     double2 xp[N];
     float2 uf[N];
     double mf[N];
@@ -199,16 +200,15 @@ __device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const Hydr
     double2 uref;
 #pragma unroll
     for (int k = 0; k < N; ++k) {
-        const int32_t p = __ldg(a.mapsp1 + s0 + k);
-        const double2 u0 = pu0[p];
-        xp[k] = add(px0[p], smul(dth, u0));
+        const double2 u0 = in.u0(k);
+        xp[k] = add(in.x0(k), smul(dth, u0));
         if (k == 0) uref = u0;
         // velocities relative to the zone's first point: QCS works on
         // velocity differences, which absolute FP32 values would round away
         uf[k] = f2(sub(u0, uref));
-        mf[k] = __ldg(a.smf + s0 + k);
+        mf[k] = in.mf(k);
     }
-    const double zm = a.zm[z], zr = a.zr[z], ze = a.ze[z], zwrate = a.zwrate[z], zvol0 = a.zvol[z];
+    const double zm = in.zm(), zr = in.zr(), ze = in.ze(), zwrate = in.zwrate(), zvol0 = in.zvol();
     // FP64: positions, zone centre, side areas and volumes
     const double rn = 1. / (double)N;
     double zx = xp[0].x * rn, zy = xp[0].y * rn;
@@ -475,12 +475,14 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_MIXED_ZT_MIN_BLOCKS) pass_
         const int cur = ctl->cycle & 1;
         const double dt = ctl->dt;
         if (kQuads) {
-            pass_a_mixed_zone<4, kLearned>(a, c, cur, dt, z, 4 * z, zdthyd, bad, cnt, sp);
+            const fp64::GlobalZoneIn in{a, cur, z, 4 * z};
+            pass_a_mixed_zone<4, kLearned>(a, c, in, cur, dt, z, 4 * z, zdthyd, bad, cnt, sp);
         } else {
             const int n = a.znump[z];
             const int64_t s0 = a.zfirst[z];
-            if (n == 4) pass_a_mixed_zone<4, kLearned>(a, c, cur, dt, z, s0, zdthyd, bad, cnt, sp);
-            else pass_a_mixed_zone<3, kLearned>(a, c, cur, dt, z, s0, zdthyd, bad, cnt, sp);
+            const fp64::GlobalZoneIn in{a, cur, z, s0};
+            if (n == 4) pass_a_mixed_zone<4, kLearned>(a, c, in, cur, dt, z, s0, zdthyd, bad, cnt, sp);
+            else pass_a_mixed_zone<3, kLearned>(a, c, in, cur, dt, z, s0, zdthyd, bad, cnt, sp);
         }
     }
     __shared__ unsigned wcount[kLearned ? kZoneThreadsZT / 32 : 1][3];
@@ -497,6 +499,74 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_MIXED_ZT_MIN_BLOCKS) pass_
             unsigned t = 0;
             for (int w = 0; w < kZoneThreadsZT / 32; ++w) t += wcount[w][threadIdx.x];
             if (t) atomicAdd(a.closure_counts + kCounted[threadIdx.x] * 64 + (blockIdx.x & 63), (unsigned long long)t);
+        }
+    }
+    fp64::block_to_cycle<true, kZoneThreadsZT>(a.cyc_red, zdthyd, nbad);
+}
+
+// Pass A over row tiles of a rect mesh (row_tiles.cuh): the same zone body
+// reading its inputs from the tile's shared-memory stage, persistent CTAs,
+// two stages.  3 CTAs per SM (168 registers): at 1920^2 Sedov 0.239 ms for
+// the learned cycle against 0.247 ms at 4 CTAs (spills) and 0.258 ms for
+// the gathering kernel; three stages were slower (fewer resident CTAs).
+#ifndef PNT_ROWS_A_STAGES
+#define PNT_ROWS_A_STAGES 2
+#endif
+#ifndef PNT_ROWS_A_MIN_BLOCKS
+#define PNT_ROWS_A_MIN_BLOCKS 3
+#endif
+constexpr int kRowsAStages = PNT_ROWS_A_STAGES;
+using AStage = rows::PassAStage<kZoneThreadsZT>;
+constexpr int kRowsASmem = kRowsAStages * AStage::kBytes;
+
+template <bool kLearned>
+__global__ void __launch_bounds__(kZoneThreadsZT, PNT_ROWS_A_MIN_BLOCKS) pass_a_mixed_rows(DevArrays a,
+                                                                                            HydroConst c) {
+    extern __shared__ __align__(128) unsigned char smem_a[];
+    __shared__ __align__(8) uint64_t bars[kRowsAStages];
+    __shared__ double2 s_sfp[4 * kZoneThreadsZT];
+    __shared__ float2 s_sft[4 * kZoneThreadsZT];
+    const Ctl* ctl = a.ctl;
+    if (skip_cycle(ctl)) return;
+    const int cur = ctl->cycle & 1;
+    const double dt = ctl->dt;
+    const int32_t nzx = a.rect_nzx;
+    const int64_t npx = (int64_t)nzx + 1;
+    const int64_t ntiles = rows::num_tiles<kZoneThreadsZT>(nzx, a.numz);
+    const int t = threadIdx.x;
+    const SideSpill sp{s_sfp, s_sft, t};
+    double zdthyd = 1.e99;
+    int bad = 0;
+    int cnt[3] = {0, 0, 0};
+    auto bytes = [&](int64_t g) { return AStage::bytes(rows::tile_of<kZoneThreadsZT>(g, nzx)); };
+    auto issue = [&](unsigned char* st, int64_t g, uint32_t bar) {
+        AStage::issue(st, a, cur, rows::tile_of<kZoneThreadsZT>(g, nzx), npx, bar);
+    };
+    auto compute = [&](const unsigned char* st, int64_t g) {
+        const rows::Tile tl = rows::tile_of<kZoneThreadsZT>(g, nzx);
+        if (t >= tl.nt) return;
+        const rows::RowZoneIn<kZoneThreadsZT> in{st, t, (int)(tl.z0 & 1)};
+        const int64_t z = tl.z0 + t;
+        double v = 1.e99;
+        pass_a_mixed_zone<4, kLearned>(a, c, in, cur, dt, z, 4 * z, v, bad, cnt, sp);
+        zdthyd = dmin(zdthyd, v);
+    };
+    if (!rows::for_tiles<kRowsAStages, AStage::kBytes>(ntiles, smem_a, bars, bytes, issue, compute) && t == 0)
+        atomicOr(reinterpret_cast<unsigned long long*>(a.cyc_red + 4), 1ull);
+    __shared__ unsigned wcount[kLearned ? kZoneThreadsZT / 32 : 1][3];
+    if constexpr (kLearned) {
+        for (int q = 0; q < 3; ++q) {
+            const unsigned tt = __reduce_add_sync(kFull, (unsigned)cnt[q]);
+            if ((threadIdx.x & 31) == 0) wcount[threadIdx.x >> 5][q] = tt;
+        }
+    }
+    const int nbad = tiles::block_isum<kZoneThreadsZT>(bad);   // its barrier also orders wcount
+    if constexpr (kLearned) {
+        constexpr int kCounted[3] = {kClassZero, kClassDead, kClassAcute};
+        if (threadIdx.x < 3) {
+            unsigned tt = 0;
+            for (int w = 0; w < kZoneThreadsZT / 32; ++w) tt += wcount[w][threadIdx.x];
+            if (tt) atomicAdd(a.closure_counts + kCounted[threadIdx.x] * 64 + (blockIdx.x & 63), (unsigned long long)tt);
         }
     }
     fp64::block_to_cycle<true, kZoneThreadsZT>(a.cyc_red, zdthyd, nbad);
@@ -702,7 +772,10 @@ cudaError_t launch_cycle_mixed_impl(const DevArrays& a, const HydroConst& c, cud
     const int zba = (int)((a.numz + kZoneThreadsZT - 1) / kZoneThreadsZT);
     if (phases & kPhaseForces) {
         if (ev) cudaEventRecord(ev[0], stream);
-        if (learned) {
+        if (a.rect_nzx > 0) {
+            if (learned) pass_a_mixed_rows<true><<<a.gridA, kZoneThreadsZT, kRowsASmem, stream>>>(a, c);
+            else pass_a_mixed_rows<false><<<a.gridA, kZoneThreadsZT, kRowsASmem, stream>>>(a, c);
+        } else if (learned) {
             if (a.quads) pass_a_mixed_zt<true, true><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
             else pass_a_mixed_zt<false, true><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
         } else {
@@ -733,6 +806,12 @@ cudaError_t launch_cycle_mixed(const DevArrays& a, const HydroConst& c, cudaStre
 cudaError_t launch_cycle_learned(const DevArrays& a, const HydroConst& c, cudaStream_t stream, cudaEvent_t* ev,
                                  int phases) {
     return launch_cycle_mixed_impl(a, c, stream, ev, true, phases);
+}
+
+cudaError_t prepare_pass_a_rows_mixed(bool learned, int32_t rect_nzx, int32_t numz, int nsm, int32_t* grid) {
+    const int64_t nt = rows::num_tiles<kZoneThreadsZT>(rect_nzx, numz);
+    return learned ? rows::prepare(pass_a_mixed_rows<true>, kZoneThreadsZT, kRowsASmem, nt, nsm, grid)
+                   : rows::prepare(pass_a_mixed_rows<false>, kZoneThreadsZT, kRowsASmem, nt, nsm, grid);
 }
 
 cudaError_t prepare_learned_kernels() {

@@ -95,21 +95,18 @@ __device__ __forceinline__ double2 proj(double2 v, double ux, double uy) {
     return mk2(v.x - ux * d, v.y - uy * d);
 }
 
-// One zone's corrector from stage st, slot t: writes zvol, zr, zetot, ze,
-// zwrate; returns |dV/V0| and adds the zone's inverted sides to nbad.
-template <bool kQuads, bool kMixed>
-__device__ __forceinline__ double zone(const DevArrays& a, const HydroConst& c, const unsigned char* st, int t,
-                                       int64_t z, double dt, double dtinv, int& nbad) {
-    const int meta = reinterpret_cast<const int*>(st + kOffMeta)[t];
-    const int n = kQuads ? 4 : (meta & 15);
-    const double* sx0x = reinterpret_cast<const double*>(st + kOffX0x);
-    const double2* su0 = reinterpret_cast<const double2*>(st + kOffU0);
-    const double2* sx = reinterpret_cast<const double2*>(st + kOffX);
-    const double2* su = reinterpret_cast<const double2*>(st + kOffU);
-    const double2* ssf = reinterpret_cast<const double2*>(st + kOffSf);
-    const uint32_t* smw = reinterpret_cast<const uint32_t*>(st + kOffMw);
-    const double* szs = reinterpret_cast<const double*>(st + kOffZs);
-    const double zm = szs[t], zetot0 = szs[kTile + t], zvol0 = szs[2 * kTile + t], zp = szs[3 * kTile + t];
+// One zone's corrector from its inputs, read through `in` where they are
+// used: for side k < n, in.x(k) / in.u(k) the new position and velocity of
+// the side's first point, in.u0(k) its start-of-cycle velocity (before the
+// boundary projections), in.x0x(k) its start-of-cycle x, in.mask(k) its BC
+// plane mask, in.sf(k) the side's sfp + sfq; in.zm() etc. the zone's
+// scalars.  Writes zvol, zr, zetot, ze, zwrate; returns |dV/V0| and adds the
+// zone's inverted sides to nbad.
+template <bool kQuads, bool kMixed, typename In>
+__device__ __forceinline__ double zone_core(const DevArrays& a, const HydroConst& c, int n, const In& in, int64_t z,
+                                            double dt, double dtinv, int& nbad) {
+    if (kQuads) n = 4;
+    const double zm = in.zm(), zetot0 = in.zetot(), zvol0 = in.zvol(), zp = in.zp();
     const double dth = 0.5 * dt;
 
     double2 x[4], ub[4];
@@ -117,11 +114,11 @@ __device__ __forceinline__ double zone(const DevArrays& a, const HydroConst& c, 
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         if (k < n) {
-            x[k] = sx[k * kTile + t];
-            const double2 u0 = su0[k * kTile + t];
-            xpx[k] = sx0x[k * kTile + t] + u0.x * dth;   // advPosHalf's x, from pu0 before the BCs
+            x[k] = in.x(k);
+            const double2 u0 = in.u0(k);
+            xpx[k] = in.x0x(k) + u0.x * dth;   // advPosHalf's x, from pu0 before the BCs
             // applyFixedBC on pu0 (Hydro.cc:1008-1032), planes in deck order
-            const unsigned mask = (smw[k * kTile + t] >> (((meta >> (4 + k)) & 1) * 16)) & 0xffffu;
+            const unsigned mask = in.mask(k);
             double2 u0b = u0;
             if (mask) {
                 for (int b = 0; b < c.nbc; ++b)
@@ -160,9 +157,9 @@ __device__ __forceinline__ double zone(const DevArrays& a, const HydroConst& c, 
             nbad += (sv <= 0.) ? 1 : 0;
             // calcWork (Hydro.cc:1339-1406): the side's force against the
             // average velocity of its two points, at the half-step positions
-            const double2 sf = ssf[k * kTile + t];
-            const double2 u = su[k * kTile + t];
-            const double2 u2 = su[k2 * kTile + t];
+            const double2 sf = in.sf(k);
+            const double2 u = in.u(k);
+            const double2 u2 = in.u(k2);
             const double sd1 = sf.x * (ub[k].x + u.x) + sf.y * (ub[k].y + u.y);
             const double sd2 = (-sf.x) * (ub[k2].x + u2.x) + (-sf.y) * (ub[k2].y + u2.y);
             const double dwork = -dth * (sd1 * xpx[k] + sd2 * xpx[k2]);
@@ -187,6 +184,45 @@ __device__ __forceinline__ double zone(const DevArrays& a, const HydroConst& c, 
     a.ze[z] = zetot / (zm + 1.e-99);
     a.zwrate[z] = zwrate;
     return fabs((zvol - zvol0) / zvol0);
+}
+
+// The staged layout above, slot t of stage st.
+struct StagedIn {
+    const unsigned char* st;
+    int t, meta;
+    __device__ __forceinline__ double2 x(int k) const {
+        return reinterpret_cast<const double2*>(st + kOffX)[k * kTile + t];
+    }
+    __device__ __forceinline__ double2 u(int k) const {
+        return reinterpret_cast<const double2*>(st + kOffU)[k * kTile + t];
+    }
+    __device__ __forceinline__ double2 u0(int k) const {
+        return reinterpret_cast<const double2*>(st + kOffU0)[k * kTile + t];
+    }
+    __device__ __forceinline__ double x0x(int k) const {
+        return reinterpret_cast<const double*>(st + kOffX0x)[k * kTile + t];
+    }
+    __device__ __forceinline__ double2 sf(int k) const {
+        return reinterpret_cast<const double2*>(st + kOffSf)[k * kTile + t];
+    }
+    __device__ __forceinline__ unsigned mask(int k) const {
+        const uint32_t w = reinterpret_cast<const uint32_t*>(st + kOffMw)[k * kTile + t];
+        return (w >> (((meta >> (4 + k)) & 1) * 16)) & 0xffffu;
+    }
+    __device__ __forceinline__ double zs(int f) const { return reinterpret_cast<const double*>(st + kOffZs)[f * kTile + t]; }
+    __device__ __forceinline__ double zm() const { return zs(0); }
+    __device__ __forceinline__ double zetot() const { return zs(1); }
+    __device__ __forceinline__ double zvol() const { return zs(2); }
+    __device__ __forceinline__ double zp() const { return zs(3); }
+};
+
+// One zone's corrector from stage st, slot t.
+template <bool kQuads, bool kMixed>
+__device__ __forceinline__ double zone(const DevArrays& a, const HydroConst& c, const unsigned char* st, int t,
+                                       int64_t z, double dt, double dtinv, int& nbad) {
+    const int meta = reinterpret_cast<const int*>(st + kOffMeta)[t];
+    const StagedIn in{st, t, meta};
+    return zone_core<kQuads, kMixed>(a, c, meta & 15, in, z, dt, dtinv, nbad);
 }
 
 // The persistent pass C over the CTA's tiles: the maximum |dV/V0| into

@@ -38,6 +38,7 @@ struct Mesh {
     std::vector<int32_t> zfirst;       // first side of each zone
     std::vector<int32_t> poff, pcorner;  // point -> sides CSR (ascending side)
     bool all_quads = false;            // every zone has 4 sides at 4z..4z+3
+    int32_t rect_nzx = 0;              // > 0: the rect generator's numbering, nzx zones a row
     // initial geometry (Mesh::init, Mesh.cc:619-623)
     std::vector<double> zx, zarea, zvol, sarea, svol, smf;
     // Multi-piece runs (make_piece): this mesh is piece `piece` of
