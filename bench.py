@@ -322,16 +322,16 @@ def run_leblanc(args, pb, np, torch):
     return 0
 
 
-def run_batch(args, pb, np, torch):
+def batch_record(pb, torch, count=256):
     """The seeded 256-instance Sedov batch (decks/make_decks.py sedov_batch:
     N log-uniform in [32, 512], E0 in [0.1, 1], gamma in [1.4, 5/3], t = 0.5)
     in one pnt_batch (autotuned tile shape, persistent launches, CUDA graph),
     against the same instances run one after another as single-mesh objects
     (graph replay each).  Both timings are wall clock around the runs with
-    the objects already created; a sample of instances is compared bit for
-    bit."""
+    the objects already created; every 16th instance is compared bit for
+    bit with its single run."""
     from make_decks import sedov_batch
-    insts = sedov_batch(256)
+    insts = sedov_batch(count)
     decks = [pb.Deck(text=i["text"]) for i in insts]
     meshes = [pb.Mesh(deck=d) for d in decks]
     params = [d.params() for d in decks]
@@ -356,16 +356,114 @@ def run_batch(args, pb, np, torch):
     for i in range(0, len(insts), 16):
         for k in ("zr", "ze", "px", "pu"):
             mismatch += int(hs[i].download(k).tobytes() != b.download(i, k).tobytes())
-    out = {"metric": "zone-cycles/s, 256-instance Sedov batch to t=0.5", "unit": "zone-cycles/s",
-           "value": zc / t_batch, "data": "synthetic", "dtype": "f64",
-           "config": {"instances": len(insts), "zones": sum(m.numz for m in meshes), "zone_cycles": zc,
-                      "cycles_min": min(s["cycle"] for s in sc), "cycles_max": max(s["cycle"] for s in sc),
-                      "tile_zones": zpt, "ctas_per_sm": cps, "tuned_ms_per_cycle": ms_tune,
-                      "left_running": left},
-           "batch_wall_s": t_batch, "sequential_wall_s": t_seq, "sequential_value": zc / t_seq,
-           "speedup_vs_sequential": t_seq / t_batch, "sampled_instances_bitwise_mismatches": mismatch,
-           "status_nonzero": sum(1 for s in sc if s["status"])}
+    for h in hs:
+        h.close()
+    b.close()
+    return {"metric": f"zone-cycles/s, {len(insts)}-instance Sedov batch to t=0.5", "unit": "zone-cycles/s",
+            "value": zc / t_batch, "dtype": "f64",
+            "config": {"instances": len(insts), "zones": sum(m.numz for m in meshes), "zone_cycles": zc,
+                       "cycles_min": min(s["cycle"] for s in sc), "cycles_max": max(s["cycle"] for s in sc),
+                       "tile_zones": zpt, "ctas_per_sm": cps, "tuned_ms_per_cycle": ms_tune,
+                       "left_running": left},
+            "batch_wall_s": t_batch, "sequential_wall_s": t_seq, "sequential_value": zc / t_seq,
+            "speedup_vs_sequential": t_seq / t_batch, "sampled_instances_bitwise_mismatches": mismatch,
+            "status_nonzero": sum(1 for s in sc if s["status"])}
+
+
+def run_batch(args, pb, np, torch):
+    """--workload batch: the config-3 batch record alone (batch_record)."""
+    out = batch_record(pb, torch)
+    out["data"] = "synthetic"
     print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_pieces(args, pb, np, torch, dist, rank, world, local_rank):
+    """--decomp pieces: the deck's mesh split into `world` pieces, one per
+    rank (pnt_mesh_piece; the reference's numpcs decomposition), stepped
+    over NCCL with the halo sums of corner mass and force and the dt
+    reductions every cycle.  Every rank replays CUDA graphs of whole cycles
+    (kernels, NCCL sends/receives and all-reduces); `value` = zones of the
+    whole mesh x K / (max over ranks of the CUDA-event time of K cycles):
+    strong scaling.  The start state is the FP64 pieces' run to
+    --start-cycles, copied into the timed path's pieces."""
+    from datetime import timedelta
+    from pennant_b200.pieces import PieceHydro
+    if world == 1:   # a single piece run without a launcher
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29517")
+        os.environ.setdefault("RANK", "0")
+        os.environ.setdefault("WORLD_SIZE", "1")
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
+    deck = pb.Deck(path=args.deck)
+    mesh = pb.Mesh(deck=deck)
+    numz, nums, nump = mesh.numz, mesh.nums, mesh.nump
+    closure = pb.Closure(path=args.closure, device=local_rank) if args.precision == "learned" else None
+
+    def params(precision):
+        d = pb.Deck(path=args.deck)
+        d.set("precision", precision)
+        return d.params()
+
+    chunk = 10
+    t0 = time.perf_counter()
+    base = PieceHydro(mesh, params("fp64"), device=local_rank)
+    base.capture(chunk)
+    for _ in range(args.start_cycles // chunk):
+        base.replay()
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    start = base.scalars()
+    head = PieceHydro(mesh, params(args.precision), device=local_rank, closure=closure)
+    head.hydro.copy_state_from(base.hydro)
+    base.close()
+    # host cost of one eagerly stepped cycle (library calls and NCCL
+    # launches from Python), then the graph of `chunk` cycles
+    torch.cuda.synchronize()
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.warmup):
+        head.cycle()
+    torch.cuda.synchronize()
+    eager_ms = (time.perf_counter() - t0) * 1e3 / args.warmup
+    head.capture(chunk)
+    for _ in range(max(1, args.warmup // chunk)):
+        head.replay()
+    nrep = max(1, args.steps // chunk)
+    torch.cuda.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(head.stream)
+    for _ in range(nrep):
+        head.replay()
+    ev1.record(head.stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    steps = nrep * chunk
+    s = head.scalars()
+    head.close()
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank == 0:
+        line = {"metric": METRIC, "value": numz * steps / (ms / 1e3), "unit": UNIT, "n_gpus": world,
+                "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None,
+                "dtype": {"learned": "bf16+f32+f64", "mixed": "f32+f64", "fp64": "f64"}[args.precision],
+                "data": "synthetic",
+                "config": dict(workload_config(args.deck, numz, nums, nump, world),
+                               parallelism=f"pieces x{world}"),
+                "details": {"decomp": "pnt_mesh_piece zone strips, halo corner sums over NCCL, graph-replayed "
+                                      f"cycles ({chunk} a graph)", "path": args.precision,
+                            "start_state": {"cycle": start["cycle"], "time": start["time"], "setup_s": setup_s},
+                            "end_cycle": s["cycle"], "eager_ms_per_cycle": eager_ms},
+                "gpu_launches": None}
+        print(json.dumps(line), flush=True)
     return 0
 
 
@@ -424,6 +522,11 @@ def main():
     ap.add_argument("--probe", type=int, default=0, metavar="N",
                     help="profiling probe instead of the benchmark: Sedov N^2, the FP64 cycle to "
                          "--start-cycles, then one single-launch cycle of each path inside NVTX range 'prof'")
+    ap.add_argument("--decomp", default="replicas", choices=["replicas", "pieces"],
+                    help="N > 1: independent replicas (weak scaling) or the mesh split into N pieces that "
+                         "exchange halo corner sums over NCCL every cycle (strong scaling)")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the seeded 256-instance batch record of the default line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()
@@ -449,6 +552,8 @@ def main():
         return run_leblanc(args, pb, np, torch)
     if args.workload == "batch":
         return run_batch(args, pb, np, torch)
+    if args.decomp == "pieces":
+        return run_pieces(args, pb, np, torch, dist, rank, world, local_rank)
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local_rank))
@@ -629,6 +734,7 @@ def main():
                 accuracy["fallback_fraction"] = hp["fallback_fraction"]
                 accuracy["wait_timeouts"] = hp["wait_timeouts"]
     base.close()
+    batch = None if (args.no_batch or rank != 0) else batch_record(pb, torch)
 
     hbm, peak_kind = measured_peaks()
     names = ["A", "B", "C", "end_of_cycle", "closure"]   # the order of pnt_hydro_time_kernels
@@ -689,6 +795,7 @@ def main():
             "data": "synthetic",
             "config": workload_config(args.deck, numz, nums, nump, world),
             "accuracy": accuracy,
+            "batch": batch,
             "details": {"path": paths[args.precision], "start_state": start, "others": others,
                         "speedup_vs_fp64": res[args.precision]["value"] / res["fp64"]["value"],
                         "l1_rel_err_vs_fp64_window": window_err,

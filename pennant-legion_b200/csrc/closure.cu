@@ -8,17 +8,18 @@
 // (QCS.cc:116-327) on the state at the start of a cycle, sub-sampled by a
 // hash of (seed, cycle, side) and compacted in a deterministic order.
 //
-// Training: BF16 mma.sync (m16n8k16) with FP32 accumulation, 128 rows per
-// CTA: forward with the activations kept as the next layer's A fragments,
-// backward through the transposed weights, and the weight gradients as
-// contractions over the CTA's rows (ldmatrix.trans); per-CTA partial
-// gradients are summed in a fixed order and applied with Adam, so a run is
-// deterministic.  The inference in the hydro cycle uses the tcgen05 block
-// of closure_dev.cuh on the same parameters.
+// Training: the loss gradient of 128 rows per CTA on the tensor cores
+// (closure_train.cuh: tcgen05.mma with BF16 operands in shared memory and
+// FP32 accumulators in TMEM, forward, backward and the weight gradients as
+// contractions over the CTA's rows); per-CTA partial gradients are summed
+// in a fixed order and applied with Adam, so a run is deterministic.  The
+// inference in the hydro cycle uses the tcgen05 block of closure_dev.cuh on
+// the same parameters.
 //
 // Compiled with -fmad=false: the harvested targets repeat the FP64
 // cycle's QCS arithmetic.
 #include "closure_dev.cuh"
+#include "closure_train.cuh"
 #include "hydro_fp64_body.cuh"
 #include "pnt_internal.h"
 
@@ -284,355 +285,55 @@ __global__ void prepare_kernel(const float* feats, const float* targs, int64_t n
 // ----------------------------------------------------------------------
 // Parameter images
 // ----------------------------------------------------------------------
-// Training image (bf16, padded row strides for conflict-free fragments):
-constexpr int kTrW1 = 0;        // [64][24]
-constexpr int kTrW2 = 3072;     // [64][72]
-constexpr int kTrW2T = 12288;   // [64][72] transposed
-constexpr int kTrW3 = 21504;    // [8][72] (rows 4..7 zero)
-constexpr int kTrW3T = 22656;   // [64][24] transposed (cols 4.. zero)
-constexpr int kTrB1 = 25728;    // f32 [64]
-constexpr int kTrB2 = 25984;    // f32 [64]
-constexpr int kTrB3 = 26240;    // f32 [8]
-constexpr int kTrImgBytes = 26272;
-
+// The training image is train::kImg* (closure_train.cuh): the inference
+// operands W1, W2, W3 in the same canonical layout, the transposed W3^T and
+// W2^T the backward pass multiplies by, and the biases.
 __device__ __forceinline__ void put_bf16(uint8_t* img, int off, float v) {
     *reinterpret_cast<__nv_bfloat16*>(img + off) = __float2bfloat16_rn(v);
 }
 
 __global__ void pack_images(const float* P, Norm nm, float thr0, float thr1, float thr2, uint8_t* inf, uint8_t* tr) {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 8192; e += gridDim.x * blockDim.x) {
-        // W1 and W2, W2T: (j, i) over 64 x 64
+        // W1, W2 and W2^T: (j, i) over 64 x 64
         if (e < 4096) {
             const int j = e >> 6, i = e & 63;
             const float w2 = P[kClW2 + j * 64 + i];
             put_bf16(inf, kImgW2 + canon_off(j, i, 64), w2);
-            put_bf16(tr, kTrW2 + (j * 72 + i) * 2, w2);
-            put_bf16(tr, kTrW2T + (i * 72 + j) * 2, w2);
+            put_bf16(tr, train::kImgW2 + canon_off(j, i, 64), w2);
+            put_bf16(tr, train::kImgW2T + canon_off(i, j, 64), w2);
             if (i < 16) {
                 const float w1 = (i < kClIn) ? P[kClW1 + j * kClIn + i] : 0.f;
                 put_bf16(inf, kImgW1 + canon_off(j, i, 64), w1);
+                put_bf16(tr, train::kImgW1 + canon_off(j, i, 64), w1);
             }
-            if (i < 24) put_bf16(tr, kTrW1 + (j * 24 + i) * 2, (i < kClIn) ? P[kClW1 + j * kClIn + i] : 0.f);
-            if (i < 8) put_bf16(tr, kTrW2 + (j * 72 + 64 + i) * 2, 0.f), put_bf16(tr, kTrW2T + (j * 72 + 64 + i) * 2, 0.f);
         } else {
-            const int r = e - 4096;            // 0..4095
+            // W3 (o, j) over 16 x 64 (rows o >= 4 zero) and W3^T (j, o)
+            const int r = e - 4096;
             const int o = r >> 6, j = r & 63;   // o 0..63
             if (o < 16) {
                 const float w3 = (o < kClOut) ? P[kClW3 + o * 64 + j] : 0.f;
                 put_bf16(inf, kImgW3 + canon_off(o, j, 16), w3);
-                if (o < 8) put_bf16(tr, kTrW3 + (o * 72 + j) * 2, w3);
-                if (o < 8 && j < 8) put_bf16(tr, kTrW3 + (o * 72 + 64 + j) * 2, 0.f);
+                put_bf16(tr, train::kImgW3 + canon_off(o, j, 16), w3);
+                put_bf16(tr, train::kImgW3T + canon_off(j, o, 64), w3);
             }
-            if (o < 24) put_bf16(tr, kTrW3T + (j * 24 + o) * 2, (o < kClOut) ? P[kClW3 + o * 64 + j] : 0.f);
         }
         if (e < 64) {
             reinterpret_cast<float*>(inf + kImgB1)[e] = P[kClB1 + e];
             reinterpret_cast<float*>(inf + kImgB2)[e] = P[kClB2 + e];
-            reinterpret_cast<float*>(tr + kTrB1)[e] = P[kClB1 + e];
-            reinterpret_cast<float*>(tr + kTrB2)[e] = P[kClB2 + e];
+            reinterpret_cast<float*>(tr + train::kImgB1)[e] = P[kClB1 + e];
+            reinterpret_cast<float*>(tr + train::kImgB2)[e] = P[kClB2 + e];
         }
         if (e < 16) {
             reinterpret_cast<float*>(inf + kImgB3)[e] = (e < kClOut) ? P[kClB3 + e] : 0.f;
+            reinterpret_cast<float*>(tr + train::kImgB3)[e] = (e < kClOut) ? P[kClB3 + e] : 0.f;
             reinterpret_cast<float*>(inf + kImgFMean)[e] = nm.fmean[e];
             reinterpret_cast<float*>(inf + kImgFIstd)[e] = nm.fistd[e];
         }
-        if (e < 8) reinterpret_cast<float*>(tr + kTrB3)[e] = (e < kClOut) ? P[kClB3 + e] : 0.f;
         if (e < 4) {
             reinterpret_cast<float*>(inf + kImgTMean)[e] = nm.tmean[e];
             reinterpret_cast<float*>(inf + kImgTStd)[e] = nm.tstd[e];
             reinterpret_cast<float*>(inf + kImgThr)[e] = (e == 0) ? thr0 : (e == 1) ? thr1 : (e == 2) ? thr2 : 0.f;
         }
-    }
-}
-
-// ----------------------------------------------------------------------
-// Training: loss gradient of 128 rows per CTA
-// ----------------------------------------------------------------------
-constexpr int kTrThreads = 128;
-constexpr int kTrRows = 128;
-constexpr int kSmX = kTrImgBytes;                 // [128][24] bf16
-constexpr int kSmH1 = kSmX + kTrRows * 48;        // [128][72] bf16
-constexpr int kSmH2 = kSmH1 + kTrRows * 144;
-constexpr int kSmDZ1 = kSmH2 + kTrRows * 144;
-constexpr int kSmDZ2 = kSmDZ1 + kTrRows * 144;
-constexpr int kSmDY = kSmDZ2 + kTrRows * 144;     // [128][24] bf16
-constexpr int kSmZ = kSmDY + kTrRows * 48;        // f32 [warp][layer][64][32]
-constexpr int kSmBG = kSmZ + 4 * 2 * 64 * 32 * 4; // f32 [warp][132] bias gradients
-constexpr int kSmLoss = kSmBG + 4 * 132 * 4;      // f32 [warp]
-constexpr int kTrainSmem = kSmLoss + 16;
-static_assert(kSmX % 16 == 0 && kSmH1 % 16 == 0 && kSmDY % 16 == 0 && kSmZ % 16 == 0, "alignment");
-
-struct TrainArgs {
-    const uint8_t* img;
-    const __nv_bfloat16* x;   // [n][16]
-    const float* t;           // [n][4]
-    int64_t n, first, rows;   // this step: rows (first + i) mod n, i < rows
-    float inv_count;          // 1 / (rows * 4)
-    float* partial;           // [gridDim.x][kClParams + 1]
-};
-
-__device__ __forceinline__ void mma_bf16(float* d, const uint32_t* a, uint32_t b0, uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-__device__ __forceinline__ void ldsm4(uint32_t addr, uint32_t* r) {
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(addr));
-}
-__device__ __forceinline__ void ldsm4t(uint32_t addr, uint32_t* r) {
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(addr));
-}
-__device__ __forceinline__ uint32_t lds32(const uint8_t* p) { return *reinterpret_cast<const uint32_t*>(p); }
-__device__ __forceinline__ void sts32(uint8_t* p, uint32_t v) { *reinterpret_cast<uint32_t*>(p) = v; }
-
-// GELU and its derivative with the accurate tanh (training)
-__device__ __forceinline__ void gelu_exact(float x, float& y, float& dy) {
-    const float x2 = x * x;
-    const float u = kGeluC * (x + kGeluA * x2 * x);
-    const float th = tanhf(u);
-    y = 0.5f * x * (1.f + th);
-    dy = 0.5f * (1.f + th) + 0.5f * x * (1.f - th * th) * kGeluC * (1.f + 3.f * kGeluA * x2);
-}
-
-__global__ void __launch_bounds__(kTrThreads, 1) closure_grad_kernel(TrainArgs A) {
-    extern __shared__ __align__(16) uint8_t sm[];
-    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
-    const int q8 = lane >> 3, j8 = lane & 7;
-    for (int i = tid; i < kTrImgBytes / 16; i += kTrThreads)
-        reinterpret_cast<uint4*>(sm)[i] = __ldg(reinterpret_cast<const uint4*>(A.img) + i);
-    for (int i = tid; i < kTrRows * 2; i += kTrThreads) {
-        const int r = i >> 1, half = i & 1;
-        const int64_t idx = (int64_t)blockIdx.x * kTrRows + r;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-        if (idx < A.rows) {
-            const int64_t row = (A.first + idx) % A.n;
-            v = __ldg(reinterpret_cast<const uint4*>(A.x + row * 16) + half);
-        }
-        *reinterpret_cast<uint4*>(sm + kSmX + r * 48 + half * 16) = v;
-        if (half == 0) *reinterpret_cast<uint4*>(sm + kSmX + r * 48 + 32) = make_uint4(0u, 0u, 0u, 0u);
-    }
-    for (int i = tid; i < kTrRows * 3; i += kTrThreads)
-        reinterpret_cast<uint4*>(sm + kSmDY)[i] = make_uint4(0u, 0u, 0u, 0u);
-    __syncthreads();
-
-    const float* b1s = reinterpret_cast<const float*>(sm + kTrB1);
-    const float* b2s = reinterpret_cast<const float*>(sm + kTrB2);
-    const float* b3s = reinterpret_cast<const float*>(sm + kTrB3);
-    float* z1s = reinterpret_cast<float*>(sm + kSmZ) + (w * 2 + 0) * 64 * 32;
-    float* z2s = reinterpret_cast<float*>(sm + kSmZ) + (w * 2 + 1) * 64 * 32;
-    const uint32_t sbase = smem_addr(sm);
-
-    float db1[16], db2[16], db3[2] = {0.f, 0.f}, loss = 0.f;
-    for (int i = 0; i < 16; ++i) db1[i] = db2[i] = 0.f;
-
-    for (int mt = 0; mt < 2; ++mt) {
-        const int r0 = 32 * w + 16 * mt;
-        // ---- forward
-        uint32_t ax[4];
-        ldsm4(sbase + kSmX + (r0 + j8 + 8 * (q8 & 1)) * 48 + 16 * (q8 >> 1), ax);
-        uint32_t ah[4][4];
-        for (int nt = 0; nt < 8; ++nt) {
-            float acc[4] = {0.f, 0.f, 0.f, 0.f};
-            const uint8_t* wr = sm + kTrW1 + (8 * nt + g) * 48;
-            mma_bf16(acc, ax, lds32(wr + 4 * t4), lds32(wr + 16 + 4 * t4));
-            float hv[4];
-            for (int e = 0; e < 4; ++e) {
-                const float zz = acc[e] + b1s[8 * nt + 2 * t4 + (e & 1)];
-                z1s[((mt * 8 + nt) * 4 + e) * 32 + lane] = zz;
-                float dd;
-                gelu_exact(zz, hv[e], dd);
-            }
-            const uint32_t lo = pack_bf16(hv[0], hv[1]), hi = pack_bf16(hv[2], hv[3]);
-            sts32(sm + kSmH1 + (r0 + g) * 144 + (8 * nt + 2 * t4) * 2, lo);
-            sts32(sm + kSmH1 + (r0 + g + 8) * 144 + (8 * nt + 2 * t4) * 2, hi);
-            ah[nt >> 1][(nt & 1) * 2 + 0] = lo;
-            ah[nt >> 1][(nt & 1) * 2 + 1] = hi;
-        }
-        uint32_t ah2[4][4];
-        for (int nt = 0; nt < 8; ++nt) {
-            float acc[4] = {0.f, 0.f, 0.f, 0.f};
-            const uint8_t* wr = sm + kTrW2 + (8 * nt + g) * 144;
-            for (int kb = 0; kb < 4; ++kb) mma_bf16(acc, ah[kb], lds32(wr + 32 * kb + 4 * t4), lds32(wr + 32 * kb + 16 + 4 * t4));
-            float hv[4];
-            for (int e = 0; e < 4; ++e) {
-                const float zz = acc[e] + b2s[8 * nt + 2 * t4 + (e & 1)];
-                z2s[((mt * 8 + nt) * 4 + e) * 32 + lane] = zz;
-                float dd;
-                gelu_exact(zz, hv[e], dd);
-            }
-            const uint32_t lo = pack_bf16(hv[0], hv[1]), hi = pack_bf16(hv[2], hv[3]);
-            sts32(sm + kSmH2 + (r0 + g) * 144 + (8 * nt + 2 * t4) * 2, lo);
-            sts32(sm + kSmH2 + (r0 + g + 8) * 144 + (8 * nt + 2 * t4) * 2, hi);
-            ah2[nt >> 1][(nt & 1) * 2 + 0] = lo;
-            ah2[nt >> 1][(nt & 1) * 2 + 1] = hi;
-        }
-        float y[4] = {0.f, 0.f, 0.f, 0.f};
-        {
-            const uint8_t* wr = sm + kTrW3 + g * 144;
-            for (int kb = 0; kb < 4; ++kb) mma_bf16(y, ah2[kb], lds32(wr + 32 * kb + 4 * t4), lds32(wr + 32 * kb + 16 + 4 * t4));
-        }
-        // ---- loss and dY (outputs 2*t4, 2*t4+1 of rows g, g+8; t4 < 2 are real)
-        float dy[4] = {0.f, 0.f, 0.f, 0.f};
-        for (int hrow = 0; hrow < 2; ++hrow) {
-            const int64_t idx = (int64_t)blockIdx.x * kTrRows + r0 + g + 8 * hrow;
-            if (t4 < 2 && idx < A.rows) {
-                const int64_t row = (A.first + idx) % A.n;
-                const float2 tt = __ldg(reinterpret_cast<const float2*>(A.t + row * 4 + 2 * t4));
-                const float d0 = y[2 * hrow] + b3s[2 * t4] - tt.x;
-                const float d1 = y[2 * hrow + 1] + b3s[2 * t4 + 1] - tt.y;
-                loss += d0 * d0 + d1 * d1;
-                dy[2 * hrow] = 2.f * d0 * A.inv_count;
-                dy[2 * hrow + 1] = 2.f * d1 * A.inv_count;
-            }
-        }
-        db3[0] += dy[0] + dy[2];
-        db3[1] += dy[1] + dy[3];
-        uint32_t ady[4];
-        ady[0] = pack_bf16(dy[0], dy[1]);
-        ady[1] = pack_bf16(dy[2], dy[3]);
-        ady[2] = ady[3] = 0u;
-        if (t4 < 2) {
-            sts32(sm + kSmDY + (r0 + g) * 48 + 4 * t4, ady[0]);
-            sts32(sm + kSmDY + (r0 + g + 8) * 48 + 4 * t4, ady[1]);
-        }
-        // ---- dH2 = dY W3, dZ2 = dH2 * gelu'(Z2)
-        uint32_t adz[4][4];
-        for (int nt = 0; nt < 8; ++nt) {
-            float acc[4] = {0.f, 0.f, 0.f, 0.f};
-            const uint8_t* wr = sm + kTrW3T + (8 * nt + g) * 48;
-            mma_bf16(acc, ady, lds32(wr + 4 * t4), lds32(wr + 16 + 4 * t4));
-            float dz[4];
-            for (int e = 0; e < 4; ++e) {
-                float hh, dd;
-                gelu_exact(z2s[((mt * 8 + nt) * 4 + e) * 32 + lane], hh, dd);
-                dz[e] = acc[e] * dd;
-            }
-            db2[2 * nt] += dz[0] + dz[2];
-            db2[2 * nt + 1] += dz[1] + dz[3];
-            const uint32_t lo = pack_bf16(dz[0], dz[1]), hi = pack_bf16(dz[2], dz[3]);
-            sts32(sm + kSmDZ2 + (r0 + g) * 144 + (8 * nt + 2 * t4) * 2, lo);
-            sts32(sm + kSmDZ2 + (r0 + g + 8) * 144 + (8 * nt + 2 * t4) * 2, hi);
-            adz[nt >> 1][(nt & 1) * 2 + 0] = lo;
-            adz[nt >> 1][(nt & 1) * 2 + 1] = hi;
-        }
-        // ---- dH1 = dZ2 W2, dZ1 = dH1 * gelu'(Z1)
-        for (int nt = 0; nt < 8; ++nt) {
-            float acc[4] = {0.f, 0.f, 0.f, 0.f};
-            const uint8_t* wr = sm + kTrW2T + (8 * nt + g) * 144;
-            for (int kb = 0; kb < 4; ++kb) mma_bf16(acc, adz[kb], lds32(wr + 32 * kb + 4 * t4), lds32(wr + 32 * kb + 16 + 4 * t4));
-            float dz[4];
-            for (int e = 0; e < 4; ++e) {
-                float hh, dd;
-                gelu_exact(z1s[((mt * 8 + nt) * 4 + e) * 32 + lane], hh, dd);
-                dz[e] = acc[e] * dd;
-            }
-            db1[2 * nt] += dz[0] + dz[2];
-            db1[2 * nt + 1] += dz[1] + dz[3];
-            sts32(sm + kSmDZ1 + (r0 + g) * 144 + (8 * nt + 2 * t4) * 2, pack_bf16(dz[0], dz[1]));
-            sts32(sm + kSmDZ1 + (r0 + g + 8) * 144 + (8 * nt + 2 * t4) * 2, pack_bf16(dz[2], dz[3]));
-        }
-    }
-    // bias gradients and loss: reduce over the 8 row groups (lanes with the same t4)
-    for (int o = 4; o < 32; o <<= 1) {
-        for (int i = 0; i < 16; ++i) {
-            db1[i] += __shfl_xor_sync(kFull, db1[i], o);
-            db2[i] += __shfl_xor_sync(kFull, db2[i], o);
-        }
-        db3[0] += __shfl_xor_sync(kFull, db3[0], o);
-        db3[1] += __shfl_xor_sync(kFull, db3[1], o);
-    }
-    for (int o = 1; o < 32; o <<= 1) loss += __shfl_xor_sync(kFull, loss, o);
-    float* bg = reinterpret_cast<float*>(sm + kSmBG) + w * 132;
-    if (g == 0) {
-        for (int nt = 0; nt < 8; ++nt) {
-            bg[8 * nt + 2 * t4] = db1[2 * nt];
-            bg[8 * nt + 2 * t4 + 1] = db1[2 * nt + 1];
-            bg[64 + 8 * nt + 2 * t4] = db2[2 * nt];
-            bg[64 + 8 * nt + 2 * t4 + 1] = db2[2 * nt + 1];
-        }
-        if (t4 < 2) {
-            bg[128 + 2 * t4] = db3[0];
-            bg[128 + 2 * t4 + 1] = db3[1];
-        }
-    }
-    if (lane == 0) reinterpret_cast<float*>(sm + kSmLoss)[w] = loss;
-    __syncthreads();
-
-    float* P = A.partial + (int64_t)blockIdx.x * (kClParams + 1);
-    // ---- dW2[j][i] = sum_r dZ2[r][j] H1[r][i]: warp w owns j in [16w, 16w+16)
-    {
-        float acc[8][4];
-        for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
-        for (int kb = 0; kb < 8; ++kb) {
-            uint32_t a[4];
-            ldsm4t(sbase + kSmDZ2 + (16 * kb + j8 + 8 * (q8 >> 1)) * 144 + (16 * w + 8 * (q8 & 1)) * 2, a);
-            for (int np = 0; np < 4; ++np) {
-                uint32_t b[4];
-                ldsm4t(sbase + kSmH1 + (16 * kb + j8 + 8 * (q8 & 1)) * 144 + (16 * np + 8 * (q8 >> 1)) * 2, b);
-                mma_bf16(acc[2 * np], a, b[0], b[1]);
-                mma_bf16(acc[2 * np + 1], a, b[2], b[3]);
-            }
-        }
-        for (int nt = 0; nt < 8; ++nt) {
-            const int j = 16 * w + g, i = 8 * nt + 2 * t4;
-            P[kClW2 + j * 64 + i] = acc[nt][0];
-            P[kClW2 + j * 64 + i + 1] = acc[nt][1];
-            P[kClW2 + (j + 8) * 64 + i] = acc[nt][2];
-            P[kClW2 + (j + 8) * 64 + i + 1] = acc[nt][3];
-        }
-    }
-    // ---- dW1[j][i] = sum_r dZ1[r][j] X[r][i] (i < 14)
-    {
-        float acc[2][4];
-        for (int i = 0; i < 2; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
-        for (int kb = 0; kb < 8; ++kb) {
-            uint32_t a[4], b[4];
-            ldsm4t(sbase + kSmDZ1 + (16 * kb + j8 + 8 * (q8 >> 1)) * 144 + (16 * w + 8 * (q8 & 1)) * 2, a);
-            ldsm4t(sbase + kSmX + (16 * kb + j8 + 8 * (q8 & 1)) * 48 + (8 * (q8 >> 1)) * 2, b);
-            mma_bf16(acc[0], a, b[0], b[1]);
-            mma_bf16(acc[1], a, b[2], b[3]);
-        }
-        for (int nt = 0; nt < 2; ++nt)
-            for (int e = 0; e < 4; ++e) {
-                const int j = 16 * w + g + 8 * (e >> 1), i = 8 * nt + 2 * t4 + (e & 1);
-                if (i < kClIn) P[kClW1 + j * kClIn + i] = acc[nt][e];
-            }
-    }
-    // ---- dW3[o][j] = sum_r dY[r][o] H2[r][j]: warp w owns j in [16w, 16w+16)
-    {
-        float acc[2][4];
-        for (int i = 0; i < 2; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
-        for (int kb = 0; kb < 8; ++kb) {
-            uint32_t a[4], b[4];
-            ldsm4t(sbase + kSmDY + (16 * kb + j8 + 8 * (q8 >> 1)) * 48 + (8 * (q8 & 1)) * 2, a);
-            ldsm4t(sbase + kSmH2 + (16 * kb + j8 + 8 * (q8 & 1)) * 144 + (16 * w + 8 * (q8 >> 1)) * 2, b);
-            mma_bf16(acc[0], a, b[0], b[1]);
-            mma_bf16(acc[1], a, b[2], b[3]);
-        }
-        if (g < kClOut)
-            for (int nt = 0; nt < 2; ++nt) {
-                const int j = 16 * w + 8 * nt + 2 * t4;
-                P[kClW3 + g * 64 + j] = acc[nt][0];
-                P[kClW3 + g * 64 + j + 1] = acc[nt][1];
-            }
-    }
-    // ---- biases (warps summed in order) and loss
-    const float* bgs = reinterpret_cast<const float*>(sm + kSmBG);
-    for (int i = tid; i < 132; i += kTrThreads) {
-        const float s = ((bgs[i] + bgs[132 + i]) + bgs[264 + i]) + bgs[396 + i];
-        if (i < 64) P[kClB1 + i] = s;
-        else if (i < 128) P[kClB2 + i - 64] = s;
-        else if (i < 128 + kClOut) P[kClB3 + i - 128] = s;
-    }
-    if (tid == 0) {
-        const float* ls = reinterpret_cast<const float*>(sm + kSmLoss);
-        P[kClParams] = ((ls[0] + ls[1]) + ls[2]) + ls[3];
     }
 }
 
@@ -743,13 +444,14 @@ struct pnt_closure {
     int partial_cap = 0;
     float* d_loss = nullptr;     // [2]: loss, error flag
     float* d_grad = nullptr;
+    int* d_err = nullptr;        // set by a training step whose tensor-core wait ran out
     int64_t adam_t = 0;
     cudaStream_t stream = nullptr;
 
     ~pnt_closure() {
         DeviceGuard dg(device);
         for (void* p : {(void*)d_params, (void*)d_m, (void*)d_v, (void*)d_img, (void*)d_trimg, (void*)d_partial,
-                        (void*)d_loss, (void*)d_grad})
+                        (void*)d_loss, (void*)d_grad, (void*)d_err})
             if (p) cudaFree(p);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -773,16 +475,19 @@ struct pnt_closure {
         CUDA_TRY(cudaMalloc(&d_m, kClParams * sizeof(float)));
         CUDA_TRY(cudaMalloc(&d_v, kClParams * sizeof(float)));
         CUDA_TRY(cudaMalloc(&d_img, kImgBytes));
-        CUDA_TRY(cudaMalloc(&d_trimg, kTrImgBytes));
+        CUDA_TRY(cudaMalloc(&d_trimg, train::kImgBytes));
+        CUDA_TRY(cudaMalloc(&d_err, sizeof(int)));
+        CUDA_TRY(cudaMemset(d_err, 0, sizeof(int)));
         CUDA_TRY(cudaMalloc(&d_loss, 16));
         CUDA_TRY(cudaMalloc(&d_grad, kClParams * sizeof(float)));
         CUDA_TRY(cudaMemset(d_img, 0, kImgBytes));
-        CUDA_TRY(cudaMemset(d_trimg, 0, kTrImgBytes));
+        CUDA_TRY(cudaMemset(d_trimg, 0, train::kImgBytes));
         CUDA_TRY(cudaMemset(d_m, 0, kClParams * sizeof(float)));
         CUDA_TRY(cudaMemset(d_v, 0, kClParams * sizeof(float)));
         static bool attr_done[64] = {};
         if (device < 64 && !attr_done[device]) {
-            CUDA_TRY(cudaFuncSetAttribute(closure_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem));
+            CUDA_TRY(cudaFuncSetAttribute(train::grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          train::kSmemBytes));
             CUDA_TRY(cudaFuncSetAttribute(closure_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           kForwardSmem));
             attr_done[device] = true;
@@ -801,6 +506,15 @@ struct pnt_closure {
         CUDA_TRY(cudaStreamSynchronize(stream));
         return PNT_OK;
     }
+    // a training step's tensor-core wait that ran out (the flag is cleared)
+    pnt_status check_err() {
+        int e = 0;
+        CUDA_TRY(cudaMemcpyAsync(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        if (!e) return PNT_OK;
+        CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
+        return fail(PNT_ERR_TIMEOUT, "a tensor-core wait of the training kernel ran out");
+    }
     pnt_status download() {
         CUDA_TRY(cudaMemcpyAsync(params.data(), d_params, kClParams * sizeof(float), cudaMemcpyDeviceToHost, stream));
         CUDA_TRY(cudaStreamSynchronize(stream));
@@ -818,12 +532,12 @@ struct pnt_closure {
     // One gradient pass over rows (first + i) mod n, i < rows; Adam step when apply.
     pnt_status step(const void* x, const float* t, int64_t n, int64_t first, int64_t rows, float lr, bool apply,
                     float* grad_host, float* loss_host) {
-        const int nparts = (int)((rows + kTrRows - 1) / kTrRows);
+        const int nparts = (int)((rows + train::kRows - 1) / train::kRows);
         pnt_status st = ensure_partial(nparts);
         if (st) return st;
-        TrainArgs A{d_trimg, static_cast<const __nv_bfloat16*>(x), t, n, first, rows, 1.f / (float)(rows * 4),
-                    d_partial};
-        closure_grad_kernel<<<nparts, kTrThreads, kTrainSmem, stream>>>(A);
+        train::Args A{d_trimg, static_cast<const __nv_bfloat16*>(x), t, n, first, rows, 1.f / (float)(rows * 4),
+                      d_partial, d_err};
+        train::grad_kernel<<<nparts, train::kThreads, train::kSmemBytes, stream>>>(A);
         CUDA_TRY(cudaGetLastError());
         float bc1 = 1.f, bc2 = 1.f;
         if (apply) {
@@ -1020,6 +734,7 @@ pnt_status pnt_closure_train(pnt_closure* c, const void* x, const float* t, int6
         if (st) return st;
     }
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (pnt_status st = c->check_err()) return st;
     return c->download();
 }
 
@@ -1029,6 +744,7 @@ pnt_status pnt_closure_gradient(pnt_closure* c, const void* x, const float* t, i
     float l = 0.f;
     pnt_status st = c->step(x, t, n, 0, n, 0.f, false, grad, &l);
     if (st) return st;
+    if ((st = c->check_err())) return st;
     if (loss) *loss = l;
     return PNT_OK;
 }

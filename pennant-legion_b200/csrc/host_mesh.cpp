@@ -210,7 +210,7 @@ pnt_status generate_mesh(const Deck& d, Mesh& m) {
 // zone (i, j) starting at point (i, j), (i+1, j), (i+1, j+1), (i, j+1)),
 // else 0.  The row-tile passes (row_tiles.cuh) rely on exactly this.
 int32_t rect_columns(const Mesh& m, bool quads) {
-    if (!quads || m.npieces != 1 || m.numz < 1) return 0;
+    if (!quads || m.is_piece || m.numz < 1) return 0;
     const int64_t npx = m.mapsp1[3];   // zone 0's left side starts at point (0, 1)
     const int64_t nzx = npx - 1, nz = m.numz;
     if (nzx < 1 || nz % nzx != 0 || (int64_t)m.nump != (nz / nzx + 1) * npx) return 0;
@@ -319,7 +319,7 @@ pnt_status finish_mesh(Mesh& m) {
 // points through Legion reductions instead, Hydro.cc:571-574, 766-769).
 // ---------------------------------------------------------------------
 pnt_status make_piece(const Mesh& g, int npieces, int piece, Mesh& m) {
-    if (g.npieces != 1) return fail(PNT_ERR_INVALID_ARG, "the mesh is already a piece");
+    if (g.is_piece) return fail(PNT_ERR_INVALID_ARG, "the mesh is already a piece");
     if (npieces < 1 || npieces > 64 || piece < 0 || piece >= npieces)
         return fail(PNT_ERR_INVALID_ARG, "piece %d of %d: 1-64 pieces", piece, npieces);
     const int64_t np = g.nump, nz = g.numz, ns = g.nums;
@@ -340,6 +340,7 @@ pnt_status make_piece(const Mesh& g, int npieces, int piece, Mesh& m) {
     m = Mesh();
     m.piece = piece;
     m.npieces = npieces;
+    m.is_piece = true;
     m.zone0 = z0;
     m.side0 = s0;
     std::vector<int32_t> lp(np, -1);
@@ -631,14 +632,14 @@ pnt_status pnt_mesh_piece_describe(const pnt_mesh* mesh, pnt_piece_desc* out) {
     out->npieces = m.npieces;
     out->zone0 = m.zone0;
     out->side0 = m.side0;
-    out->gpoint = m.npieces > 1 ? m.gpoint.data() : nullptr;
+    out->gpoint = m.is_piece ? m.gpoint.data() : nullptr;
     out->nhalo = m.nhalo;
     out->halo_side = m.halo_side.data();
     out->nnbr = (int32_t)m.nbr.size();
     out->nbr = m.nbr.data();
-    out->send_off = m.npieces > 1 ? m.send_off.data() : nullptr;
+    out->send_off = m.is_piece ? m.send_off.data() : nullptr;
     out->send_side = m.send_side.data();
-    out->recv_off = m.npieces > 1 ? m.recv_off.data() : nullptr;
+    out->recv_off = m.is_piece ? m.recv_off.data() : nullptr;
     return PNT_OK;
 }
 

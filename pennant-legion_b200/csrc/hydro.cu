@@ -333,7 +333,7 @@ pnt_status init_hydro(pnt_hydro* h, const Mesh& m, const pnt_params& p) {
     a.poff = poff;
     a.pcorner = pcorner;
     a.bcmask = mask;
-    if (m.npieces > 1) {
+    if (m.is_piece) {
         // a piece: halo corner slots follow the local sides in cmass/cforce
         h->piece = true;
         h->nhalo = m.nhalo;

@@ -49,6 +49,7 @@ struct Mesh {
     // grouped by owning neighbour (nbr, recv_off) in global side order.
     // send_side[send_off[j] .. send_off[j+1]) are the local sides whose
     // corner values neighbour nbr[j] needs, in global side order.
+    bool is_piece = false;             // made by make_piece (1 piece included): stepped piece by piece
     int32_t piece = 0, npieces = 1;
     int32_t zone0 = 0, side0 = 0;
     std::vector<int32_t> gpoint;

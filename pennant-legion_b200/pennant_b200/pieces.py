@@ -140,17 +140,50 @@ class PieceHydro:
 
     def cycle(self) -> None:
         """One cycle of every piece (all ranks call it together)."""
-        h = self.hydro.h
         with torch.cuda.stream(self.stream):
-            check(lib.pnt_hydro_piece_forces(h))
-            if dist.get_backend(self.group) != "nccl":
-                self.stream.synchronize()
-            self.halo.exchange(self.send, self.halo_m, self.halo_f)
-            check(lib.pnt_hydro_piece_advance(h))
-            if dist.get_backend(self.group) != "nccl":
-                self.stream.synchronize()
-            reduce_scalars(self.red, self.group)
-            check(lib.pnt_hydro_piece_finish(h))
+            self._cycle_ops()
+
+    def _cycle_ops(self) -> None:
+        h = self.hydro.h
+        nccl = dist.get_backend(self.group) == "nccl"
+        check(lib.pnt_hydro_piece_forces(h))
+        if not nccl:
+            self.stream.synchronize()
+        self.halo.exchange(self.send, self.halo_m, self.halo_f)
+        check(lib.pnt_hydro_piece_advance(h))
+        if not nccl:
+            self.stream.synchronize()
+        reduce_scalars(self.red, self.group)
+        check(lib.pnt_hydro_piece_finish(h))
+
+    def capture(self, ncycles: int) -> None:
+        """Records `ncycles` whole cycles -- the library's kernels, the NCCL
+        halo sends and receives and both reductions -- in one CUDA graph on
+        the piece's stream (NCCL groups only; every rank captures the same
+        count).  replay() then runs them with one launch from the host, the
+        analogue of the reference's traced cycle loop (Driver.cc:113-145).
+        close() releases the graph, which must happen before the process
+        group is destroyed."""
+        if dist.get_backend(self.group) != "nccl":
+            raise RuntimeError("graph capture needs the NCCL backend (gloo transfers go through the host)")
+        self.release_graph()
+        torch.cuda.synchronize(self.device)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=self.stream, capture_error_mode="thread_local"):
+            for _ in range(ncycles):
+                self._cycle_ops()
+        self.graph, self.graph_cycles = g, ncycles
+
+    def replay(self) -> None:
+        """One launch of the captured cycles on the piece's stream."""
+        with torch.cuda.stream(self.stream):
+            self.graph.replay()
+
+    def release_graph(self) -> None:
+        if getattr(self, "graph", None) is not None:
+            torch.cuda.synchronize(self.device)
+            self.graph.reset()
+            self.graph = None
 
     def run(self, max_cycles: int = 0, check_every: int = 16) -> dict:
         """Cycles until the run is done (or max_cycles); identical on every
@@ -174,4 +207,5 @@ class PieceHydro:
         return {k: self.hydro.download(k) for k in names}
 
     def close(self) -> None:
+        self.release_graph()
         self.hydro.close()

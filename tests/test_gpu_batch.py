@@ -11,7 +11,7 @@ from oracle import Oracle
 import pennant_b200 as pb
 
 sys.path.insert(0, DECKS)
-from make_decks import sedov  # noqa: E402
+from make_decks import sedov, sedov_batch  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -100,6 +100,26 @@ def test_batch_partial_run_and_instances_finishing_early():
     b.run()
     cycles = [b.scalars(i)["cycle"] for i in range(len(texts))]
     assert len(set(cycles)) > 1   # uneven meshes and stop times finish apart
+
+
+@pytest.mark.timeout(900)
+def test_seeded_batch_workload_subset_matches_single_runs_bitwise():
+    """The first 32 instances of the seeded 256-instance Sedov batch (sizes
+    log-uniform in [32, 512], E0 in [0.1, 1], gamma in [1.4, 5/3], to
+    t = 0.5) with the autotuned shape: every instance ends exactly as its
+    own single-mesh run."""
+    insts = sedov_batch(256)[:32]
+    texts = [i["text"] for i in insts]
+    assert min(i["n"] for i in insts) < 64 and max(i["n"] for i in insts) > 256
+    ref = single_runs(texts)
+    b, _, _ = make_batch(texts)
+    zpt, cps, _ = b.tune(2)
+    b.close()
+    b, _, _ = make_batch(texts)
+    b.set_shape(zpt, cps)
+    assert b.run() == 0
+    check_batch(b, ref)
+    assert all(abs(b.scalars(i)["time"] - 0.5) < 1e-12 for i in range(len(texts)))
 
 
 def test_batch_rejects_mixed_precision():

@@ -129,3 +129,45 @@ def test_native_pieces_match_the_single_piece_run_bitwise(case, npieces, tmp_pat
     ps.write_xy(str(tmp_path / "p.xy"))
     assert (tmp_path / "p.xy").stat().st_size > 0
     ps.close()
+
+
+def _graph_rank(rank, port, text, precision, cycles_per_graph, out):
+    import torch
+    import torch.distributed as dist
+    from pennant_b200.pieces import PieceHydro
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device("cuda", 0))
+    try:
+        d = _deck(text, precision)
+        clo = pb.Closure(path=CLOSURE) if precision == "learned" else None
+        ph = PieceHydro(pb.Mesh(deck=d), d.params(), device=0, closure=clo)
+        ph.cycle()                       # one eager cycle first, as bench.py's warm-up does
+        ph.capture(cycles_per_graph)
+        for _ in range(100000):
+            ph.replay()
+            if ph.scalars()["done"]:
+                break
+        out[0] = (ph.scalars(), ph.fields(ZONE + POINT))
+        ph.close()                       # releases the graph before the group goes
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(600)
+@pytest.mark.parametrize("case", ["sedov-fp64", "sedov-learned"])
+def test_graph_captured_piece_cycles_match_the_single_piece_run_bitwise(case):
+    """One rank over NCCL: whole piece cycles (kernels, halo send/receive,
+    both reductions) captured in a CUDA graph and replayed until the run
+    ends give the single-piece run bit for bit (cycles the graph runs past
+    the end are skipped on the device)."""
+    text, precision, _ = CASES[case]
+    s1, f1 = single(text, precision)
+    out = mp.get_context("spawn").Manager().dict()
+    mp.start_processes(_graph_rank, args=(_port(), text, precision, 7, out), nprocs=1, join=True,
+                       start_method="spawn")
+    s, f = out[0]
+    assert s["cycle"] == s1["cycle"] and s["time"] == s1["time"] and s["done"] == 1, (case, s, s1)
+    for k in ZONE + POINT:
+        assert f[k].tobytes() == f1[k].tobytes(), (case, k)
