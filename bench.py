@@ -56,10 +56,11 @@ DEFAULT_DECK = os.path.join(PKG, "decks", "sedov1920.pnt")
 DEFAULT_CLOSURE = os.path.join(PKG, "closure", "qcs_mlp.bin")
 MLP_FLOP_PER_ROW = 2 * (16 * 64 + 64 * 64 + 64 * 16)   # tensor-core MMA shapes, padded
 # DRAM bytes (read + write) of one pass A launch per zone, from the ncu
-# capture of profiles/pass_a_pass_c_sedov1024.md (1,048,576 zones; the
-# bench scales them by its zone count)
-PASS_A_TRAFFIC_PER_ZONE = {"learned": (125.963e6 + 92.962e6) / 1048576,
-                           "mixed": (125.960e6 + 84.336e6) / 1048576,
+# captures of profiles/pass_a_rows_learned_sedov1024.md (learned, mixed)
+# and profiles/pass_a_fp64_sedov1024.md (FP64), 1,048,576 zones each; the
+# bench scales them by its zone count
+PASS_A_TRAFFIC_PER_ZONE = {"learned": (109.737e6 + 88.343e6) / 1048576,
+                           "mixed": (109.363e6 + 76.074e6) / 1048576,
                            "fp64": (125.973e6 + 130.137e6) / 1048576}
 
 
@@ -806,7 +807,8 @@ def main():
                          "algorithmic_bytes_per_launch": per_launch[names[dom]], "launch_ms": kms_head[dom],
                          "traffic": PASS_A_TRAFFIC_PER_ZONE[args.precision] * numz if names[dom] == "A" else None,
                          "traffic_note": "ncu DRAM read+write of one pass A launch at 1024^2 (cycle 16000), "
-                                         "scaled by the zone count"},
+                                         "scaled by the zone count (writes still in L2 at the kernel's end "
+                                         "are not counted)"},
             "roofline_cycle": {"achieved": ach_cycle, "peak": hbm, "unit": "GB/s", "frac": ach_cycle / hbm,
                                "algorithmic_bytes_per_cycle": ab["cycle"],
                                "note": "FP64 schedule bytes B = 164 Np + 100 Ns + 104 Nz for every path"},

@@ -301,13 +301,15 @@ pnt_status pnt_hydro_stream(pnt_hydro* hydro, void** cuda_stream);
 /* ------------------------------------------------------------------ */
 /* Batches of independent meshes on one GPU (project extension: the       */
 /* reference advances one mesh per Driver).  Every instance runs the FP64 */
-/* cycle bit-identically to its own pnt_hydro; the batch advances all     */
-/* running instances by one of their own cycles per batch cycle.          */
+/* (or, for a batch of precision-mixed decks, the mixed) cycle            */
+/* bit-identically to its own pnt_hydro; the batch advances all running   */
+/* instances by one of their own cycles per batch cycle.                  */
 /* ------------------------------------------------------------------ */
 typedef struct pnt_batch pnt_batch;
 
-/* n meshes with their own parameters (params[i], precision FP64); the
- * meshes are copied.  Each instance starts as pnt_hydro_create would. */
+/* n meshes with their own parameters (params[i]; one precision for all,
+ * FP64 or mixed, else PNT_ERR_UNSUPPORTED); the meshes are copied.  Each
+ * instance starts as pnt_hydro_create would. */
 pnt_status pnt_batch_create(const pnt_mesh* const* meshes, const pnt_params* params, int32_t n,
                             int32_t device, pnt_batch** out);
 void pnt_batch_destroy(pnt_batch* batch);

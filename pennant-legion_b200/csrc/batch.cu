@@ -17,6 +17,7 @@
 // results do not depend on the shape).
 //
 // Compiled with -fmad=false (FP64 parity).
+#include "batch_dev.h"
 #include "hydro_fp64_body.cuh"
 #include "pass_c_staged.cuh"
 #include "pnt_internal.h"
@@ -34,30 +35,6 @@ namespace pnt {
 namespace {
 
 using namespace fp64;
-
-struct Tile {
-    int32_t inst;   // instance
-    int32_t beg;    // first zone (zone tiles) or point (point tiles), global
-    int32_t end;    // one past the last
-    int32_t quads;  // the instance's zones are all quads at sides 4z..4z+3
-};
-
-struct BatchDev {
-    DevArrays a;              // concatenated mesh and state; a.ctl unused
-    const Tile* ztiles;       // zone tiles grouped by instance
-    const Tile* ptiles;       // point tiles
-    int32_t nztiles, nptiles;
-    const int32_t* inst_tbeg; // [ninst+1] zone-tile range of each instance
-    const HydroConst* consts; // [ninst]
-    Ctl* ctls;                // [ninst]
-    int32_t ninst;
-};
-
-constexpr int kBatchThreads = 256;          // points per point-pass iteration; finalize warps
-constexpr int kBatchZT = 128;               // pass A: one zone per thread
-constexpr int kZonesPerIter = 64;           // zone tiles are whole multiples of this
-
-__device__ __forceinline__ bool inst_skip(const Ctl& ctl) { return ctl.done || ctl.cycle >= ctl.stop_at; }
 
 // Pass A: one CTA per tile (no persistent loop: its state would cost the
 // zone body registers), one thread per zone (pass_a_zone_thread), 128 zones
@@ -102,7 +79,7 @@ __global__ void __launch_bounds__(kBatchZT, 3) batch_pass_a(BatchDev b) {
 // computed); one partial per tile.
 // kAllQuads as in batch_pass_a; quad tiles load the next step's point
 // indices while the current step's copies are in flight.
-template <bool kAllQuads>
+template <bool kAllQuads, bool kMixed>
 __global__ void __launch_bounds__(stagedc::kTile) batch_pass_c(BatchDev b) {
     extern __shared__ __align__(16) unsigned char smem_c[];
     const int th = threadIdx.x;
@@ -129,8 +106,8 @@ __global__ void __launch_bounds__(stagedc::kTile) batch_pass_c(BatchDev b) {
             if (quads && z + stagedc::kTile < tile.end) nix = tiles::load_idx<true>(b.a, z + stagedc::kTile);
             tiles::wait_groups<0>();
             if (zok) {
-                const double d = quads ? stagedc::zone<true, false>(b.a, c, smem_c, th, z, dt, dtinv, nbad)
-                                       : stagedc::zone<false, false>(b.a, c, smem_c, th, z, dt, dtinv, nbad);
+                const double d = quads ? stagedc::zone<true, kMixed>(b.a, c, smem_c, th, z, dt, dtinv, nbad)
+                                       : stagedc::zone<false, kMixed>(b.a, c, smem_c, th, z, dt, dtinv, nbad);
                 dvm = (d > dvm) ? d : dvm;
             }
         }
@@ -226,6 +203,7 @@ struct pnt_batch {
     std::vector<int32_t> nz, np, ns;
     std::vector<int32_t> quads;
     bool all_quads = false;                      // every instance: quads at sides 4z..4z+3
+    bool mixed = false;                          // the mixed-precision cycle (every instance)
     Ctl* ctl_host = nullptr;                     // pinned [ninst]
     int* running_dev = nullptr;
     int* running_host = nullptr;                 // pinned
@@ -324,14 +302,22 @@ struct pnt_batch {
         const int grid_p = std::max(1, std::min(b.nptiles, nsm * shape.ctas_per_sm));
         const int grid_f = (ninst * 32 + kBatchThreads - 1) / kBatchThreads;
         if (ev) cudaEventRecord(ev[0], stream);
-        if (all_quads) batch_pass_a<true><<<std::max(1, b.nztiles), kBatchZT, 0, stream>>>(b);
+        if (mixed) launch_batch_pass_a_mixed(b, all_quads, stream);
+        else if (all_quads) batch_pass_a<true><<<std::max(1, b.nztiles), kBatchZT, 0, stream>>>(b);
         else batch_pass_a<false><<<std::max(1, b.nztiles), kBatchZT, 0, stream>>>(b);
         if (ev) cudaEventRecord(ev[1], stream);
-        batch_point_pass<<<grid_p, kBatchThreads, 0, stream>>>(b);
+        if (mixed) launch_batch_point_pass_mixed(b, grid_p, stream);
+        else batch_point_pass<<<grid_p, kBatchThreads, 0, stream>>>(b);
         if (ev) cudaEventRecord(ev[2], stream);
         const int gc = std::max(1, std::min(b.nztiles, grid_c));
-        if (all_quads) batch_pass_c<true><<<gc, stagedc::kTile, stagedc::kSmemBytes, stream>>>(b);
-        else batch_pass_c<false><<<gc, stagedc::kTile, stagedc::kSmemBytes, stream>>>(b);
+        const size_t smc = stagedc::kSmemBytes;
+        if (mixed) {
+            if (all_quads) batch_pass_c<true, true><<<gc, stagedc::kTile, smc, stream>>>(b);
+            else batch_pass_c<false, true><<<gc, stagedc::kTile, smc, stream>>>(b);
+        } else {
+            if (all_quads) batch_pass_c<true, false><<<gc, stagedc::kTile, smc, stream>>>(b);
+            else batch_pass_c<false, false><<<gc, stagedc::kTile, smc, stream>>>(b);
+        }
         if (ev) cudaEventRecord(ev[3], stream);
         batch_finalize<<<grid_f, kBatchThreads, 0, stream>>>(b);
         if (ev) cudaEventRecord(ev[4], stream);
@@ -482,8 +468,10 @@ pnt_status pnt_batch_create(const pnt_mesh* const* meshes, const pnt_params* par
     if (device < 0 || device >= ndev) return fail(PNT_ERR_INVALID_ARG, "device %d out of range", device);
     for (int i = 0; i < n; ++i) {
         if (!meshes[i]) return fail(PNT_ERR_INVALID_ARG, "null mesh %d", i);
-        if (params[i].precision != PNT_PREC_FP64)
-            return fail(PNT_ERR_UNSUPPORTED, "batched instances run the FP64 cycle (instance %d)", i);
+        if (params[i].precision == PNT_PREC_LEARNED)
+            return fail(PNT_ERR_UNSUPPORTED, "batched instances run the FP64 or the mixed cycle (instance %d)", i);
+        if (params[i].precision != params[0].precision)
+            return fail(PNT_ERR_UNSUPPORTED, "batched instances share one precision (instance %d)", i);
         if (params[i].nbcx + params[i].nbcy > kMaxBC) return fail(PNT_ERR_UNSUPPORTED, "too many BC planes");
     }
     DeviceGuard dg(device);
@@ -491,6 +479,7 @@ pnt_status pnt_batch_create(const pnt_mesh* const* meshes, const pnt_params* par
     if (!bt) return fail(PNT_ERR_NOMEM, "out of memory");
     bt->device = device;
     bt->ninst = n;
+    bt->mixed = params[0].precision == PNT_PREC_MIXED;
     cudaDeviceGetAttribute(&bt->nsm, cudaDevAttrMultiProcessorCount, device);
     pnt_status st = PNT_OK;
     try {
@@ -569,6 +558,9 @@ pnt_status pnt_batch_create(const pnt_mesh* const* meshes, const pnt_params* par
         a.poff = d_poff;
         a.pcorner = d_pcorner;
         a.bcmask = d_mask;
+        a.cmass_f = reinterpret_cast<float*>(a.cmass);
+        a.cforce_f = reinterpret_cast<float2*>(a.cforce);
+        a.sftot_f = reinterpret_cast<float2*>(a.sftot);
         a.ctl = nullptr;
         bt->b.consts = d_consts;
         bt->b.ctls = d_ctls;
@@ -593,14 +585,15 @@ pnt_status pnt_batch_create(const pnt_mesh* const* meshes, const pnt_params* par
         if (e == cudaSuccess) e = cudaMemset(d_mask + NP, 0, 4);   // pass C copies 32-bit mask words
         if (e == cudaSuccess) {
             // the staged pass C: its shared-memory limit and resident CTAs per SM
-            e = cudaFuncSetAttribute(batch_pass_c<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, stagedc::kSmemBytes);
-            if (e == cudaSuccess)
-                e = cudaFuncSetAttribute(batch_pass_c<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         stagedc::kSmemBytes);
+            for (auto k : {batch_pass_c<true, false>, batch_pass_c<false, false>, batch_pass_c<true, true>,
+                           batch_pass_c<false, true>})
+                if (e == cudaSuccess)
+                    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, stagedc::kSmemBytes);
             int occ = 0;
             if (e == cudaSuccess)
-                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_pass_c<false>, stagedc::kTile,
-                                                                  stagedc::kSmemBytes);
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &occ, bt->mixed ? batch_pass_c<false, true> : batch_pass_c<false, false>, stagedc::kTile,
+                    stagedc::kSmemBytes);
             if (e == cudaSuccess && occ < 1) e = cudaErrorInvalidConfiguration;
             bt->grid_c = bt->nsm * std::max(occ, 1);
         }

@@ -29,6 +29,7 @@
 // error against the FP64 run (tests/test_gpu_mixed.py).
 #include "closure_dev.cuh"
 #include "hydro_fp64_body.cuh"
+#include "batch_dev.h"
 #include "hydro_dev.h"
 #include "row_tiles.cuh"
 #include "zone_tiles.cuh"
@@ -548,8 +549,11 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_ROWS_A_MIN_BLOCKS) pass_a_
         const rows::RowZoneIn<kZoneThreadsZT> in{st, t, (int)(tl.z0 & 1)};
         const int64_t z = tl.z0 + t;
         double v = 1.e99;
-        pass_a_mixed_zone<4, kLearned>(a, c, in, cur, dt, z, 4 * z, v, bad, cnt, sp);
+        int zc[3] = {0, 0, 0};   // the zone's own corner classes (an acute zone overwrites them)
+        pass_a_mixed_zone<4, kLearned>(a, c, in, cur, dt, z, 4 * z, v, bad, zc, sp);
         zdthyd = dmin(zdthyd, v);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) cnt[q] += zc[q];
     };
     if (!rows::for_tiles<kRowsAStages, AStage::kBytes>(ntiles, smem_a, bars, bytes, issue, compute) && t == 0)
         atomicOr(reinterpret_cast<unsigned long long*>(a.cyc_red + 4), 1ull);
@@ -575,15 +579,8 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_ROWS_A_MIN_BLOCKS) pass_a_
 // ---------------------------------------------------------------------
 // Pass B, mixed: FP32 corner inputs summed in FP64
 // ---------------------------------------------------------------------
-__global__ void __launch_bounds__(kPointThreads) pass_b_mixed(DevArrays a, HydroConst c) {
-    const Ctl* ctl = a.ctl;
-    // the closure pass has consumed this cycle's zone records
-    if (a.closure_nrec && blockIdx.x == 0 && threadIdx.x == 0) *a.closure_nrec = 0;
-    if (skip_cycle(ctl)) return;
-    const int64_t p = (int64_t)blockIdx.x * kPointThreads + threadIdx.x;
-    if (p >= a.nump) return;
-    const int cur = ctl->cycle & 1;
-    const double dt = ctl->dt;
+__device__ __forceinline__ void pass_b_mixed_point(const DevArrays& a, const HydroConst& c, int cur, double dt,
+                                                   int64_t p) {
     const double2 x0 = a.px[cur][p];
     double2 u0 = a.pu[cur][p];
     const int32_t o0 = a.poff[p], o1 = a.poff[p + 1];
@@ -610,6 +607,70 @@ __global__ void __launch_bounds__(kPointThreads) pass_b_mixed(DevArrays a, Hydro
     const double2 x = add(x0, smul(dt * 0.5, add(u0, u)));
     a.px[cur ^ 1][p] = x;
     a.pu[cur ^ 1][p] = u;
+}
+
+__global__ void __launch_bounds__(kPointThreads) pass_b_mixed(DevArrays a, HydroConst c) {
+    const Ctl* ctl = a.ctl;
+    // the closure pass has consumed this cycle's zone records
+    if (a.closure_nrec && blockIdx.x == 0 && threadIdx.x == 0) *a.closure_nrec = 0;
+    if (skip_cycle(ctl)) return;
+    const int64_t p = (int64_t)blockIdx.x * kPointThreads + threadIdx.x;
+    if (p >= a.nump) return;
+    pass_b_mixed_point(a, c, ctl->cycle & 1, ctl->dt, p);
+}
+
+// ---------------------------------------------------------------------
+// The mixed cycle of a batch of meshes (batch.cu): the zone and point
+// bodies above over the batch's work lists, as batch_pass_a and
+// batch_point_pass run the FP64 ones.
+// ---------------------------------------------------------------------
+template <bool kAllQuads>
+__global__ void __launch_bounds__(kBatchZT, PNT_MIXED_ZT_MIN_BLOCKS) batch_pass_a_mixed(BatchDev b) {
+    const int t = blockIdx.x;
+    if (t >= b.nztiles) return;   // no tiles left: the grid is one idle CTA
+    const Tile tile = b.ztiles[t];
+    const Ctl& ctl = b.ctls[tile.inst];
+    if (inst_skip(ctl)) return;   // uniform over the CTA
+    const HydroConst& c = b.consts[tile.inst];
+    const int cur = ctl.cycle & 1;
+    const double dt = ctl.dt;
+    __shared__ double2 s_sfp[4 * kBatchZT];
+    __shared__ float2 s_sft[4 * kBatchZT];
+    const SideSpill sp{s_sfp, s_sft, (int)threadIdx.x};
+    double fold = 1.e99;
+    int nbad = 0;
+    for (int zb = tile.beg; zb < tile.end; zb += kBatchZT) {
+        const int64_t z = (int64_t)zb + threadIdx.x;
+        if (z >= tile.end) continue;
+        double v = 1.e99;
+        int cnt[3] = {0, 0, 0};
+        if (kAllQuads || tile.quads) {
+            const fp64::GlobalZoneIn in{b.a, cur, z, 4 * z};
+            pass_a_mixed_zone<4, false>(b.a, c, in, cur, dt, z, 4 * z, v, nbad, cnt, sp);
+        } else {
+            const int n = b.a.znump[z];
+            const int64_t s0 = b.a.zfirst[z];
+            const fp64::GlobalZoneIn in{b.a, cur, z, s0};
+            if (n == 4) pass_a_mixed_zone<4, false>(b.a, c, in, cur, dt, z, s0, v, nbad, cnt, sp);
+            else pass_a_mixed_zone<3, false>(b.a, c, in, cur, dt, z, s0, v, nbad, cnt, sp);
+        }
+        fold = dmin(fold, v);
+    }
+    nbad = tiles::block_isum<kBatchZT>(nbad);
+    block_fold<true, kBatchZT>(fold, b.a.part_dtnew + t);
+    if (threadIdx.x == 0) b.a.part_badA[t] = nbad;
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batch_point_pass_mixed(BatchDev b) {
+    for (int t = blockIdx.x; t < b.nptiles; t += gridDim.x) {
+        const Tile tile = b.ptiles[t];
+        const Ctl& ctl = b.ctls[tile.inst];
+        if (inst_skip(ctl)) continue;
+        const HydroConst& c = b.consts[tile.inst];
+        const int cur = ctl.cycle & 1;
+        for (int64_t p = (int64_t)tile.beg + threadIdx.x; p < tile.end; p += kBatchThreads)
+            pass_b_mixed_point(b.a, c, cur, ctl.dt, p);
+    }
 }
 
 // ---------------------------------------------------------------------
@@ -812,6 +873,16 @@ cudaError_t prepare_pass_a_rows_mixed(bool learned, int32_t rect_nzx, int32_t nu
     const int64_t nt = rows::num_tiles<kZoneThreadsZT>(rect_nzx, numz);
     return learned ? rows::prepare(pass_a_mixed_rows<true>, kZoneThreadsZT, kRowsASmem, nt, nsm, grid)
                    : rows::prepare(pass_a_mixed_rows<false>, kZoneThreadsZT, kRowsASmem, nt, nsm, grid);
+}
+
+void launch_batch_pass_a_mixed(const BatchDev& b, bool all_quads, cudaStream_t stream) {
+    const int grid = b.nztiles > 1 ? b.nztiles : 1;
+    if (all_quads) batch_pass_a_mixed<true><<<grid, kBatchZT, 0, stream>>>(b);
+    else batch_pass_a_mixed<false><<<grid, kBatchZT, 0, stream>>>(b);
+}
+
+void launch_batch_point_pass_mixed(const BatchDev& b, int grid, cudaStream_t stream) {
+    batch_point_pass_mixed<<<grid, kBatchThreads, 0, stream>>>(b);
 }
 
 cudaError_t prepare_learned_kernels() {

@@ -122,9 +122,42 @@ def test_seeded_batch_workload_subset_matches_single_runs_bitwise():
     assert all(abs(b.scalars(i)["time"] - 0.5) < 1e-12 for i in range(len(texts)))
 
 
-def test_batch_rejects_mixed_precision():
+def _with_precision(texts, precision):
+    out = []
+    for t in texts:
+        d = pb.Deck(text=t)
+        d.set("precision", precision)
+        out.append(d)
+    return out
+
+
+def test_mixed_batch_matches_single_mixed_runs_bitwise():
+    """The mixed-precision cycle in a batch: every instance (quad and pie
+    meshes together) ends exactly as its own single-mesh mixed run."""
+    texts = instance_decks()
+    ref = []
+    for d in _with_precision(texts, "mixed"):
+        h = pb.Hydro(pb.Mesh(deck=d), d.params())
+        s = h.run()
+        ref.append((s, {k: h.download(k) for k in STATE}))
+        h.close()
+    decks = _with_precision(texts, "mixed")
+    b = pb.Batch([pb.Mesh(deck=d) for d in decks], [d.params() for d in decks])
+    assert b.run() == 0
+    check_batch(b, ref)
+    # and differs from the FP64 batch: the instances really ran the mixed cycle
+    fp = single_runs(texts[:1])
+    assert b.download(0, "ze").tobytes() != fp[0][1]["ze"].tobytes()
+
+
+def test_batch_rejects_learned_and_mixed_precisions():
     d = pb.Deck(text=sedov(16, tstop=0.01))
-    d.set("precision", "mixed")
+    d.set("precision", "learned")
     with pytest.raises(pb.PntError) as e:
         pb.Batch([pb.Mesh(deck=d)], [d.params()])
+    assert e.value.status == pb.PNT_ERR_UNSUPPORTED
+    d1, d2 = pb.Deck(text=sedov(16, tstop=0.01)), pb.Deck(text=sedov(16, tstop=0.01))
+    d2.set("precision", "mixed")
+    with pytest.raises(pb.PntError) as e:
+        pb.Batch([pb.Mesh(deck=d1), pb.Mesh(deck=d2)], [d1.params(), d2.params()])
     assert e.value.status == pb.PNT_ERR_UNSUPPORTED
