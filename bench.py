@@ -64,6 +64,14 @@ PASS_A_TRAFFIC_PER_ZONE = {"learned": (109.737e6 + 88.343e6) / 1048576,
                            "fp64": (125.973e6 + 130.137e6) / 1048576}
 
 
+# FP64 thread-instructions a zone of one FP64 pass A launch (ncu
+# sm__sass_thread_inst_executed_op_fp64_pred_on, 1024^2 Sedov at cycle
+# 16000: profiles/pass_a_fp64_sedov1024.md), and the B200's FP64 rate a
+# clock per SM (sm__sass_thread_inst_executed_op_dfma_pred_on peak)
+FP64_PASS_A_INST_PER_ZONE = 907.6
+FP64_INST_PER_CLOCK_PER_SM = 64
+
+
 def algorithmic_bytes(nump, nums, numz):
     """Compulsory HBM bytes of the 3-pass schedule (per cycle and per pass)."""
     a = 32 * nump + 44 * numz + 52 * nums   # pass A: px0,pu0; 4 zone fields + offsets; mapsp1,smf; 3 side outputs; zp
@@ -749,6 +757,22 @@ def main():
             d["closure"] = kms[4]
         return d
 
+    def fp64_pipe_roofline(ms, nz):
+        """The FP64 pass A against the FP64 pipe: its FP64 instructions (ncu
+        count a zone x zones) per second over 64 a clock per SM."""
+        nsm = torch.cuda.get_device_properties(local_rank).multi_processor_count
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                mhz = float(json.load(f)["sm_max_mhz"])
+        except Exception:
+            mhz = 1965.0
+        peak = FP64_INST_PER_CLOCK_PER_SM * nsm * mhz * 1e6 / 1e12
+        ach = FP64_PASS_A_INST_PER_ZONE * nz / (ms / 1e3) / 1e12
+        return {"bound": "fp64 pipe", "kernel": "pass A (fp64)", "achieved": ach, "peak": peak,
+                "unit": "T FP64 thread-instructions/s", "frac": ach / peak, "launch_ms": ms,
+                "note": "FP64 instructions a zone from profiles/pass_a_fp64_sedov1024.md (1024^2 at cycle "
+                        "16000); the count depends on how much of the mesh is quiescent"}
+
     kms_head = res[args.precision]["kernel_ms"]
     dom = int(np.argmax(kms_head[:3]))
     if args.precision in ("mixed", "learned"):
@@ -809,6 +833,7 @@ def main():
                          "traffic_note": "ncu DRAM read+write of one pass A launch at 1024^2 (cycle 16000), "
                                          "scaled by the zone count (writes still in L2 at the kernel's end "
                                          "are not counted)"},
+            "roofline_fp64_pass_a": fp64_pipe_roofline(res["fp64"]["kernel_ms"][0], numz),
             "roofline_cycle": {"achieved": ach_cycle, "peak": hbm, "unit": "GB/s", "frac": ach_cycle / hbm,
                                "algorithmic_bytes_per_cycle": ab["cycle"],
                                "note": "FP64 schedule bytes B = 164 Np + 100 Ns + 104 Nz for every path"},
