@@ -381,10 +381,39 @@ __device__ __forceinline__ void pass_a_zone_thread(const DevArrays& a, const Hyd
 // ---------------------------------------------------------------------
 // Pass B, one point
 // ---------------------------------------------------------------------
+// The point from its corner sums m (mass) and f (force): applyFixedBC per
+// plane in deck order (Hydro.cc:773-798, HydroBC.cc:150-182), calcAccel
+// (Hydro.cc:1235-1254, pa = f * (1 / max(m, 1e-99))) and advPosFull
+// (:1281-1306).  Written with explicit round-to-nearest operations, so the
+// result does not depend on the including file's contraction flags: the
+// FP64 and mixed cycles, the batch and the fused row-tile pass all advance
+// a point bit-identically from the same sums.
+__device__ __forceinline__ double2 project_rn(double2 v, double ux, double uy) {
+    const double d = __dadd_rn(__dmul_rn(v.x, ux), __dmul_rn(v.y, uy));
+    return mk(__dsub_rn(v.x, __dmul_rn(ux, d)), __dsub_rn(v.y, __dmul_rn(uy, d)));
+}
+__device__ __forceinline__ void advance_point(const HydroConst& c, double dt, unsigned mask, double m, double2 f,
+                                              double2 x0, double2 u0, double2& x, double2& u) {
+    if (mask) {
+        for (int b = 0; b < c.nbc; ++b) {
+            if (mask & (1u << b)) {
+                u0 = project_rn(u0, c.vfix[b][0], c.vfix[b][1]);
+                f = project_rn(f, c.vfix[b][0], c.vfix[b][1]);
+            }
+        }
+    }
+    const double rinv = __ddiv_rn(1., dmax(m, 1.e-99));
+    const double2 pa = mk(__dmul_rn(f.x, rinv), __dmul_rn(f.y, rinv));
+    u = mk(__dadd_rn(u0.x, __dmul_rn(pa.x, dt)), __dadd_rn(u0.y, __dmul_rn(pa.y, dt)));
+    const double dth = __dmul_rn(dt, 0.5);
+    x = mk(__dadd_rn(x0.x, __dmul_rn(__dadd_rn(u0.x, u.x), dth)),
+           __dadd_rn(x0.y, __dmul_rn(__dadd_rn(u0.y, u.y), dth)));
+}
+
 __device__ __forceinline__ void pass_b_point(const DevArrays& a, const HydroConst& c, int cur, double dt,
                                              int64_t p) {
     const double2 x0 = a.px[cur][p];
-    double2 u0 = a.pu[cur][p];
+    const double2 u0 = a.pu[cur][p];
     // corner mass and force, ascending side order from zero (Hydro.cc:1100-1116, :1175-1192)
     const int32_t o0 = a.poff[p], o1 = a.poff[p + 1];
     double m = 0.;
@@ -395,20 +424,8 @@ __device__ __forceinline__ void pass_b_point(const DevArrays& a, const HydroCons
         const double2 cf = a.cforce[s];
         f = mk(__dadd_rn(f.x, cf.x), __dadd_rn(f.y, cf.y));
     }
-    // applyFixedBC per plane in deck order (Hydro.cc:773-798, HydroBC.cc:150-182)
-    const unsigned mask = a.bcmask[p];
-    if (mask) {
-        for (int b = 0; b < c.nbc; ++b) {
-            if (mask & (1u << b)) {
-                u0 = project(u0, c.vfix[b][0], c.vfix[b][1]);
-                f = project(f, c.vfix[b][0], c.vfix[b][1]);
-            }
-        }
-    }
-    // calcAccel (Hydro.cc:1235-1254), advPosFull (:1281-1306)
-    const double2 pa = sdiv(f, dmax(m, 1.e-99));
-    const double2 u = add(u0, smul(dt, pa));
-    const double2 x = add(x0, smul(dt * 0.5, add(u0, u)));
+    double2 x, u;
+    advance_point(c, dt, a.bcmask[p], m, f, x0, u0, x, u);
     a.px[cur ^ 1][p] = x;
     a.pu[cur ^ 1][p] = u;
 }

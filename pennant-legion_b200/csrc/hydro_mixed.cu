@@ -582,29 +582,18 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_ROWS_A_MIN_BLOCKS) pass_a_
 __device__ __forceinline__ void pass_b_mixed_point(const DevArrays& a, const HydroConst& c, int cur, double dt,
                                                    int64_t p) {
     const double2 x0 = a.px[cur][p];
-    double2 u0 = a.pu[cur][p];
+    const double2 u0 = a.pu[cur][p];
     const int32_t o0 = a.poff[p], o1 = a.poff[p + 1];
     double m = 0.;
     double2 f = mk(0., 0.);
     for (int32_t i = o0; i < o1; ++i) {
         const int32_t s = __ldg(a.pcorner + i);
-        m += (double)a.cmass_f[s];
+        m = __dadd_rn(m, (double)a.cmass_f[s]);
         const float2 cf = a.cforce_f[s];
-        f = mk(f.x + (double)cf.x, f.y + (double)cf.y);
+        f = mk(__dadd_rn(f.x, (double)cf.x), __dadd_rn(f.y, (double)cf.y));
     }
-    const unsigned mask = a.bcmask[p];
-    if (mask) {
-        for (int b = 0; b < c.nbc; ++b) {
-            if (mask & (1u << b)) {
-                u0 = project(u0, c.vfix[b][0], c.vfix[b][1]);
-                f = project(f, c.vfix[b][0], c.vfix[b][1]);
-            }
-        }
-    }
-    const double minv = 1. / dmax(m, 1.e-99);
-    const double2 pa = mk(f.x * minv, f.y * minv);
-    const double2 u = add(u0, smul(dt, pa));
-    const double2 x = add(x0, smul(dt * 0.5, add(u0, u)));
+    double2 x, u;
+    fp64::advance_point(c, dt, a.bcmask[p], m, f, x0, u0, x, u);
     a.px[cur ^ 1][p] = x;
     a.pu[cur ^ 1][p] = u;
 }
