@@ -62,6 +62,18 @@ def test_mixed_leblanc_shock_tube():
     assert max(err.values()) <= L1_BOUND, err
 
 
+@pytest.mark.timeout(300)
+def test_mixed_leblanc_full_size_config():
+    """The mixed-precision workload at its full size: the Leblanc-type tube
+    on 2880 x 288 zones over [0, 9] x [0, 0.9] to t = 6.0 (~9300 cycles a
+    path), the mixed cycle against the FP64 cycle; the same deck as
+    decks/leblanc2880x288.pnt and bench.py --workload leblanc."""
+    s64, s32, err = compare(leblanc(2880, 288, 6.0))
+    assert abs(s32["time"] - 6.0) < 1e-12 and abs(s64["time"] - 6.0) < 1e-12
+    assert s64["cycle"] > 9000 and s32["cycle"] > 9000
+    assert max(err.values()) <= L1_BOUND, err
+
+
 def test_mixed_pie_noh():
     """Noh on the pie mesh (3-sided zones and 3-degree corners at the centre)
     up to cycle 150, before the stagnation zone at the origin starts to
