@@ -372,7 +372,8 @@ __global__ void __launch_bounds__(kMlpRows, 1) closure_forward_kernel(const uint
     float f[kClIn];
     for (int i = 0; i < kClIn; ++i) f[i] = (r < n) ? feats[r * kClIn + i] : 0.f;
     float y[4];
-    const bool ok = closure_mlp_block(smem, img, f, y);
+    const int64_t left = n - (int64_t)blockIdx.x * kMlpRows;
+    const bool ok = closure_mlp_block(smem, img, f, left < kMlpRows ? (int)left : kMlpRows, y);
     if (!ok && threadIdx.x == 0) atomicExch(err, 1);
     if (r < n)
         for (int i = 0; i < 4; ++i) out[r * 4 + i] = y[i];

@@ -73,15 +73,26 @@ constexpr int kImgBytes = 13056;
 __host__ __device__ constexpr int canon_off(int r, int k, int rows) { return (k >> 3) * rows * 16 + r * 16 + (k & 7) * 2; }
 
 // Deferred corners of the learned cycle: pass A records every zone that has
-// a compressing corner outside the dead zone (64 zones = 256 rows per
-// inference batch) with the raw FP32 data of each corner, relative to the
-// zone's first point: position, previous and next points, zone centre,
-// velocities of the point, previous and next points and the zone centre,
-// the mean corner velocity (absolute), the zone's sound speed and density,
-// and a flag (1 = deferred corner).  Per zone: first side, sides.
-constexpr int kRecFloats = 24;
-enum { kRecX = 0, kRecXp = 2, kRecXn = 4, kRecXz = 6, kRecU = 8, kRecUp = 10, kRecUn = 12, kRecUz = 14,
-       kRecUav = 16, kRecSs = 18, kRecRho = 19, kRecFlag = 20 };
+// a compressing corner outside the dead zone, kZoneRecF4 float4 (112 B) a
+// zone, in FP32 relative to the zone's first point:
+//   [0], [1]  positions of points 0..3 (x, y pairs)
+//   [2], [3]  velocities of points 0..3 (relative to point 0's)
+//   [4]       zone centre, mean velocity of the zone's points
+//   [5]       velocity of point 0 (absolute), sound speed, density
+//   [6]       first side, sides, deferred-corner bits (int bits), unused
+// (points 3 of a 3-sided zone are zeros).
+constexpr int kZoneRecF4 = 7;
+
+// Shared memory of the closure pass: the parameter image, the BF16 input
+// rows of up to kCpRows corners (four 128-row operand tiles), the hidden
+// activations of one 256-row run (two tiles), an mbarrier and the TMEM
+// address.  The outputs of a run overwrite the first 4 KB of its own two
+// input tiles (row r of the run at 16 r), whose MMAs are complete by then.
+constexpr int kCpRows = 512;
+constexpr int kCpA0 = 13312;
+constexpr int kCpH = kCpA0 + kCpRows * 32;
+constexpr int kCpBar = kCpH + 2 * 128 * 64 * 2;
+constexpr int kCpSmemBytes = kCpBar + 64;
 
 // Shared memory of the 256-row inference block.
 constexpr int kMlpRows = 256;
@@ -161,9 +172,13 @@ __device__ __forceinline__ float tanh_approx(float x) {
     asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
+// Every rounding written out: the same bits in every kernel that inlines
+// it, whatever the compiler's contraction flags.
 __device__ __forceinline__ float gelu_fast(float x) {
-    const float u = kGeluC * (x + kGeluA * x * x * x);
-    return 0.5f * x * (1.f + tanh_approx(u));
+    const float p = __fmaf_rn(__fmul_rn(kGeluA, __fmul_rn(x, x)), x, x);   // x + a x^3
+    const float th = tanh_approx(__fmul_rn(kGeluC, p));
+    const float hx = __fmul_rn(0.5f, x);
+    return __fmaf_rn(hx, th, hx);
 }
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
@@ -272,95 +287,113 @@ __device__ __forceinline__ void mlp_hidden_epilogue(uint32_t tacc, const float* 
         uint32_t w[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i)
-            w[i] = pack_bf16(gelu_fast(v[2 * i] + bias[16 * c + 2 * i]), gelu_fast(v[2 * i + 1] + bias[16 * c + 2 * i + 1]));
+            w[i] = pack_bf16(gelu_fast(__fadd_rn(v[2 * i], bias[16 * c + 2 * i])),
+                             gelu_fast(__fadd_rn(v[2 * i + 1], bias[16 * c + 2 * i + 1])));
         // k = 16c..16c+7 is K chunk 2c, k = 16c+8.. chunk 2c+1 (128 rows: 2048 B apart)
         *reinterpret_cast<uint4*>(hrow + (2 * c) * 2048) = make_uint4(w[0], w[1], w[2], w[3]);
         *reinterpret_cast<uint4*>(hrow + (2 * c + 1) * 2048) = make_uint4(w[4], w[5], w[6], w[7]);
     }
 }
 
-// The network on the kMlpRows (256) rows of a CTA of 256 threads: thread t
-// owns row t (row t % 128 of M tile t / 128, whose accumulator is TMEM lane
-// t % 128).  Every thread of the CTA calls setup once, rows once per batch
-// of 256 rows, and teardown once.  smem: kMlpSmemBytes of dynamic shared
-// memory (16-byte aligned); gimg: the parameter image in global memory.
+// Tensor-core state of a CTA running the network.  Every thread of the CTA
+// calls setup once, the row functions once per batch, and teardown once.
 //
 // Tensor-core waits are bounded.  Once a wait runs out on any thread, the
 // CTA agrees on it at its next barrier (__syncthreads_and) and issues no
 // further MMA, commit or TMEM load: the rows of that batch and of every
-// later one come out as zeros, and teardown waits (bounded again) for the
-// last commit issued, which covers every MMA still in flight, before it
-// frees the TMEM columns.
+// later one get no output, and teardown waits (bounded again) for the last
+// commit issued, which covers every MMA still in flight, before it frees
+// the TMEM columns.
 struct MlpState {
-    uint32_t tbase;   // TMEM columns of the two accumulators
+    uint32_t tbase;   // TMEM columns of the accumulators (64 per 128-row M tile)
+    uint32_t ncols;   // TMEM columns allocated
     uint32_t phase;   // commits issued (each ends one mbarrier phase)
+    uint32_t bar;     // shared-memory address of the mbarrier
     bool ok;          // every tensor-core wait so far completed
 };
 
-__device__ __forceinline__ void closure_mlp_setup(uint8_t* smem, const uint8_t* __restrict__ gimg, MlpState& st) {
+// img: kImgBytes of shared memory (16-byte aligned) for the parameter image,
+// copied from gimg; bar: an mbarrier; tslot: where tcgen05.alloc writes the
+// TMEM address; ncols: TMEM columns to allocate (64 per M tile).
+__device__ __forceinline__ void closure_mlp_setup(uint8_t* img, const uint8_t* __restrict__ gimg, uint64_t* bar,
+                                                  uint32_t* tslot, uint32_t ncols, MlpState& st) {
     const int t = threadIdx.x;
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kSmBar + 8);
-    for (int i = t; i < kImgBytes / 16; i += kMlpRows)
-        reinterpret_cast<uint4*>(smem + kSmImg)[i] = __ldg(reinterpret_cast<const uint4*>(gimg) + i);
-    if (t == 0) mbar_init(smem_addr(smem + kSmBar), 1);
+    for (int i = t; i < kImgBytes / 16; i += blockDim.x)
+        reinterpret_cast<uint4*>(img)[i] = __ldg(reinterpret_cast<const uint4*>(gimg) + i);
+    if (t == 0) mbar_init(smem_addr(bar), 1);
     if ((t >> 5) == 0) {
-        tmem_alloc(smem_addr(tslot), kTmemCols);
+        tmem_alloc(smem_addr(tslot), ncols);
         tmem_relinquish();
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     st.tbase = *tslot;
+    st.ncols = ncols;
     st.phase = 0;
+    st.bar = smem_addr(bar);
     st.ok = true;
 }
 
-// f: this row's raw inputs; out: its 4 outputs, denormalised (zero after a
-// wait ran out, in this batch or an earlier one).
-__device__ __forceinline__ void closure_mlp_rows(uint8_t* smem, MlpState& st, const float* f, float* out) {
+// Row `slot` of a staged input operand a0 (128-row tiles of 4 KB): this
+// corner's inputs, normalised, in BF16.
+__device__ __forceinline__ void closure_stage_row(uint8_t* a0, int slot, const float* f, const float* mean,
+                                                  const float* istd) {
+    float z[kClInPad];
+#pragma unroll
+    for (int i = 0; i < kClInPad; ++i) z[i] = (i < kClIn) ? __fmul_rn(__fsub_rn(f[i], mean[i]), istd[i]) : 0.f;
+    uint8_t* arow = a0 + (slot >> 7) * 4096 + (slot & 127) * 16;
+    *reinterpret_cast<uint4*>(arow) =
+        make_uint4(pack_bf16(z[0], z[1]), pack_bf16(z[2], z[3]), pack_bf16(z[4], z[5]), pack_bf16(z[6], z[7]));
+    *reinterpret_cast<uint4*>(arow + 2048) = make_uint4(pack_bf16(z[8], z[9]), pack_bf16(z[10], z[11]),
+                                                       pack_bf16(z[12], z[13]), pack_bf16(z[14], z[15]));
+}
+
+// The network on staged rows [base, base + 2 * 128) of the operand tiles at
+// a0 (its M tiles base / 128 and base / 128 + 1, the second only when more
+// than 128 of the n staged rows fall in the run; a CTA of 128 threads runs
+// one M tile), hidden activations in h (16 KB per M tile).  Thread t takes
+// row base + t (TMEM lane t % 128 of M tile t / 128), and warps without
+// staged rows skip the epilogues.  The output of row base + t
+// (denormalised) goes to float4 t of the run's first operand tile, whose
+// MMAs are complete by then.  Every thread of the CTA calls it; the caller
+// has staged the rows and issued fence_async_smem().  After a wait runs out
+// no further MMA is issued and the run's outputs are not written.
+__device__ __forceinline__ void closure_mlp_run(const uint8_t* img, uint8_t* a0, uint8_t* h, MlpState& st, int base,
+                                                int n) {
     const int t = threadIdx.x;
     const int warp = t >> 5;
     const int tile = t >> 7;
     const int row = t & 127;
-    const uint32_t mbar = smem_addr(smem + kSmBar);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) out[i] = 0.f;
-    // a wait that ran out earlier on any thread: no more tensor-core work
-    st.ok = __syncthreads_and(st.ok) != 0;
-    if (!st.ok) return;
-    // normalised inputs -> this row of the layer-1 A operand
-    {
-        const float* mean = reinterpret_cast<const float*>(smem + kImgFMean);
-        const float* istd = reinterpret_cast<const float*>(smem + kImgFIstd);
-        float z[kClInPad];
-#pragma unroll
-        for (int i = 0; i < kClInPad; ++i) z[i] = (i < kClIn) ? (f[i] - mean[i]) * istd[i] : 0.f;
-        uint8_t* arow = smem + kSmA0 + tile * 4096 + row * 16;
-        *reinterpret_cast<uint4*>(arow) =
-            make_uint4(pack_bf16(z[0], z[1]), pack_bf16(z[2], z[3]), pack_bf16(z[4], z[5]), pack_bf16(z[6], z[7]));
-        *reinterpret_cast<uint4*>(arow + 2048) = make_uint4(pack_bf16(z[8], z[9]), pack_bf16(z[10], z[11]),
-                                                           pack_bf16(z[12], z[13]), pack_bf16(z[14], z[15]));
-    }
-    fence_async_smem();
+    const int mt = (n - base > 128 && blockDim.x > 128) ? 2 : 1;
+    const bool live = base + 32 * warp < n;   // warp-uniform
+    const uint32_t mbar = st.bar;
+    // the previous run's TMEM loads finish before this run's MMAs overwrite
+    // the accumulators; the staged rows are visible to the tensor cores
     tc_fence_before();
-    __syncthreads();
+    st.ok = __syncthreads_and(st.ok) != 0;
     tc_fence_after();
+    if (!st.ok) return;
     const uint32_t tbase = st.tbase;
     const uint32_t tacc = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(tile * 64);
-    const uint32_t sb = smem_addr(smem);
+    const uint32_t si = smem_addr(img);
+    const uint32_t sh = smem_addr(h);
+    uint8_t* out_tile = a0 + (base >> 7) * 4096;
+    const uint32_t sa = smem_addr(out_tile);
+    const float* fimg = reinterpret_cast<const float*>(img);
 
-    // layer 1: [128 x 16] x [16 x 64] per tile
+    // layer 1: [128 x 16] x [16 x 64] per M tile
     if (t == 0) {
-        for (int j = 0; j < 2; ++j)
-            umma_bf16(tbase + j * 64, umma_desc(sb + kSmA0 + j * 4096, 2048, 128), umma_desc(sb + kImgW1, 1024, 128),
+        for (int j = 0; j < mt; ++j)
+            umma_bf16(tbase + j * 64, umma_desc(sa + j * 4096, 2048, 128), umma_desc(si + kImgW1, 1024, 128),
                       umma_idesc_bf16(128, 64), 0u);
         umma_commit(mbar);
     }
     ++st.phase;
-    bool w = mbar_wait(mbar, (st.phase - 1) & 1);
+    bool w = __all_sync(0xffffffffu, mbar_wait(mbar, (st.phase - 1) & 1));
     tc_fence_after();
-    uint8_t* hrow = smem + kSmH + tile * 16384 + row * 16;
-    if (w) mlp_hidden_epilogue(tacc, reinterpret_cast<const float*>(smem + kImgB1), hrow);
+    uint8_t* hrow = h + tile * 16384 + row * 16;
+    if (w && live) mlp_hidden_epilogue(tacc, fimg + kImgB1 / 4, hrow);
     fence_async_smem();
     tc_fence_before();
     st.ok = __syncthreads_and(w) != 0;
@@ -369,16 +402,16 @@ __device__ __forceinline__ void closure_mlp_rows(uint8_t* smem, MlpState& st, co
 
     // layer 2: [128 x 64] x [64 x 64]
     if (t == 0) {
-        for (int j = 0; j < 2; ++j)
+        for (int j = 0; j < mt; ++j)
             for (int kb = 0; kb < 4; ++kb)
-                umma_bf16(tbase + j * 64, umma_desc(sb + kSmH + j * 16384 + kb * 4096, 2048, 128),
-                          umma_desc(sb + kImgW2 + kb * 2048, 1024, 128), umma_idesc_bf16(128, 64), kb > 0 ? 1u : 0u);
+                umma_bf16(tbase + j * 64, umma_desc(sh + j * 16384 + kb * 4096, 2048, 128),
+                          umma_desc(si + kImgW2 + kb * 2048, 1024, 128), umma_idesc_bf16(128, 64), kb > 0 ? 1u : 0u);
         umma_commit(mbar);
     }
     ++st.phase;
-    w = mbar_wait(mbar, (st.phase - 1) & 1);
+    w = __all_sync(0xffffffffu, mbar_wait(mbar, (st.phase - 1) & 1));
     tc_fence_after();
-    if (w) mlp_hidden_epilogue(tacc, reinterpret_cast<const float*>(smem + kImgB2), hrow);
+    if (w && live) mlp_hidden_epilogue(tacc, fimg + kImgB2 / 4, hrow);
     fence_async_smem();
     tc_fence_before();
     st.ok = __syncthreads_and(w) != 0;
@@ -387,57 +420,73 @@ __device__ __forceinline__ void closure_mlp_rows(uint8_t* smem, MlpState& st, co
 
     // layer 3: [128 x 64] x [64 x 16] (4 outputs used)
     if (t == 0) {
-        for (int j = 0; j < 2; ++j)
+        for (int j = 0; j < mt; ++j)
             for (int kb = 0; kb < 4; ++kb)
-                umma_bf16(tbase + j * 64, umma_desc(sb + kSmH + j * 16384 + kb * 4096, 2048, 128),
-                          umma_desc(sb + kImgW3 + kb * 512, 256, 128), umma_idesc_bf16(128, 16), kb > 0 ? 1u : 0u);
+                umma_bf16(tbase + j * 64, umma_desc(sh + j * 16384 + kb * 4096, 2048, 128),
+                          umma_desc(si + kImgW3 + kb * 512, 256, 128), umma_idesc_bf16(128, 16), kb > 0 ? 1u : 0u);
         umma_commit(mbar);
     }
     ++st.phase;
-    w = mbar_wait(mbar, (st.phase - 1) & 1);
+    w = __all_sync(0xffffffffu, mbar_wait(mbar, (st.phase - 1) & 1));
     tc_fence_after();
-    if (w) {
+    if (w && live) {
         float y[4];
         tmem_ld4(tacc, y);
-        const float* b3 = reinterpret_cast<const float*>(smem + kImgB3);
-        const float* tmean = reinterpret_cast<const float*>(smem + kImgTMean);
-        const float* tstd = reinterpret_cast<const float*>(smem + kImgTStd);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) out[i] = (y[i] + b3[i]) * tstd[i] + tmean[i];
+        const float* b3 = fimg + kImgB3 / 4;
+        const float* tmean = fimg + kImgTMean / 4;
+        const float* tstd = fimg + kImgTStd / 4;
+        if (base + t < n)
+            reinterpret_cast<float4*>(out_tile)[t] = make_float4(
+                __fmaf_rn(__fadd_rn(y[0], b3[0]), tstd[0], tmean[0]), __fmaf_rn(__fadd_rn(y[1], b3[1]), tstd[1], tmean[1]),
+                __fmaf_rn(__fadd_rn(y[2], b3[2]), tstd[2], tmean[2]), __fmaf_rn(__fadd_rn(y[3], b3[3]), tstd[3], tmean[3]));
     }
-    // this thread's view; the next batch's (or teardown's) barrier makes it
+    // this thread's view; the next run's (or teardown's) barrier makes it
     // the CTA's
     st.ok = w;
-    // the next batch's layer-1 MMA overwrites these accumulators after the
-    // barrier that follows its input writes
     tc_fence_before();
 }
 
 // Frees the TMEM columns.  After a wait that ran out, first waits (bounded)
 // for the last commit issued, so no MMA still writes the columns; returns
 // false on every thread if any tensor-core wait ran out.
-__device__ __forceinline__ bool closure_mlp_teardown(uint8_t* smem, MlpState& st) {
+__device__ __forceinline__ bool closure_mlp_teardown(MlpState& st) {
     tc_fence_before();
     const bool ok = __syncthreads_and(st.ok) != 0;
     if (!ok && st.phase > 0) {
-        mbar_wait(smem_addr(smem + kSmBar), (st.phase - 1) & 1);
+        mbar_wait(st.bar, (st.phase - 1) & 1);
         tc_fence_before();
         __syncthreads();
     }
     if ((threadIdx.x >> 5) == 0) {
         tc_fence_after();
-        tmem_dealloc(st.tbase, kTmemCols);
+        tmem_dealloc(st.tbase, st.ncols);
     }
     return ok;
 }
 
-// One batch of 256 rows (the standalone inference).
+// One batch of up to 256 rows in a CTA of 256 threads (the standalone
+// inference): thread t's inputs f -> its outputs (zeros for rows >= n or
+// after a wait ran out).  smem: kMlpSmemBytes of dynamic shared memory
+// (16-byte aligned); gimg: the parameter image in global memory.
 __device__ __forceinline__ bool closure_mlp_block(uint8_t* smem, const uint8_t* __restrict__ gimg, const float* f,
-                                                  float* out) {
+                                                  int n, float* out) {
     MlpState st;
-    closure_mlp_setup(smem, gimg, st);
-    closure_mlp_rows(smem, st, f, out);
-    return closure_mlp_teardown(smem, st);
+    closure_mlp_setup(smem + kSmImg, gimg, reinterpret_cast<uint64_t*>(smem + kSmBar),
+                      reinterpret_cast<uint32_t*>(smem + kSmBar + 8), kTmemCols, st);
+    const int t = threadIdx.x;
+    if (t < n)
+        closure_stage_row(smem + kSmA0, t, f, reinterpret_cast<const float*>(smem + kImgFMean),
+                          reinterpret_cast<const float*>(smem + kImgFIstd));
+    fence_async_smem();
+    closure_mlp_run(smem + kSmImg, smem + kSmA0, smem + kSmH, st, 0, n);
+    const bool ok = closure_mlp_teardown(st);   // its barrier publishes the outputs
+    const float4 y = reinterpret_cast<const float4*>(smem + kSmA0)[t];
+    const bool have = ok && t < n;
+    out[0] = have ? y.x : 0.f;
+    out[1] = have ? y.y : 0.f;
+    out[2] = have ? y.z : 0.f;
+    out[3] = have ? y.w : 0.f;
+    return ok;
 }
 
 }  // namespace pnt

@@ -826,11 +826,9 @@ pnt_status pnt_hydro_set_closure(pnt_hydro* h, const pnt_closure* c, int32_t mod
     if (!h->a.closure_img) {
         uint8_t* img = nullptr;
         float* rec = nullptr;
-        int2* hdr = nullptr;
         int32_t* nrec = nullptr;
         if (pnt_status st = h->alloc(&img, kImgBytes)) return st;
-        if (pnt_status st = h->alloc(&rec, (size_t)h->numz * 4 * kRecFloats)) return st;
-        if (pnt_status st = h->alloc(&hdr, (size_t)h->numz)) return st;
+        if (pnt_status st = h->alloc(&rec, (size_t)h->numz * kZoneRecF4 * 4)) return st;
         if (pnt_status st = h->alloc(&nrec, 1)) return st;
         CUDA_TRY(cudaMemset(nrec, 0, sizeof(int32_t)));
         CUDA_TRY(prepare_learned_kernels());
@@ -838,10 +836,8 @@ pnt_status pnt_hydro_set_closure(pnt_hydro* h, const pnt_closure* c, int32_t mod
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
         h->a.closure_img = img;
         h->a.closure_rec = rec;
-        h->a.closure_zhdr = hdr;
         h->a.closure_nrec = nrec;
-        // 128 TMEM columns and 54 KB of shared memory per CTA; 3 per SM (4, at
-        // 64 registers, measured slower: more CTAs pay the image setup)
+        // 128 TMEM columns and 61 KB of shared memory per CTA; 3 per SM
         h->a.closure_grid = PNT_CLOSURE_CTAS_PER_SM * nsm;
     }
     // the image lives in this object: a copy of the closure's, with the mode

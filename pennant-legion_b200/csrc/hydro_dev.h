@@ -90,10 +90,9 @@ struct DevArrays {
     // class counters [class][64] (closure_dev.cuh)
     const uint8_t* closure_img;
     unsigned long long* closure_counts;
-    // zones whose corners the closure pass evaluates: records [numz][4][24],
-    // headers (first side, sides) [numz], and this cycle's count
+    // zones whose corners the closure pass evaluates: records
+    // [numz][kZoneRecF4] float4 (closure_dev.cuh) and this cycle's count
     float* closure_rec;
-    int2* closure_zhdr;
     int32_t* closure_nrec;
     int32_t closure_grid;   // CTAs of the persistent closure pass
     int32_t gridC;          // CTAs of the persistent pass C (pass_c_staged.cuh)

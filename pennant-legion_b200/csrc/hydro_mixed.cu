@@ -186,14 +186,23 @@ struct SideSpill {
     __device__ __forceinline__ float2& sft(int k) const { return sft_[k * kZoneThreadsZT + t]; }
 };
 
+// Where the learned cycle's pass A records a zone for the closure: record
+// i at base + (i & mask) * kZoneRecF4, i from an atomic counter (global or
+// shared memory).
+struct RecSink {
+    int* count;
+    float4* base;
+    int mask;
+};
+
 // nbad counts the zone's inverted sides; cnt[3]: its corners without
 // compression, in the dead zone, in an acute zone (learned cycle).
 // in: the zone's inputs (fp64::GlobalZoneIn, or a row tile's shared-memory
-// stage).
+// stage); sink: where a zone with deferred corners is recorded (learned).
 template <int N, bool kLearned, typename In>
 __device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const HydroConst& c, const In& in, int cur,
                                                   double dt, int64_t z, int64_t s0, double& zdthyd, int& nbad,
-                                                  int* cnt, const SideSpill& sp) {
+                                                  int* cnt, const SideSpill& sp, const RecSink& sink = RecSink{}) {
     double2 xp[N];
     float2 uf[N];
     double mf[N];
@@ -381,29 +390,18 @@ __device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const Hydr
             const int lane = threadIdx.x & 31;
             const int leader = __ffs(m) - 1;
             int base = 0;
-            if (lane == leader) base = atomicAdd(a.closure_nrec, __popc(m));
+            if (lane == leader) base = atomicAdd(sink.count, __popc(m));
             base = __shfl_sync(m, base, leader);
             const int idx = base + __popc(m & ((1u << lane) - 1u));
-#pragma unroll
-            for (int k = 0; k < N; ++k) {
-                const int pk = (k == 0) ? N - 1 : k - 1;
-                const int nk = (k + 1 == N) ? 0 : k + 1;
-                const float2 up1 = fmul(0.5f, fadd(uf[k], uf[nk]));
-                const float2 up3 = fmul(0.5f, fadd(uf[pk], uf[k]));
-                const float2 uav = fadd(fmul(0.25f, fadd(fadd(fadd(uf[k], up1), zuc), up3)), f2(uref));
-                float4* rec = reinterpret_cast<float4*>(a.closure_rec + ((int64_t)idx * 4 + k) * kRecFloats);
-                rec[0] = make_float4(r[k].x, r[k].y, r[pk].x, r[pk].y);
-                rec[1] = make_float4(r[nk].x, r[nk].y, zc.x, zc.y);
-                rec[2] = make_float4(uf[k].x, uf[k].y, uf[pk].x, uf[pk].y);
-                rec[3] = make_float4(uf[nk].x, uf[nk].y, zuc.x, zuc.y);
-                rec[4] = make_float4(uav.x, uav.y, zssf, zrpf);
-                rec[5] = make_float4((defer_bits >> k) & 1u ? 1.f : 0.f, 0.f, 0.f, 0.f);
-            }
-            if (N == 3) {   // the idle fourth row of a 3-sided zone
-                float4* rec = reinterpret_cast<float4*>(a.closure_rec + ((int64_t)idx * 4 + 3) * kRecFloats);
-                for (int i = 0; i < kRecFloats / 4; ++i) rec[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-            a.closure_zhdr[idx] = make_int2((int)s0, N);
+            float4* rec = sink.base + (int64_t)(idx & sink.mask) * kZoneRecF4;
+            const float2 r3 = (N == 4) ? r[N - 1] : fk(0.f, 0.f), u3 = (N == 4) ? uf[N - 1] : fk(0.f, 0.f);
+            rec[0] = make_float4(r[0].x, r[0].y, r[1].x, r[1].y);
+            rec[1] = make_float4(r[2].x, r[2].y, r3.x, r3.y);
+            rec[2] = make_float4(uf[0].x, uf[0].y, uf[1].x, uf[1].y);
+            rec[3] = make_float4(uf[2].x, uf[2].y, u3.x, u3.y);
+            rec[4] = make_float4(zc.x, zc.y, zuc.x, zuc.y);
+            rec[5] = make_float4((float)uref.x, (float)uref.y, zssf, zrpf);
+            rec[6] = make_float4(__int_as_float((int)s0), __int_as_float(N), __int_as_float((int)defer_bits), 0.f);
         }
     }
     // QCS::setForce (QCS.cc:331-380); in the learned cycle no corner outside
@@ -475,15 +473,16 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_MIXED_ZT_MIN_BLOCKS) pass_
     if (z < a.numz) {
         const int cur = ctl->cycle & 1;
         const double dt = ctl->dt;
+        const RecSink sink{a.closure_nrec, reinterpret_cast<float4*>(a.closure_rec), 0x7fffffff};
         if (kQuads) {
             const fp64::GlobalZoneIn in{a, cur, z, 4 * z};
-            pass_a_mixed_zone<4, kLearned>(a, c, in, cur, dt, z, 4 * z, zdthyd, bad, cnt, sp);
+            pass_a_mixed_zone<4, kLearned>(a, c, in, cur, dt, z, 4 * z, zdthyd, bad, cnt, sp, sink);
         } else {
             const int n = a.znump[z];
             const int64_t s0 = a.zfirst[z];
             const fp64::GlobalZoneIn in{a, cur, z, s0};
-            if (n == 4) pass_a_mixed_zone<4, kLearned>(a, c, in, cur, dt, z, s0, zdthyd, bad, cnt, sp);
-            else pass_a_mixed_zone<3, kLearned>(a, c, in, cur, dt, z, s0, zdthyd, bad, cnt, sp);
+            if (n == 4) pass_a_mixed_zone<4, kLearned>(a, c, in, cur, dt, z, s0, zdthyd, bad, cnt, sp, sink);
+            else pass_a_mixed_zone<3, kLearned>(a, c, in, cur, dt, z, s0, zdthyd, bad, cnt, sp, sink);
         }
     }
     __shared__ unsigned wcount[kLearned ? kZoneThreadsZT / 32 : 1][3];
@@ -503,6 +502,295 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_MIXED_ZT_MIN_BLOCKS) pass_
         }
     }
     fp64::block_to_cycle<true, kZoneThreadsZT>(a.cyc_red, zdthyd, nbad);
+}
+
+// ---------------------------------------------------------------------
+// The learned closure's corner work.  Pass A records every zone with
+// deferred corners (closure_dev.cuh: kZoneRecF4 float4 a zone).  A round
+// takes up to J * blockDim.x / 4 recorded zones, thread t corner t & 3 of
+// zones t / 4, t / 4 + blockDim.x / 4, ...  Each deferred corner is
+// classified (compression past rho_max or inputs out of distribution: plain
+// QCS, QCS.cc:116-327 in FP32 as in the mixed pass A; otherwise the
+// network); the network's corners of a round are packed into consecutive
+// rows of the tensor-core operand, so the network (tcgen05, closure_dev.cuh)
+// runs on those corners only.  A corner's QCS forces cqe1, cqe2 enter
+// QCS::setForce (QCS.cc:331-380) linearly: its side s gets
+// d1 = cw (cqe2 + ccos cqe1) / elen[s] and the previous side
+// d2 = cw (cqe1 + ccos cqe2) / elen[s3].  The corner force of side s,
+// ftot[s] - ftot[s3] (Hydro.cc:1159-1193), and sfp + sfq of side s then
+// change by
+//   dcforce[s] = d1(s) - d2(s) - d1(s3) + d2(s4),  dsftot[s] = d1(s) + d2(s4),
+// which only touch the recorded zone's own sides: no two records write the
+// same side, so the update is deterministic without atomics.
+// ---------------------------------------------------------------------
+
+// Corner k of a zone record; deferred = k is a corner of the zone and was
+// deferred by pass A.
+struct RecCorner {
+    float2 x, xpv, xn, xz, u, upv, un, uz, uav;
+    float css, rho;
+    int s0, n;
+    bool deferred;
+};
+
+__device__ __forceinline__ float2 sel4(int k, float2 a, float2 b, float2 c, float2 d) {
+    return k == 0 ? a : (k == 1 ? b : (k == 2 ? c : d));
+}
+
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+// A zone record as loaded (kZoneRecF4 float4).
+struct ZoneRec {
+    float4 q[kZoneRecF4];
+};
+__device__ __forceinline__ ZoneRec load_zone_rec(const float4* __restrict__ rec) {
+    ZoneRec r;
+#pragma unroll
+    for (int i = 0; i < kZoneRecF4; ++i) r.q[i] = rec[i];
+    return r;
+}
+
+__device__ __forceinline__ RecCorner rec_corner(const ZoneRec& zr, int k) {
+    const float4 q0 = zr.q[0], q1 = zr.q[1], q2 = zr.q[2], q3 = zr.q[3], q4 = zr.q[4], q5 = zr.q[5], q6 = zr.q[6];
+    RecCorner o;
+    o.s0 = __float_as_int(q6.x);
+    o.n = __float_as_int(q6.y);
+    const int n = o.n;
+    o.deferred = k < n && ((__float_as_int(q6.z) >> k) & 1);
+    const int pk = (k == 0) ? n - 1 : k - 1;
+    const int nk = (k + 1 >= n) ? 0 : k + 1;
+    const float2 r0 = fk(q0.x, q0.y), r1 = fk(q0.z, q0.w), r2 = fk(q1.x, q1.y), r3 = fk(q1.z, q1.w);
+    const float2 v0 = fk(q2.x, q2.y), v1 = fk(q2.z, q2.w), v2 = fk(q3.x, q3.y), v3 = fk(q3.z, q3.w);
+    o.x = sel4(k, r0, r1, r2, r3);
+    o.xpv = sel4(pk, r0, r1, r2, r3);
+    o.xn = sel4(nk, r0, r1, r2, r3);
+    o.u = sel4(k, v0, v1, v2, v3);
+    o.upv = sel4(pk, v0, v1, v2, v3);
+    o.un = sel4(nk, v0, v1, v2, v3);
+    o.xz = fk(q4.x, q4.y);
+    o.uz = fk(q4.z, q4.w);
+    // the mean corner velocity as pass A forms it (absolute)
+    const float2 up1 = fmul(0.5f, fadd(o.u, o.un)), up3 = fmul(0.5f, fadd(o.upv, o.u));
+    o.uav = fadd(fmul(0.25f, fadd(fadd(fadd(o.u, up1), o.uz), up3)), fk(q5.x, q5.y));
+    o.css = q5.z;
+    o.rho = q5.w;
+    return o;
+}
+
+// Corner k of the zone record zr: its class (-1: not deferred or in the
+// dead zone; kClassMlp, kClassFallback, kClassOod) and, when classified,
+// its inputs f, frame (cx, cy) and force scale rho D (a D + b c) in
+// frame[0..2].  img: the parameter image (shared memory).
+__device__ __forceinline__ int closure_classify(const ZoneRec& zr, int k, const uint8_t* img, float qa, float qb,
+                                                float* f, float* frame) {
+    const RecCorner q = rec_corner(zr, k);
+    float cx = 0.f, cy = 0.f, scale = 0.f;
+    if (!q.deferred ||
+        !closure_features<float>({q.x.x, q.x.y}, {q.xpv.x, q.xpv.y}, {q.xn.x, q.xn.y}, {q.xz.x, q.xz.y},
+                                 {q.u.x, q.u.y}, {q.upv.x, q.upv.y}, {q.un.x, q.un.y}, {q.uz.x, q.uz.y},
+                                 {q.uav.x, q.uav.y}, q.css, qa, qb, 0.f, f, cx, cy, scale))
+        return -1;
+    frame[0] = cx;
+    frame[1] = cy;
+    frame[2] = q.rho * scale;
+    const float* thr = reinterpret_cast<const float*>(img + kImgThr);
+    if (f[11] > thr[1]) return kClassFallback;   // rho_max
+    const float* mean = reinterpret_cast<const float*>(img + kImgFMean);
+    const float* istd = reinterpret_cast<const float*>(img + kImgFIstd);
+    float zmax = 0.f;
+#pragma unroll
+    for (int i = 0; i < kClIn; ++i) zmax = fmaxf(zmax, fabsf((f[i] - mean[i]) * istd[i]));
+    return (zmax > thr[2]) ? kClassOod : kClassMlp;   // ood_kappa
+}
+
+// The QCS forces of corner k of the record, as QCS::setForce distributes
+// them: d[0..1] = d1 to side k, d[2..3] = d2 to side k - 1.  how: 1 the
+// network's outputs y in the frame (cx, cy) scaled by frame[2], 2 plain
+// QCS (FP32 as in the mixed pass A), 0 none.
+__device__ __forceinline__ void closure_corner_forces(const ZoneRec& zr, int k, int how, float4 y, const float* frame,
+                                                      float qa, float qb, float* d) {
+    const RecCorner q = rec_corner(zr, k);
+    // corner geometry (QCS::setCornerDiv / setForce)
+    const float2 xc = q.x, xpv = q.xpv, xn = q.xn, xz = q.xz;
+    const float2 ex = fmul(0.5f, fadd(xc, xn));
+    const float2 xq3 = fmul(0.5f, fadd(xpv, xc));
+    const float cvolume = 0.5f * fcross(fsub(xz, xc), fsub(xq3, ex));
+    const float2 v1 = fsub(xq3, xc), v2 = fsub(ex, xc);
+    const float de1 = flen(fsub(xc, xpv)), de2 = flen(fsub(xn, xc));
+    const float rinv_de1 = 1.f / de1, rinv_el = 1.f / de2;
+    const float minelen = fminf(de1, de2);
+    float ccos = (minelen < 1.e-12f) ? 0.f : 4.f * fdot(v1, v2) / (de1 * de2);
+    float2 q1 = fk(0.f, 0.f), q2 = fk(0.f, 0.f);
+    if (how == 1) {
+        const float cx = frame[0], cy = frame[1], sc = frame[2];
+        q1 = fk((cx * y.x - cy * y.y) * sc, (cy * y.x + cx * y.y) * sc);
+        q2 = fk((cx * y.z - cy * y.w) * sc, (cy * y.z + cx * y.w) * sc);
+    } else if (how == 2) {
+        const float2 u = q.u, upv = q.upv, un = q.un, uz = q.uz, uav = q.uav;
+        const float2 up1 = fmul(0.5f, fadd(u, un)), up3 = fmul(0.5f, fadd(upv, u));
+        const float2 dxx1 = fmul(0.5f, fsub(fsub(fadd(ex, xz), xc), xq3));
+        const float2 dxx2 = fmul(0.5f, fsub(fsub(fadd(xz, xq3), xc), ex));
+        const float dx1 = flen(dxx1), dx2 = flen(dxx2);
+        const float test1 = fabsf(fdot(dxx1, uav) * dx2);
+        const float test2 = fabsf(fdot(dxx2, uav) * dx1);
+        const float rr = (test1 > test2) ? dx1 / dx2 : dx2 / dx1;
+        const float evol = fminf(sqrtf(4.f * cvolume * rr), 2.f * minelen);
+        const float du = sqrtf(fmaxf(flen2(fsub(fsub(fadd(up1, uz), u), up3)),
+                                     flen2(fsub(fsub(fadd(uz, up3), u), up1))));
+        const float ztmp2 = qa * du;
+        const float ztmp1 = qb * q.css;
+        const float crmu = (ztmp2 + sqrtf(ztmp2 * ztmp2 + ztmp1 * ztmp1)) * q.rho * evol;
+        q1 = fmul(crmu * rinv_de1, fsub(u, upv));
+        q2 = fmul(crmu * rinv_el, fsub(un, u));
+    }
+    const float ssin = 4.f * fcross(v1, v2) / (de1 * de2);
+    const float csin2 = (minelen < 1.e-12f) ? 1.f : ssin * ssin;
+    const float cw = (csin2 < 1.e-4f) ? 0.f : cvolume / csin2;
+    ccos = (csin2 < 1.e-4f) ? 0.f : ccos;
+    const float2 d1 = fmul(cw * rinv_el, fadd(q2, fmul(ccos, q1)));
+    const float2 d2 = fmul(cw * rinv_de1, fadd(q1, fmul(ccos, q2)));
+    d[0] = d1.x;
+    d[1] = d1.y;
+    d[2] = d2.x;
+    d[3] = d2.y;
+}
+
+// A CTA's closure state: the parameter image (shared memory), the packed
+// operand tiles and hidden activations (closure_mlp_run), the packed-row
+// counter (zero between rounds) and the class counters (network, fallback,
+// out of distribution) in shared memory.
+struct ClosureCtx {
+    const uint8_t* img;
+    uint8_t* a0;
+    uint8_t* h;
+    int* nrow;
+    unsigned* ncls;
+};
+
+// Zones zfirst .. zfirst + nz - 1 of the records rec_at(i); every thread of
+// the CTA calls it.
+template <int J, typename RecAt>
+__device__ __forceinline__ void closure_round(const DevArrays& a, const HydroConst& c, const ClosureCtx& x,
+                                              MlpState& st, RecAt&& rec_at, int zfirst, int nz) {
+    const int t = threadIdx.x, k = t & 3, lane = t & 31, g = lane & ~3;
+    const int zpj = (int)(blockDim.x >> 2);
+    const int mode = (int)reinterpret_cast<const float*>(x.img + kImgThr)[3];   // 0 network, 1 no force, 2 plain QCS
+    const float* mean = reinterpret_cast<const float*>(x.img + kImgFMean);
+    const float* istd = reinterpret_cast<const float*>(x.img + kImgFIstd);
+    const float qa = (float)(c.q2 * 0.25 * c.gammap1), qb = (float)c.q1;
+    // the previous round's readers of the operand tiles are done
+    __syncthreads();
+    int slot[J], how[J], s0[J], nsd[J];
+    float frame[J][3];
+    // every record of the round in flight before the first is used (into
+    // L1: no registers held)
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+        const int zl = j * zpj + (t >> 2);
+        if (j * zpj < nz && zl < nz) {
+            const float4* r = rec_at(zfirst + zl);
+            prefetch_l1(r);
+            prefetch_l1(r + kZoneRecF4 - 1);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+        slot[j] = -1;
+        how[j] = 0;
+        s0[j] = 0;
+        nsd[j] = 4;
+        if (j * zpj >= nz) continue;   // CTA-uniform
+        const int zl = j * zpj + (t >> 2);
+        int cls = -1;
+        float f[kClIn];
+        if (zl < nz) {
+            const ZoneRec zr = load_zone_rec(rec_at(zfirst + zl));
+            s0[j] = __float_as_int(zr.q[6].x);
+            nsd[j] = __float_as_int(zr.q[6].y);
+            cls = closure_classify(zr, k, x.img, qa, qb, f, frame[j]);
+        }
+        const bool net = cls == kClassMlp && mode == 0;
+        how[j] = net ? 1 : ((cls == kClassFallback || cls == kClassOod || (cls == kClassMlp && mode == 2)) ? 2 : 0);
+        const unsigned mnet = __ballot_sync(kFull, net);
+        const unsigned nm = __popc(__ballot_sync(kFull, cls == kClassMlp));
+        const unsigned nf = __popc(__ballot_sync(kFull, cls == kClassFallback));
+        const unsigned no = __popc(__ballot_sync(kFull, cls == kClassOod));
+        int base = 0;
+        if (lane == 0) {
+            if (nm) atomicAdd(x.ncls + 0, nm);
+            if (nf) atomicAdd(x.ncls + 1, nf);
+            if (no) atomicAdd(x.ncls + 2, no);
+            if (mnet) base = atomicAdd(x.nrow, (int)__popc(mnet));
+        }
+        base = __shfl_sync(kFull, base, 0);
+        if (net) {
+            slot[j] = base + __popc(mnet & ((1u << lane) - 1u));
+            closure_stage_row(x.a0, slot[j], f, mean, istd);
+        }
+    }
+    fence_async_smem();
+    __syncthreads();
+    const int n = *x.nrow;
+    for (int base = 0; base < n; base += (int)blockDim.x) closure_mlp_run(x.img, x.a0, x.h, st, base, n);
+    // the runs' outputs are visible to every thread; after a tensor-core
+    // wait ran out the network's corners get no force
+    const bool mlp_ok = __syncthreads_and(st.ok) != 0;
+    if (t == 0) *x.nrow = 0;
+    // the records of the forced corners and the side values to update in
+    // flight at once
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+        if (j * zpj + (t >> 2) < nz && k < nsd[j]) {
+            prefetch_l1(a.cforce_f + s0[j] + k);
+            prefetch_l1(a.sftot + s0[j] + k);
+            if (how[j]) {
+                const float4* r = rec_at(zfirst + j * zpj + (t >> 2));
+                prefetch_l1(r);
+                prefetch_l1(r + kZoneRecF4 - 1);
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+        if (j * zpj >= nz) continue;   // CTA-uniform
+        const bool zok = j * zpj + (t >> 2) < nz;
+        float d[4] = {0.f, 0.f, 0.f, 0.f};
+        const int hw = (how[j] == 1 && !mlp_ok) ? 0 : how[j];
+        if (hw) {
+            float4 y = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (hw == 1) {
+                const int run = slot[j] / (int)blockDim.x;
+                y = reinterpret_cast<const float4*>(x.a0 + run * (int)(blockDim.x >> 7) * 4096)
+                    [slot[j] - run * (int)blockDim.x];
+            }
+            const ZoneRec zr = load_zone_rec(rec_at(zfirst + j * zpj + (t >> 2)));
+            closure_corner_forces(zr, k, hw, y, frame[j], qa, qb, d);
+        }
+        const int n4 = nsd[j];
+        const int lp = g + (k == 0 ? n4 - 1 : k - 1);
+        const int ln = g + (k + 1 >= n4 ? 0 : k + 1);
+        const float2 d1 = fk(d[0], d[1]), d2 = fk(d[2], d[3]);
+        const float2 d1p = shflf2(d1, lp);
+        const float2 d2n = shflf2(d2, ln);
+        if (zok && k < n4) {
+            const int64_t sd = (int64_t)s0[j] + k;
+            const float2 cf = a.cforce_f[sd];
+            a.cforce_f[sd] = fadd(cf, fadd(fsub(d1, d2), fsub(d2n, d1p)));
+            const double2 sf = a.sftot[sd];
+            const float2 ds = fadd(d1, d2n);
+            a.sftot[sd] = mk(sf.x + (double)ds.x, sf.y + (double)ds.y);
+        }
+    }
+}
+
+// Adds a CTA's closure class counts and recorded zones to the counters.
+__device__ __forceinline__ void closure_add_counts(const DevArrays& a, const unsigned* ncls, int zones) {
+    if (threadIdx.x < 3 && ncls[threadIdx.x]) {
+        const int q = threadIdx.x == 0 ? kClassMlp : (threadIdx.x == 1 ? kClassFallback : kClassOod);
+        atomicAdd(a.closure_counts + q * 64 + (blockIdx.x & 63), (unsigned long long)ncls[threadIdx.x]);
+    }
+    if (threadIdx.x == 3 && zones)
+        atomicAdd(a.closure_counts + kClassZones * 64 + (blockIdx.x & 63), (unsigned long long)zones);
 }
 
 // Pass A over row tiles of a rect mesh (row_tiles.cuh): the same zone body
@@ -539,6 +827,7 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_ROWS_A_MIN_BLOCKS) pass_a_
     double zdthyd = 1.e99;
     int bad = 0;
     int cnt[3] = {0, 0, 0};
+    const RecSink sink{a.closure_nrec, reinterpret_cast<float4*>(a.closure_rec), 0x7fffffff};
     auto bytes = [&](int64_t g) { return AStage::bytes(rows::tile_of<kZoneThreadsZT>(g, nzx)); };
     auto issue = [&](unsigned char* st, int64_t g, uint32_t bar) {
         AStage::issue(st, a, cur, rows::tile_of<kZoneThreadsZT>(g, nzx), npx, bar);
@@ -550,7 +839,7 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_ROWS_A_MIN_BLOCKS) pass_a_
         const int64_t z = tl.z0 + t;
         double v = 1.e99;
         int zc[3] = {0, 0, 0};   // the zone's own corner classes (an acute zone overwrites them)
-        pass_a_mixed_zone<4, kLearned>(a, c, in, cur, dt, z, 4 * z, v, bad, zc, sp);
+        pass_a_mixed_zone<4, kLearned>(a, c, in, cur, dt, z, 4 * z, v, bad, zc, sp, sink);
         zdthyd = dmin(zdthyd, v);
 #pragma unroll
         for (int q = 0; q < 3; ++q) cnt[q] += zc[q];
@@ -663,20 +952,9 @@ __global__ void __launch_bounds__(kBatchThreads) batch_point_pass_mixed(BatchDev
 }
 
 // ---------------------------------------------------------------------
-// Closure pass (learned cycle): the deferred corners of the zones pass A
-// recorded, 64 zones (256 corners) per batch, persistent.  Each deferred
-// corner is classified (compression past rho_max or inputs out of
-// distribution: plain QCS, QCS.cc:116-327 in FP32 as in the mixed pass A;
-// otherwise the network, tcgen05, closure_dev.cuh); a tile without network
-// corners skips the network.  A corner's QCS forces cqe1, cqe2 enter
-// QCS::setForce (QCS.cc:331-380) linearly: its side s gets
-// d1 = cw (cqe2 + ccos cqe1) / elen[s] and the previous side
-// d2 = cw (cqe1 + ccos cqe2) / elen[s3].  The corner force of side s,
-// ftot[s] - ftot[s3] (Hydro.cc:1159-1193), and sfp + sfq of side s then
-// change by
-//   dcforce[s] = d1(s) - d2(s) - d1(s3) + d2(s4),  dsftot[s] = d1(s) + d2(s4),
-// which only touch the recorded zone's own sides: no two records write the
-// same side, so the update is deterministic without atomics.
+// Closure pass (learned cycle): the zones pass A recorded, each CTA an
+// equal contiguous share, rounds of 128 zones (two corners a thread, up to
+// 512 packed rows in runs of 256).
 // ---------------------------------------------------------------------
 #ifndef PNT_CLOSURE_MIN_BLOCKS
 #define PNT_CLOSURE_MIN_BLOCKS 3
@@ -684,132 +962,25 @@ __global__ void __launch_bounds__(kBatchThreads) batch_point_pass_mixed(BatchDev
 __global__ void __launch_bounds__(kMlpRows, PNT_CLOSURE_MIN_BLOCKS) closure_pass(DevArrays a, HydroConst c) {
     if (skip_cycle(a.ctl)) return;
     const int nrec = *a.closure_nrec;
-    if (blockIdx.x == 0 && threadIdx.x == 0 && nrec)
-        atomicAdd(a.closure_counts + kClassZones * 64, (unsigned long long)nrec);
-    if ((int64_t)blockIdx.x * 64 >= nrec) return;
+    const int chunk = (nrec + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int zb = (int)blockIdx.x * chunk;
+    const int ze = min(nrec, zb + chunk);
+    if (zb >= ze) return;
     extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ unsigned ccount[3];   // network, fallback, out of distribution
-    if (threadIdx.x < 3) ccount[threadIdx.x] = 0u;
+    __shared__ unsigned s_ncls[3];
+    __shared__ int s_nrow;
+    if (threadIdx.x < 3) s_ncls[threadIdx.x] = 0u;
+    if (threadIdx.x == 0) s_nrow = 0;
     MlpState st;
-    closure_mlp_setup(smem, a.closure_img, st);   // its barrier publishes ccount's zeros
-    const float* thr = reinterpret_cast<const float*>(smem + kImgThr);
-    const float rho_max = thr[1], kappa = thr[2];
-    const int mode = (int)thr[3];   // 0 network, 1 no force, 2 plain QCS
-    const float* mean = reinterpret_cast<const float*>(smem + kImgFMean);
-    const float* istd = reinterpret_cast<const float*>(smem + kImgFIstd);
-    const float qa = (float)(c.q2 * 0.25 * c.gammap1), qb = (float)c.q1;
-    const int k = threadIdx.x & 3, lane = threadIdx.x & 31, g = lane & ~3;
-    for (int tile = blockIdx.x; (int64_t)tile * 64 < nrec; tile += gridDim.x) {
-        const int zi = tile * 64 + (threadIdx.x >> 2);
-        const bool zok = zi < nrec;
-        float v[kRecFloats];
-        const float4* rec = reinterpret_cast<const float4*>(a.closure_rec + ((int64_t)zi * 4 + k) * kRecFloats);
-#pragma unroll
-        for (int i = 0; i < kRecFloats / 4; ++i) {
-            const float4 q = zok ? rec[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-            v[4 * i] = q.x;
-            v[4 * i + 1] = q.y;
-            v[4 * i + 2] = q.z;
-            v[4 * i + 3] = q.w;
-        }
-        const int2 hdr = zok ? a.closure_zhdr[zi] : make_int2(0, 4);
-        const float2 x = fk(v[kRecX], v[kRecX + 1]), xpv = fk(v[kRecXp], v[kRecXp + 1]);
-        const float2 xn = fk(v[kRecXn], v[kRecXn + 1]), xz = fk(v[kRecXz], v[kRecXz + 1]);
-        const float2 u = fk(v[kRecU], v[kRecU + 1]), upv = fk(v[kRecUp], v[kRecUp + 1]);
-        const float2 un = fk(v[kRecUn], v[kRecUn + 1]), uz = fk(v[kRecUz], v[kRecUz + 1]);
-        const float2 uav = fk(v[kRecUav], v[kRecUav + 1]);
-        const float css = v[kRecSs], rho = v[kRecRho];
-        // classify the deferred corners
-        int cls = -1;
-        float f[kClIn];
-        float cx = 0.f, cy = 0.f, scale = 0.f;
-        if (v[kRecFlag] != 0.f &&
-            closure_features<float>({x.x, x.y}, {xpv.x, xpv.y}, {xn.x, xn.y}, {xz.x, xz.y}, {u.x, u.y},
-                                    {upv.x, upv.y}, {un.x, un.y}, {uz.x, uz.y}, {uav.x, uav.y}, css, qa, qb, 0.f,
-                                    f, cx, cy, scale)) {
-            if (f[11] > rho_max) cls = kClassFallback;
-            else {
-                float zmax = 0.f;
-#pragma unroll
-                for (int i = 0; i < kClIn; ++i) zmax = fmaxf(zmax, fabsf((f[i] - mean[i]) * istd[i]));
-                cls = (zmax > kappa) ? kClassOod : kClassMlp;
-            }
-        }
-        const bool net = cls == kClassMlp && mode == 0;
-        const bool plain = cls == kClassFallback || cls == kClassOod || (cls == kClassMlp && mode == 2);
-        {
-            const unsigned nm = __popc(__ballot_sync(kFull, cls == kClassMlp));
-            const unsigned nf = __popc(__ballot_sync(kFull, cls == kClassFallback));
-            const unsigned no = __popc(__ballot_sync(kFull, cls == kClassOod));
-            if (lane == 0) {
-                if (nm) atomicAdd(&ccount[0], nm);
-                if (nf) atomicAdd(&ccount[1], nf);
-                if (no) atomicAdd(&ccount[2], no);
-            }
-        }
-        if (!net) {
-#pragma unroll
-            for (int i = 0; i < kClIn; ++i) f[i] = 0.f;
-        }
-        float y[4] = {0.f, 0.f, 0.f, 0.f};
-        if (__syncthreads_or(net)) closure_mlp_rows(smem, st, f, y);
-        // corner geometry (QCS::setCornerDiv / setForce, FP32 as in pass A)
-        const float2 ex = fmul(0.5f, fadd(x, xn));
-        const float2 xq3 = fmul(0.5f, fadd(xpv, x));
-        const float cvolume = 0.5f * fcross(fsub(xz, x), fsub(xq3, ex));
-        const float2 v1 = fsub(xq3, x), v2 = fsub(ex, x);
-        const float de1 = flen(fsub(x, xpv)), de2 = flen(fsub(xn, x));
-        const float rinv_de1 = 1.f / de1, rinv_el = 1.f / de2;
-        const float minelen = fminf(de1, de2);
-        float ccos = (minelen < 1.e-12f) ? 0.f : 4.f * fdot(v1, v2) / (de1 * de2);
-        float2 q1 = fk(0.f, 0.f), q2 = fk(0.f, 0.f);
-        if (net) {
-            const float sc = rho * scale;
-            q1 = fk((cx * y[0] - cy * y[1]) * sc, (cy * y[0] + cx * y[1]) * sc);
-            q2 = fk((cx * y[2] - cy * y[3]) * sc, (cy * y[2] + cx * y[3]) * sc);
-        } else if (plain) {
-            const float2 up1 = fmul(0.5f, fadd(u, un)), up3 = fmul(0.5f, fadd(upv, u));
-            const float2 dxx1 = fmul(0.5f, fsub(fsub(fadd(ex, xz), x), xq3));
-            const float2 dxx2 = fmul(0.5f, fsub(fsub(fadd(xz, xq3), x), ex));
-            const float dx1 = flen(dxx1), dx2 = flen(dxx2);
-            const float test1 = fabsf(fdot(dxx1, uav) * dx2);
-            const float test2 = fabsf(fdot(dxx2, uav) * dx1);
-            const float rr = (test1 > test2) ? dx1 / dx2 : dx2 / dx1;
-            const float evol = fminf(sqrtf(4.f * cvolume * rr), 2.f * minelen);
-            const float du = sqrtf(fmaxf(flen2(fsub(fsub(fadd(up1, uz), u), up3)),
-                                         flen2(fsub(fsub(fadd(uz, up3), u), up1))));
-            const float ztmp2 = qa * du;
-            const float ztmp1 = qb * css;
-            const float crmu = (ztmp2 + sqrtf(ztmp2 * ztmp2 + ztmp1 * ztmp1)) * rho * evol;
-            q1 = fmul(crmu * rinv_de1, fsub(u, upv));
-            q2 = fmul(crmu * rinv_el, fsub(un, u));
-        }
-        const float ssin = 4.f * fcross(v1, v2) / (de1 * de2);
-        const float csin2 = (minelen < 1.e-12f) ? 1.f : ssin * ssin;
-        const float cw = (csin2 < 1.e-4f) ? 0.f : cvolume / csin2;
-        ccos = (csin2 < 1.e-4f) ? 0.f : ccos;
-        const int n = hdr.y;
-        const int lp = g + (k == 0 ? n - 1 : k - 1);
-        const int ln = g + (k + 1 >= n ? 0 : k + 1);
-        const float2 d1 = fmul(cw * rinv_el, fadd(q2, fmul(ccos, q1)));
-        const float2 d2 = fmul(cw * rinv_de1, fadd(q1, fmul(ccos, q2)));
-        const float2 d1p = shflf2(d1, lp);
-        const float2 d2n = shflf2(d2, ln);
-        if (zok && k < n) {
-            const int64_t sd = (int64_t)hdr.x + k;
-            const float2 cf = a.cforce_f[sd];
-            a.cforce_f[sd] = fadd(cf, fadd(fsub(d1, d2), fsub(d2n, d1p)));
-            const double2 sf = a.sftot[sd];
-            const float2 ds = fadd(d1, d2n);
-            a.sftot[sd] = mk(sf.x + (double)ds.x, sf.y + (double)ds.y);
-        }
-    }
-    const bool ok = closure_mlp_teardown(smem, st);
+    closure_mlp_setup(smem, a.closure_img, reinterpret_cast<uint64_t*>(smem + kCpBar),
+                      reinterpret_cast<uint32_t*>(smem + kCpBar + 8), kTmemCols, st);   // publishes the zeros
+    const ClosureCtx cx{smem, smem + kCpA0, smem + kCpH, &s_nrow, s_ncls};
+    const float4* recs = reinterpret_cast<const float4*>(a.closure_rec);
+    auto rec_at = [&](int i) { return recs + (int64_t)i * kZoneRecF4; };
+    for (int zr = zb; zr < ze; zr += 128) closure_round<2>(a, c, cx, st, rec_at, zr, min(128, ze - zr));
+    const bool ok = closure_mlp_teardown(st);   // its barrier orders the counters
     if (threadIdx.x == 0 && !ok) atomicAdd(a.closure_counts + kClassErr * 64, 1ull);
-    if (threadIdx.x < 3 && ccount[threadIdx.x]) {
-        const int q = threadIdx.x == 0 ? kClassMlp : (threadIdx.x == 1 ? kClassFallback : kClassOod);
-        atomicAdd(a.closure_counts + q * 64 + (blockIdx.x & 63), (unsigned long long)ccount[threadIdx.x]);
-    }
+    closure_add_counts(a, s_ncls, ze - zb);
 }
 
 }  // namespace
@@ -833,7 +1004,7 @@ cudaError_t launch_cycle_mixed_impl(const DevArrays& a, const HydroConst& c, cud
             else pass_a_mixed_zt<false, false><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
         }
         if (ev) cudaEventRecord(ev[1], stream);
-        if (learned) closure_pass<<<a.closure_grid, kMlpRows, kMlpSmemBytes, stream>>>(a, c);
+        if (learned) closure_pass<<<a.closure_grid, kMlpRows, kCpSmemBytes, stream>>>(a, c);
         if (ev) cudaEventRecord(ev[2], stream);
     }
     if (phases & kPhaseAdvance) {
@@ -875,7 +1046,7 @@ void launch_batch_point_pass_mixed(const BatchDev& b, int grid, cudaStream_t str
 }
 
 cudaError_t prepare_learned_kernels() {
-    return cudaFuncSetAttribute(closure_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, kMlpSmemBytes);
+    return cudaFuncSetAttribute(closure_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, kCpSmemBytes);
 }
 
 }  // namespace pnt
