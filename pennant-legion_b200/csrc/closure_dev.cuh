@@ -83,15 +83,24 @@ __host__ __device__ constexpr int canon_off(int r, int k, int rows) { return (k 
 // (points 3 of a 3-sided zone are zeros).
 constexpr int kZoneRecF4 = 7;
 
-// Shared memory of the closure pass: the parameter image, the BF16 input
-// rows of up to kCpRows corners (four 128-row operand tiles), the hidden
-// activations of one 256-row run (two tiles), an mbarrier and the TMEM
-// address.  The outputs of a run overwrite the first 4 KB of its own two
-// input tiles (row r of the run at 16 r), whose MMAs are complete by then.
-constexpr int kCpRows = 512;
+// The closure pass: kCpThreads threads a CTA, kCpCtasPerSm CTAs an SM (64
+// TMEM columns per 128 threads).  Its shared memory: the parameter image,
+// the BF16 input rows of up to kCpRows corners (two a thread, 128-row
+// operand tiles), the hidden activations of one run of kCpThreads rows, an
+// mbarrier and the TMEM address.  The outputs of a run overwrite the first
+// kCpThreads * 16 bytes of its own operand tiles, whose MMAs are complete
+// by then.
+#ifndef PNT_CLOSURE_THREADS
+#define PNT_CLOSURE_THREADS 256
+#endif
+constexpr int kCpThreads = PNT_CLOSURE_THREADS;
+static_assert(kCpThreads == 128 || kCpThreads == 256, "one or two M tiles a run");
+constexpr int kCpCtasPerSm = kCpThreads == 128 ? 6 : 3;
+constexpr uint32_t kCpTmemCols = kCpThreads / 2;
+constexpr int kCpRows = 2 * kCpThreads;
 constexpr int kCpA0 = 13312;
 constexpr int kCpH = kCpA0 + kCpRows * 32;
-constexpr int kCpBar = kCpH + 2 * 128 * 64 * 2;
+constexpr int kCpBar = kCpH + (kCpThreads / 128) * 128 * 64 * 2;
 constexpr int kCpSmemBytes = kCpBar + 64;
 
 // Shared memory of the 256-row inference block.

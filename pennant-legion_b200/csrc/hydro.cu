@@ -5,10 +5,6 @@
 #include "hydro_dev.h"
 #include "pnt_internal.h"
 
-#ifndef PNT_CLOSURE_CTAS_PER_SM
-#define PNT_CLOSURE_CTAS_PER_SM 3
-#endif
-
 #include <algorithm>
 #include <chrono>
 #include <climits>
@@ -837,8 +833,7 @@ pnt_status pnt_hydro_set_closure(pnt_hydro* h, const pnt_closure* c, int32_t mod
         h->a.closure_img = img;
         h->a.closure_rec = rec;
         h->a.closure_nrec = nrec;
-        // 128 TMEM columns and 61 KB of shared memory per CTA; 3 per SM
-        h->a.closure_grid = PNT_CLOSURE_CTAS_PER_SM * nsm;
+        h->a.closure_grid = kCpCtasPerSm * nsm;
     }
     // the image lives in this object: a copy of the closure's, with the mode
     uint8_t* img = const_cast<uint8_t*>(h->a.closure_img);

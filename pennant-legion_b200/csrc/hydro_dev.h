@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <utility>
 #include <cuda_runtime.h>
 
 struct pnt_hydro;
@@ -117,6 +118,35 @@ constexpr int kNumKernels = 5;   // A, B, C, finalize, closure pass
 
 // Phases of a cycle: the corner forces (pass A and the learned closure
 // pass) and the advance (passes B, C and the finalize step).
+// Programmatic dependent launch: the cycle's kernels are launched with
+// launch_pdl, so that each is launched while the kernel before it drains
+// rather than after it has completed.  Every such kernel calls pdl_wait()
+// before it reads anything an earlier kernel wrote or writes anything an
+// earlier kernel reads; the wait returns once the previous grid has
+// completed and its memory is visible.  No kernel signals its dependents
+// early (griddepcontrol.launch_dependents): dependent CTAs waiting on the
+// SMs while the previous kernel still ran made the 1920^2 cycles 5-17%
+// slower, against 0.1-0.7% faster without that signal.
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+#endif
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                              Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 constexpr int kPhaseForces = 1;
 constexpr int kPhaseAdvance = 2;
 constexpr int kPhaseAll = kPhaseForces | kPhaseAdvance;
@@ -129,7 +159,8 @@ cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStrea
 // The mixed-precision cycle (hydro_mixed.cu).
 cudaError_t launch_cycle_mixed(const DevArrays& a, const HydroConst& c, cudaStream_t stream,
                                cudaEvent_t* ev = nullptr, int phases = kPhaseAll);
-// The learned-closure cycle: the mixed cycle with the closure in pass A.
+// The learned-closure cycle: the mixed cycle with the closure pass after
+// pass A.
 cudaError_t launch_cycle_learned(const DevArrays& a, const HydroConst& c, cudaStream_t stream,
                                  cudaEvent_t* ev = nullptr, int phases = kPhaseAll);
 // Multi-piece runs (hydro_fp64.cu): gathers the corner mass and force of
@@ -142,7 +173,7 @@ void launch_piece_finish(const DevArrays& a, const HydroConst& c, cudaStream_t s
 // The index of the first non-finite value of a[0 .. n) into *first (an
 // atomic minimum; *first must start at ULLONG_MAX).
 void launch_find_nonfinite(const double* a, int64_t n, unsigned long long* first, cudaStream_t stream);
-// Raises the learned pass A's dynamic shared-memory limit on the current device.
+// Raises the closure pass's dynamic shared-memory limit on the current device.
 cudaError_t prepare_learned_kernels();
 // Pass C of the FP64 (mixed = false) or mixed/learned cycle (pass_c.cu):
 // prepare_pass_c raises the kernel's shared-memory limit on the current

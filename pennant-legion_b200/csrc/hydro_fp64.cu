@@ -52,6 +52,7 @@ constexpr int kZoneThreadsZT = 128;   // one zone per thread
 
 template <bool kQuads>
 __global__ void __launch_bounds__(kZoneThreadsZT, PNT_PASS_A_ZT_MIN_BLOCKS) pass_a_zt(DevArrays a, HydroConst c) {
+    pdl_wait();
     const Ctl* ctl = a.ctl;
     if (skip_cycle(ctl)) return;
     const int64_t z = (int64_t)blockIdx.x * kZoneThreadsZT + threadIdx.x;
@@ -74,6 +75,7 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_PASS_A_ZT_MIN_BLOCKS) pass
 }
 
 __global__ void __launch_bounds__(kPointThreads) pass_b(DevArrays a, HydroConst c) {
+    pdl_wait();
     const Ctl* ctl = a.ctl;
     if (skip_cycle(ctl)) return;
     const int64_t p = (int64_t)blockIdx.x * kPointThreads + threadIdx.x;
@@ -123,21 +125,22 @@ cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStrea
                               int phases) {
     const int pb = (int)((a.nump + kPointThreads - 1) / kPointThreads);
     const int zba = (int)((a.numz + kZoneThreadsZT - 1) / kZoneThreadsZT);
+    cudaError_t e = cudaSuccess;
     if (phases & kPhaseForces) {
         if (ev) cudaEventRecord(ev[0], stream);
-        if (a.quads) pass_a_zt<true><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
-        else pass_a_zt<false><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
+        e = launch_pdl(a.quads ? pass_a_zt<true> : pass_a_zt<false>, zba, kZoneThreadsZT, 0, stream, a, c);
         if (ev) cudaEventRecord(ev[1], stream);
         if (ev) cudaEventRecord(ev[2], stream);   // no closure pass
     }
     if (phases & kPhaseAdvance) {
-        pass_b<<<pb, kPointThreads, 0, stream>>>(a, c);
+        const cudaError_t eb = launch_pdl(pass_b, pb, kPointThreads, 0, stream, a, c);
+        if (e == cudaSuccess) e = eb;
         if (ev) cudaEventRecord(ev[3], stream);
         launch_pass_c(a, c, false, stream);   // its last CTA ends the cycle
         if (ev) cudaEventRecord(ev[4], stream);
         if (ev) cudaEventRecord(ev[5], stream);   // no separate finalize step
     }
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 void launch_piece_pack(const DevArrays& a, const int32_t* send_side, int32_t nsend, unsigned char* send,

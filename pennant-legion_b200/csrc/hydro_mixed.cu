@@ -461,6 +461,7 @@ __device__ __forceinline__ void pass_a_mixed_zone(const DevArrays& a, const Hydr
 
 template <bool kQuads, bool kLearned>
 __global__ void __launch_bounds__(kZoneThreadsZT, PNT_MIXED_ZT_MIN_BLOCKS) pass_a_mixed_zt(DevArrays a, HydroConst c) {
+    pdl_wait();
     const Ctl* ctl = a.ctl;
     if (skip_cycle(ctl)) return;
     const int64_t z = (int64_t)blockIdx.x * kZoneThreadsZT + threadIdx.x;
@@ -815,6 +816,7 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_ROWS_A_MIN_BLOCKS) pass_a_
     __shared__ __align__(8) uint64_t bars[kRowsAStages];
     __shared__ double2 s_sfp[4 * kZoneThreadsZT];
     __shared__ float2 s_sft[4 * kZoneThreadsZT];
+    pdl_wait();
     const Ctl* ctl = a.ctl;
     if (skip_cycle(ctl)) return;
     const int cur = ctl->cycle & 1;
@@ -888,9 +890,8 @@ __device__ __forceinline__ void pass_b_mixed_point(const DevArrays& a, const Hyd
 }
 
 __global__ void __launch_bounds__(kPointThreads) pass_b_mixed(DevArrays a, HydroConst c) {
+    pdl_wait();
     const Ctl* ctl = a.ctl;
-    // the closure pass has consumed this cycle's zone records
-    if (a.closure_nrec && blockIdx.x == 0 && threadIdx.x == 0) *a.closure_nrec = 0;
     if (skip_cycle(ctl)) return;
     const int64_t p = (int64_t)blockIdx.x * kPointThreads + threadIdx.x;
     if (p >= a.nump) return;
@@ -956,31 +957,29 @@ __global__ void __launch_bounds__(kBatchThreads) batch_point_pass_mixed(BatchDev
 // equal contiguous share, rounds of 128 zones (two corners a thread, up to
 // 512 packed rows in runs of 256).
 // ---------------------------------------------------------------------
-#ifndef PNT_CLOSURE_MIN_BLOCKS
-#define PNT_CLOSURE_MIN_BLOCKS 3
-#endif
-__global__ void __launch_bounds__(kMlpRows, PNT_CLOSURE_MIN_BLOCKS) closure_pass(DevArrays a, HydroConst c) {
-    if (skip_cycle(a.ctl)) return;
-    const int nrec = *a.closure_nrec;
-    const int chunk = (nrec + (int)gridDim.x - 1) / (int)gridDim.x;
-    const int zb = (int)blockIdx.x * chunk;
-    const int ze = min(nrec, zb + chunk);
-    if (zb >= ze) return;
+__global__ void __launch_bounds__(kCpThreads, kCpCtasPerSm) closure_pass(DevArrays a, HydroConst c) {
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ unsigned s_ncls[3];
     __shared__ int s_nrow;
     if (threadIdx.x < 3) s_ncls[threadIdx.x] = 0u;
     if (threadIdx.x == 0) s_nrow = 0;
+    // the image and the tensor memory need nothing from pass A: set up while
+    // it drains
     MlpState st;
     closure_mlp_setup(smem, a.closure_img, reinterpret_cast<uint64_t*>(smem + kCpBar),
-                      reinterpret_cast<uint32_t*>(smem + kCpBar + 8), kTmemCols, st);   // publishes the zeros
+                      reinterpret_cast<uint32_t*>(smem + kCpBar + 8), kCpTmemCols, st);   // publishes the zeros
+    pdl_wait();
+    const int nrec = skip_cycle(a.ctl) ? 0 : *a.closure_nrec;
+    const int chunk = (nrec + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int zb = (int)blockIdx.x * chunk;
+    const int ze = min(nrec, zb + chunk);
     const ClosureCtx cx{smem, smem + kCpA0, smem + kCpH, &s_nrow, s_ncls};
     const float4* recs = reinterpret_cast<const float4*>(a.closure_rec);
     auto rec_at = [&](int i) { return recs + (int64_t)i * kZoneRecF4; };
     for (int zr = zb; zr < ze; zr += 128) closure_round<2>(a, c, cx, st, rec_at, zr, min(128, ze - zr));
     const bool ok = closure_mlp_teardown(st);   // its barrier orders the counters
     if (threadIdx.x == 0 && !ok) atomicAdd(a.closure_counts + kClassErr * 64, 1ull);
-    closure_add_counts(a, s_ncls, ze - zb);
+    closure_add_counts(a, s_ncls, ze > zb ? ze - zb : 0);
 }
 
 }  // namespace
@@ -991,30 +990,32 @@ cudaError_t launch_cycle_mixed_impl(const DevArrays& a, const HydroConst& c, cud
                                     bool learned, int phases) {
     const int pb = (int)((a.nump + kPointThreads - 1) / kPointThreads);
     const int zba = (int)((a.numz + kZoneThreadsZT - 1) / kZoneThreadsZT);
+    cudaError_t e = cudaSuccess;
+    auto chk = [&](cudaError_t r) {
+        if (e == cudaSuccess) e = r;
+    };
     if (phases & kPhaseForces) {
         if (ev) cudaEventRecord(ev[0], stream);
         if (a.rect_nzx > 0) {
-            if (learned) pass_a_mixed_rows<true><<<a.gridA, kZoneThreadsZT, kRowsASmem, stream>>>(a, c);
-            else pass_a_mixed_rows<false><<<a.gridA, kZoneThreadsZT, kRowsASmem, stream>>>(a, c);
-        } else if (learned) {
-            if (a.quads) pass_a_mixed_zt<true, true><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
-            else pass_a_mixed_zt<false, true><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
+            chk(launch_pdl(learned ? pass_a_mixed_rows<true> : pass_a_mixed_rows<false>, a.gridA, kZoneThreadsZT,
+                           kRowsASmem, stream, a, c));
         } else {
-            if (a.quads) pass_a_mixed_zt<true, false><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
-            else pass_a_mixed_zt<false, false><<<zba, kZoneThreadsZT, 0, stream>>>(a, c);
+            auto k = learned ? (a.quads ? pass_a_mixed_zt<true, true> : pass_a_mixed_zt<false, true>)
+                             : (a.quads ? pass_a_mixed_zt<true, false> : pass_a_mixed_zt<false, false>);
+            chk(launch_pdl(k, zba, kZoneThreadsZT, 0, stream, a, c));
         }
         if (ev) cudaEventRecord(ev[1], stream);
-        if (learned) closure_pass<<<a.closure_grid, kMlpRows, kCpSmemBytes, stream>>>(a, c);
+        if (learned) chk(launch_pdl(closure_pass, a.closure_grid, kCpThreads, kCpSmemBytes, stream, a, c));
         if (ev) cudaEventRecord(ev[2], stream);
     }
     if (phases & kPhaseAdvance) {
-        pass_b_mixed<<<pb, kPointThreads, 0, stream>>>(a, c);
+        chk(launch_pdl(pass_b_mixed, pb, kPointThreads, 0, stream, a, c));
         if (ev) cudaEventRecord(ev[3], stream);
         launch_pass_c(a, c, true, stream);   // its last CTA ends the cycle
         if (ev) cudaEventRecord(ev[4], stream);
         if (ev) cudaEventRecord(ev[5], stream);   // no separate finalize step
     }
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 }  // namespace

@@ -70,6 +70,10 @@ template <bool kMixed>
 __global__ void __launch_bounds__(kRowT) pass_c_rows(DevArrays a, HydroConst c) {
     extern __shared__ __align__(128) unsigned char smem_r[];
     __shared__ __align__(8) uint64_t bars[kRowStages];
+    pdl_wait();
+    // the learned cycle's closure pass and pass B are done with this cycle's
+    // zone records
+    if (a.closure_nrec && blockIdx.x == 0 && threadIdx.x == 0) *a.closure_nrec = 0;
     const Ctl* ctl = a.ctl;
     if (fp64::skip_cycle(ctl)) return;
     const int cur = ctl->cycle & 1;
@@ -118,6 +122,8 @@ __global__ void __launch_bounds__(kRowT) pass_c_rows(DevArrays a, HydroConst c) 
 template <bool kQuads, bool kMixed>
 __global__ void __launch_bounds__(stagedc::kTile) pass_c_staged(DevArrays a, HydroConst c) {
     extern __shared__ __align__(16) unsigned char smem_c[];
+    pdl_wait();
+    if (a.closure_nrec && blockIdx.x == 0 && threadIdx.x == 0) *a.closure_nrec = 0;
     if (fp64::skip_cycle(a.ctl)) return;
     double dvm = 1.e-99;
     int nbad = 0;
@@ -156,10 +162,10 @@ cudaError_t prepare_pass_c(bool mixed, bool quads, int32_t rect_nzx, int32_t num
 
 void launch_pass_c(const DevArrays& a, const HydroConst& c, bool mixed, cudaStream_t stream) {
     if (a.rect_nzx > 0) {
-        (mixed ? pass_c_rows<true> : pass_c_rows<false>)<<<a.gridC, kRowT, kRowSmemBytes, stream>>>(a, c);
+        launch_pdl(mixed ? pass_c_rows<true> : pass_c_rows<false>, a.gridC, kRowT, kRowSmemBytes, stream, a, c);
         return;
     }
-    pick_kernel(mixed, a.quads != 0)<<<a.gridC, stagedc::kTile, stagedc::kSmemBytes, stream>>>(a, c);
+    launch_pdl(pick_kernel(mixed, a.quads != 0), a.gridC, stagedc::kTile, stagedc::kSmemBytes, stream, a, c);
 }
 
 }  // namespace pnt
