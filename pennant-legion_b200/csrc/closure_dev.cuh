@@ -31,6 +31,7 @@
 
 #include <cstdint>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 namespace pnt {
@@ -176,18 +177,19 @@ __device__ __forceinline__ bool closure_features(ClV<T> xp, ClV<T> xpp, ClV<T> x
 constexpr float kGeluC = 0.7978845608028654f;   // sqrt(2/pi)
 constexpr float kGeluA = 0.044715f;
 
-__device__ __forceinline__ float tanh_approx(float x) {
-    float y;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-// Every rounding written out: the same bits in every kernel that inlines
-// it, whatever the compiler's contraction flags.
-__device__ __forceinline__ float gelu_fast(float x) {
-    const float p = __fmaf_rn(__fmul_rn(kGeluA, __fmul_rn(x, x)), x, x);   // x + a x^3
-    const float th = tanh_approx(__fmul_rn(kGeluC, p));
-    const float hx = __fmul_rn(0.5f, x);
-    return __fmaf_rn(hx, th, hx);
+// GELU of two values: the argument u = c (x + a x^3) and the result
+// 0.5 x (1 + tanh u) in packed FP32 (two lanes an instruction), tanh u in
+// FP16 (tanh.approx.f16x2: two a special-function instruction, relative
+// error ~2^-11, below the BF16 rounding the activation gets next; u beyond
+// the FP16 range rounds to +-inf, whose tanh is +-1).  Every rounding is
+// written out: the same bits in every kernel that inlines it, whatever the
+// compiler's contraction flags.
+__device__ __forceinline__ float2 gelu2_fast(float2 x) {
+    const float2 p = __ffma2_rn(__fmul2_rn(make_float2(kGeluA, kGeluA), __fmul2_rn(x, x)), x, x);   // x + a x^3
+    const float2 u = __fmul2_rn(make_float2(kGeluC, kGeluC), p);
+    const float2 th = __half22float2(h2tanh_approx(__floats2half2_rn(u.x, u.y)));
+    const float2 hx = __fmul2_rn(make_float2(0.5f, 0.5f), x);
+    return __ffma2_rn(hx, th, hx);
 }
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
@@ -295,9 +297,11 @@ __device__ __forceinline__ void mlp_hidden_epilogue(uint32_t tacc, const float* 
         tmem_ld16(tacc + 16 * c, v);
         uint32_t w[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
-            w[i] = pack_bf16(gelu_fast(__fadd_rn(v[2 * i], bias[16 * c + 2 * i])),
-                             gelu_fast(__fadd_rn(v[2 * i + 1], bias[16 * c + 2 * i + 1])));
+        for (int i = 0; i < 8; ++i) {
+            const float2 g = gelu2_fast(__fadd2_rn(make_float2(v[2 * i], v[2 * i + 1]),
+                                                   make_float2(bias[16 * c + 2 * i], bias[16 * c + 2 * i + 1])));
+            w[i] = pack_bf16(g.x, g.y);
+        }
         // k = 16c..16c+7 is K chunk 2c, k = 16c+8.. chunk 2c+1 (128 rows: 2048 B apart)
         *reinterpret_cast<uint4*>(hrow + (2 * c) * 2048) = make_uint4(w[0], w[1], w[2], w[3]);
         *reinterpret_cast<uint4*>(hrow + (2 * c + 1) * 2048) = make_uint4(w[4], w[5], w[6], w[7]);
