@@ -794,8 +794,10 @@ def main():
             # plain-QCS share of the compressing corners the network could take
             # (zones with an acute corner keep the FP64 QCS whatever the compression)
             "fallback_fraction": (cnt["fallback"] + cnt["ood"]) / max(cnt["mlp"] + cnt["fallback"] + cnt["ood"], 1),
-            "zones_per_cycle": zones_per_cycle, "closure_pass_ms": cl_ms,
-            "tensor_tflops": (4 * zones_per_cycle * MLP_FLOP_PER_ROW) / (cl_ms / 1e3) / 1e12 if cl_ms > 0 else None,
+            # the closure pass runs the network on the network's corners only
+            "zones_per_cycle": zones_per_cycle, "network_rows_per_cycle": cnt["mlp"] / args.steps,
+            "closure_pass_ms": cl_ms,
+            "tensor_tflops": (cnt["mlp"] / args.steps * MLP_FLOP_PER_ROW) / (cl_ms / 1e3) / 1e12 if cl_ms > 0 else None,
             "wait_timeouts": cnt["error"], "weights": os.path.relpath(args.closure, ROOT)}
 
     result = None
