@@ -50,7 +50,8 @@ using namespace fp64;
 #endif
 constexpr int kZoneThreadsZT = 128;   // one zone per thread
 
-template <bool kQuads>
+// kRect: a rect mesh (a.rect_nzx > 0), point indices from the zone index.
+template <bool kQuads, bool kRect = false>
 __global__ void __launch_bounds__(kZoneThreadsZT, PNT_PASS_A_ZT_MIN_BLOCKS) pass_a_zt(DevArrays a, HydroConst c) {
     pdl_wait();
     const Ctl* ctl = a.ctl;
@@ -61,7 +62,10 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_PASS_A_ZT_MIN_BLOCKS) pass
     if (z < a.numz) {
         const int cur = ctl->cycle & 1;
         const double dt = ctl->dt;
-        if (kQuads) {
+        if (kRect) {
+            const RectZoneIn in(a, cur, z);
+            pass_a_zone_thread<4>(a, c, in, dt, z, 4 * z, zdthyd, bad);
+        } else if (kQuads) {
             pass_a_zone_thread<4>(a, c, cur, dt, z, 4 * z, zdthyd, bad);
         } else {
             const int n = a.znump[z];
@@ -128,7 +132,8 @@ cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStrea
     cudaError_t e = cudaSuccess;
     if (phases & kPhaseForces) {
         if (ev) cudaEventRecord(ev[0], stream);
-        e = launch_pdl(a.quads ? pass_a_zt<true> : pass_a_zt<false>, zba, kZoneThreadsZT, 0, stream, a, c);
+        e = launch_pdl(a.rect_nzx > 0 ? pass_a_zt<true, true> : (a.quads ? pass_a_zt<true> : pass_a_zt<false>), zba,
+                       kZoneThreadsZT, 0, stream, a, c);
         if (ev) cudaEventRecord(ev[1], stream);
         if (ev) cudaEventRecord(ev[2], stream);   // no closure pass
     }

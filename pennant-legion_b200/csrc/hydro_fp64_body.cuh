@@ -238,6 +238,32 @@ struct GlobalZoneIn {
     __device__ __forceinline__ double zvol() const { return a.zvol[z]; }
 };
 
+// The same reads on a mesh numbered as the rect generator numbers it
+// (zones row-major, nzx a row; side 4z + k of zone z = (i, j) starts at
+// point (i, j), (i+1, j), (i+1, j+1), (i, j+1) for k = 0..3): the point
+// indices follow from z, with no load of mapsp1 before the gathers.
+struct RectZoneIn {
+    const DevArrays& a;
+    int cur;
+    int64_t z, s0, p0, npx;
+    __device__ __forceinline__ RectZoneIn(const DevArrays& a_, int cur_, int64_t z_)
+        : a(a_), cur(cur_), z(z_), s0(4 * z_), npx((int64_t)a_.rect_nzx + 1) {
+        const int64_t zj = z_ / a_.rect_nzx;
+        p0 = zj * npx + (z_ - zj * a_.rect_nzx);
+    }
+    __device__ __forceinline__ int64_t p(int k) const {
+        return p0 + (k == 1 ? 1 : (k == 2 ? npx + 1 : (k == 3 ? npx : 0)));
+    }
+    __device__ __forceinline__ double2 x0(int k) const { return a.px[cur][p(k)]; }
+    __device__ __forceinline__ double2 u0(int k) const { return a.pu[cur][p(k)]; }
+    __device__ __forceinline__ double mf(int k) const { return __ldg(a.smf + s0 + k); }
+    __device__ __forceinline__ double zm() const { return a.zm[z]; }
+    __device__ __forceinline__ double zr() const { return a.zr[z]; }
+    __device__ __forceinline__ double ze() const { return a.ze[z]; }
+    __device__ __forceinline__ double zwrate() const { return a.zwrate[z]; }
+    __device__ __forceinline__ double zvol() const { return a.zvol[z]; }
+};
+
 template <int N, typename In>
 __device__ __forceinline__ void pass_a_zone_thread(const DevArrays& a, const HydroConst& c, const In& in, double dt,
                                                    int64_t z, int64_t s0, double& zdthyd, int& nbad) {
