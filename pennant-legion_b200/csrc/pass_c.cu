@@ -16,11 +16,13 @@ namespace {
 
 // ---------------------------------------------------------------------
 // Pass C over row tiles of a rect mesh (row_tiles.cuh): per tile of up to
-// kRowT zones, the bottom and top point rows of px0, pu0, px, pu, the
-// tile's sfp + sfq and four zone fields arrive by bulk copies; the BC plane
-// masks are read from global memory (two bytes a point, cached).  64 zones
-// and two stages a CTA: 1920^2 Sedov 0.164 ms, against 0.168 ms with 128
-// zones, 0.205-0.227 ms with three stages and 0.173 ms for the staged
+// kRowT zones, the bottom and top point rows of px0, pu0, px, pu and four
+// zone fields arrive by bulk copies; each thread reads its zone's sfp + sfq
+// (64 contiguous bytes) and the BC plane masks (two bytes a point, cached)
+// from global memory.  64 zones and two stages a CTA, shared memory for 10
+// CTAs an SM: 1920^2 Sedov 0.149 ms, against 0.163 ms with sfp + sfq in the
+// stages (7 CTAs an SM), 0.152 ms with the zone fields also from global
+// memory, 0.174-0.185 ms with three stages and 0.173 ms for the staged
 // gathers.
 // ---------------------------------------------------------------------
 #ifndef PNT_ROWS_C_T
@@ -32,8 +34,7 @@ namespace {
 constexpr int kRowT = PNT_ROWS_C_T;
 constexpr int kRowStages = PNT_ROWS_C_STAGES;
 constexpr int kRowRB = (kRowT + 1) * 16;               // one point row of a double2 field
-constexpr int kRowOffSf = 8 * kRowRB;                  // [X0 b,t][U0 b,t][X b,t][U b,t], then sfp + sfq
-constexpr int kRowOffZs = kRowOffSf + 64 * kRowT;      // zm, zetot, zvol, zp: kRowT + 2 each
+constexpr int kRowOffZs = 8 * kRowRB;                  // [X0 b,t][U0 b,t][X b,t][U b,t], then zm, zetot, zvol, zp: kRowT + 2 each
 constexpr int kRowZB = (kRowT + 2) * 8;
 constexpr int kRowStageBytes = kRowOffZs + 4 * kRowZB;
 constexpr int kRowSmemBytes = kRowStages * kRowStageBytes;
@@ -53,9 +54,8 @@ struct RowIn {
     __device__ __forceinline__ double2 u0(int k) const { return *f(1, k); }
     __device__ __forceinline__ double2 x(int k) const { return *f(2, k); }
     __device__ __forceinline__ double2 u(int k) const { return *f(3, k); }
-    __device__ __forceinline__ double2 sf(int k) const {
-        return reinterpret_cast<const double2*>(st + kRowOffSf)[4 * t + k];
-    }
+    const double2* sfg;   // the zone's sfp + sfq (global memory)
+    __device__ __forceinline__ double2 sf(int k) const { return sfg[k]; }
     __device__ __forceinline__ unsigned mask(int k) const { return __ldg(bcmask + pb + row(k) * npx + col(k)); }
     __device__ __forceinline__ double zs(int fld) const {
         return reinterpret_cast<const double*>(st + kRowOffZs + fld * kRowZB)[shift + t];
@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(kRowT) pass_c_rows(DevArrays a, HydroConst c) 
     auto bytes = [&](int64_t g) -> uint32_t {
         const rows::Tile tl = rows::tile_of<kRowT>(g, nzx);
         const rows::ZoneRun zr = rows::zone_run(tl);
-        return (uint32_t)(8 * (tl.nt + 1) * 16 + 64 * tl.nt + 4 * zr.count * 8);
+        return (uint32_t)(8 * (tl.nt + 1) * 16 + 4 * zr.count * 8);
     };
     auto issue = [&](unsigned char* st, int64_t g, uint32_t bar) {
         const rows::Tile tl = rows::tile_of<kRowT>(g, nzx);
@@ -99,7 +99,6 @@ __global__ void __launch_bounds__(kRowT) pass_c_rows(DevArrays a, HydroConst c) 
             rows::bulk_g2s(st + (2 * f) * kRowRB, fields[f] + tl.pb, rb, bar);
             rows::bulk_g2s(st + (2 * f + 1) * kRowRB, fields[f] + tl.pb + npx, rb, bar);
         }
-        rows::bulk_g2s(st + kRowOffSf, a.sftot + 4 * tl.z0, (uint32_t)(64 * tl.nt), bar);
         const double* zf[4] = {a.zm, a.zetot, a.zvol, a.zp};
 #pragma unroll
         for (int f = 0; f < 4; ++f)
@@ -108,7 +107,7 @@ __global__ void __launch_bounds__(kRowT) pass_c_rows(DevArrays a, HydroConst c) 
     auto compute = [&](const unsigned char* st, int64_t g) {
         const rows::Tile tl = rows::tile_of<kRowT>(g, nzx);
         if (t >= tl.nt) return;
-        const RowIn in{st, a.bcmask, tl.pb, npx, t, (int)(tl.z0 & 1)};
+        const RowIn in{st, a.bcmask, tl.pb, npx, t, (int)(tl.z0 & 1), a.sftot + 4 * (tl.z0 + t)};
         const double d = stagedc::zone_core<true, kMixed>(a, c, 4, in, tl.z0 + t, dt, dtinv, nbad);
         dvm = (d > dvm) ? d : dvm;
     };
