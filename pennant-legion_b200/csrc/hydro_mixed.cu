@@ -182,8 +182,9 @@ struct SideSpill {
     double2* sfp_;
     float2* sft_;
     int t;
-    __device__ __forceinline__ double2& sfp(int k) const { return sfp_[k * kZoneThreadsZT + t]; }
-    __device__ __forceinline__ float2& sft(int k) const { return sft_[k * kZoneThreadsZT + t]; }
+    int stride = kZoneThreadsZT;   // threads of the CTA
+    __device__ __forceinline__ double2& sfp(int k) const { return sfp_[k * stride + t]; }
+    __device__ __forceinline__ float2& sft(int k) const { return sft_[k * stride + t]; }
 };
 
 // Where the learned cycle's pass A records a zone for the closure: record
@@ -796,26 +797,38 @@ __device__ __forceinline__ void closure_add_counts(const DevArrays& a, const uns
 
 // Pass A over row tiles of a rect mesh (row_tiles.cuh): the same zone body
 // reading its inputs from the tile's shared-memory stage, persistent CTAs,
-// two stages.  3 CTAs per SM (168 registers): at 1920^2 Sedov 0.239 ms for
-// the learned cycle against 0.247 ms at 4 CTAs (spills) and 0.258 ms for
-// the gathering kernel; three stages were slower (fewer resident CTAs).
+// two stages, 96-zone tiles and CTAs of 96 threads, 4 CTAs per SM (168
+// registers).  At 1920^2 Sedov the learned pass A takes 0.231 ms, against
+// 0.236 ms with 128-zone tiles (3 CTAs per SM), 0.236 ms with 64-zone tiles
+// (6 CTAs), 0.247-0.254 ms with 64-zone tiles held to 144 or 128 registers
+// (7 or 8 CTAs, spills) and 0.258 ms for the gathering kernel; three stages
+// were slower (fewer resident CTAs).
 #ifndef PNT_ROWS_A_STAGES
 #define PNT_ROWS_A_STAGES 2
 #endif
+#ifndef PNT_ROWS_A_T
+#define PNT_ROWS_A_T 96
+#endif
 #ifndef PNT_ROWS_A_MIN_BLOCKS
-#define PNT_ROWS_A_MIN_BLOCKS 3
+#define PNT_ROWS_A_MIN_BLOCKS 4
 #endif
 constexpr int kRowsAStages = PNT_ROWS_A_STAGES;
-using AStage = rows::PassAStage<kZoneThreadsZT>;
+constexpr int kRowsAT = PNT_ROWS_A_T;   // zones a tile, threads a CTA
+using AStage = rows::PassAStage<kRowsAT>;
 constexpr int kRowsASmem = kRowsAStages * AStage::kBytes;
 
 template <bool kLearned>
-__global__ void __launch_bounds__(kZoneThreadsZT, PNT_ROWS_A_MIN_BLOCKS) pass_a_mixed_rows(DevArrays a,
-                                                                                            HydroConst c) {
+__global__ void
+#ifdef PNT_ROWS_A_MAXREG
+    __maxnreg__(PNT_ROWS_A_MAXREG)
+#else
+    __launch_bounds__(kRowsAT, PNT_ROWS_A_MIN_BLOCKS)
+#endif
+    pass_a_mixed_rows(DevArrays a, HydroConst c) {
     extern __shared__ __align__(128) unsigned char smem_a[];
     __shared__ __align__(8) uint64_t bars[kRowsAStages];
-    __shared__ double2 s_sfp[4 * kZoneThreadsZT];
-    __shared__ float2 s_sft[4 * kZoneThreadsZT];
+    __shared__ double2 s_sfp[4 * kRowsAT];
+    __shared__ float2 s_sft[4 * kRowsAT];
     pdl_wait();
     const Ctl* ctl = a.ctl;
     if (skip_cycle(ctl)) return;
@@ -823,21 +836,21 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_ROWS_A_MIN_BLOCKS) pass_a_
     const double dt = ctl->dt;
     const int32_t nzx = a.rect_nzx;
     const int64_t npx = (int64_t)nzx + 1;
-    const int64_t ntiles = rows::num_tiles<kZoneThreadsZT>(nzx, a.numz);
+    const int64_t ntiles = rows::num_tiles<kRowsAT>(nzx, a.numz);
     const int t = threadIdx.x;
-    const SideSpill sp{s_sfp, s_sft, t};
+    const SideSpill sp{s_sfp, s_sft, t, kRowsAT};
     double zdthyd = 1.e99;
     int bad = 0;
     int cnt[3] = {0, 0, 0};
     const RecSink sink{a.closure_nrec, reinterpret_cast<float4*>(a.closure_rec), 0x7fffffff};
-    auto bytes = [&](int64_t g) { return AStage::bytes(rows::tile_of<kZoneThreadsZT>(g, nzx)); };
+    auto bytes = [&](int64_t g) { return AStage::bytes(rows::tile_of<kRowsAT>(g, nzx)); };
     auto issue = [&](unsigned char* st, int64_t g, uint32_t bar) {
-        AStage::issue(st, a, cur, rows::tile_of<kZoneThreadsZT>(g, nzx), npx, bar);
+        AStage::issue(st, a, cur, rows::tile_of<kRowsAT>(g, nzx), npx, bar);
     };
     auto compute = [&](const unsigned char* st, int64_t g) {
-        const rows::Tile tl = rows::tile_of<kZoneThreadsZT>(g, nzx);
+        const rows::Tile tl = rows::tile_of<kRowsAT>(g, nzx);
         if (t >= tl.nt) return;
-        const rows::RowZoneIn<kZoneThreadsZT> in{st, t, (int)(tl.z0 & 1)};
+        const rows::RowZoneIn<kRowsAT> in{st, t, (int)(tl.z0 & 1)};
         const int64_t z = tl.z0 + t;
         double v = 1.e99;
         int zc[3] = {0, 0, 0};   // the zone's own corner classes (an acute zone overwrites them)
@@ -848,23 +861,23 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_ROWS_A_MIN_BLOCKS) pass_a_
     };
     if (!rows::for_tiles<kRowsAStages, AStage::kBytes>(ntiles, smem_a, bars, bytes, issue, compute) && t == 0)
         atomicOr(reinterpret_cast<unsigned long long*>(a.cyc_red + 4), 1ull);
-    __shared__ unsigned wcount[kLearned ? kZoneThreadsZT / 32 : 1][3];
+    __shared__ unsigned wcount[kLearned ? kRowsAT / 32 : 1][3];
     if constexpr (kLearned) {
         for (int q = 0; q < 3; ++q) {
             const unsigned tt = __reduce_add_sync(kFull, (unsigned)cnt[q]);
             if ((threadIdx.x & 31) == 0) wcount[threadIdx.x >> 5][q] = tt;
         }
     }
-    const int nbad = tiles::block_isum<kZoneThreadsZT>(bad);   // its barrier also orders wcount
+    const int nbad = tiles::block_isum<kRowsAT>(bad);   // its barrier also orders wcount
     if constexpr (kLearned) {
         constexpr int kCounted[3] = {kClassZero, kClassDead, kClassAcute};
         if (threadIdx.x < 3) {
             unsigned tt = 0;
-            for (int w = 0; w < kZoneThreadsZT / 32; ++w) tt += wcount[w][threadIdx.x];
+            for (int w = 0; w < kRowsAT / 32; ++w) tt += wcount[w][threadIdx.x];
             if (tt) atomicAdd(a.closure_counts + kCounted[threadIdx.x] * 64 + (blockIdx.x & 63), (unsigned long long)tt);
         }
     }
-    fp64::block_to_cycle<true, kZoneThreadsZT>(a.cyc_red, zdthyd, nbad);
+    fp64::block_to_cycle<true, kRowsAT>(a.cyc_red, zdthyd, nbad);
 }
 
 // ---------------------------------------------------------------------
@@ -997,8 +1010,8 @@ cudaError_t launch_cycle_mixed_impl(const DevArrays& a, const HydroConst& c, cud
     if (phases & kPhaseForces) {
         if (ev) cudaEventRecord(ev[0], stream);
         if (a.rect_nzx > 0) {
-            chk(launch_pdl(learned ? pass_a_mixed_rows<true> : pass_a_mixed_rows<false>, a.gridA, kZoneThreadsZT,
-                           kRowsASmem, stream, a, c));
+            chk(launch_pdl(learned ? pass_a_mixed_rows<true> : pass_a_mixed_rows<false>, a.gridA, kRowsAT, kRowsASmem,
+                           stream, a, c));
         } else {
             auto k = learned ? (a.quads ? pass_a_mixed_zt<true, true> : pass_a_mixed_zt<false, true>)
                              : (a.quads ? pass_a_mixed_zt<true, false> : pass_a_mixed_zt<false, false>);
@@ -1031,9 +1044,9 @@ cudaError_t launch_cycle_learned(const DevArrays& a, const HydroConst& c, cudaSt
 }
 
 cudaError_t prepare_pass_a_rows_mixed(bool learned, int32_t rect_nzx, int32_t numz, int nsm, int32_t* grid) {
-    const int64_t nt = rows::num_tiles<kZoneThreadsZT>(rect_nzx, numz);
-    return learned ? rows::prepare(pass_a_mixed_rows<true>, kZoneThreadsZT, kRowsASmem, nt, nsm, grid)
-                   : rows::prepare(pass_a_mixed_rows<false>, kZoneThreadsZT, kRowsASmem, nt, nsm, grid);
+    const int64_t nt = rows::num_tiles<kRowsAT>(rect_nzx, numz);
+    return learned ? rows::prepare(pass_a_mixed_rows<true>, kRowsAT, kRowsASmem, nt, nsm, grid)
+                   : rows::prepare(pass_a_mixed_rows<false>, kRowsAT, kRowsASmem, nt, nsm, grid);
 }
 
 void launch_batch_pass_a_mixed(const BatchDev& b, bool all_quads, cudaStream_t stream) {
