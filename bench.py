@@ -59,8 +59,8 @@ MLP_FLOP_PER_ROW = 2 * (16 * 64 + 64 * 64 + 64 * 16)   # tensor-core MMA shapes,
 # captures of profiles/pass_a_rows_learned_sedov1024.md (learned, mixed)
 # and profiles/pass_a_fp64_sedov1024.md (FP64), 1,048,576 zones each; the
 # bench scales them by its zone count
-PASS_A_TRAFFIC_PER_ZONE = {"learned": (109.737e6 + 88.343e6) / 1048576,
-                           "mixed": (109.363e6 + 76.074e6) / 1048576,
+PASS_A_TRAFFIC_PER_ZONE = {"learned": (109.723e6 + 81.982e6) / 1048576,
+                           "mixed": (109.362e6 + 76.070e6) / 1048576,
                            "fp64": (125.973e6 + 130.137e6) / 1048576}
 
 
