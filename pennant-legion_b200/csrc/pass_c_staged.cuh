@@ -39,17 +39,20 @@ constexpr int kStages = PNT_STAGED_C_STAGES;   // tiles resident per CTA
 static_assert(kTile % 32 == 0 && kStages >= 1, "tile of whole warps");
 
 // Bytes of one stage per zone: per side x0.x (8), u0 (16), x (16), u (16),
-// sftot (16), the 32-bit bcmask word holding the point's mask (4); per zone
-// zm, zetot, zvol, zp (32).
+// the 32-bit bcmask word holding the point's mask (4); per zone zm, zetot,
+// zvol, zp (32), the side count and mask parities (4) and the first side
+// (4).  The sides' sfp + sfq (64 contiguous bytes a quad zone) are read from
+// global memory where they are used: the smaller stage holds 12 CTAs an SM
+// instead of 10.
 constexpr int kOffX0x = 0;
 constexpr int kOffU0 = kOffX0x + 4 * 8 * kTile;
 constexpr int kOffX = kOffU0 + 4 * 16 * kTile;
 constexpr int kOffU = kOffX + 4 * 16 * kTile;
-constexpr int kOffSf = kOffU + 4 * 16 * kTile;
-constexpr int kOffMw = kOffSf + 4 * 16 * kTile;
+constexpr int kOffMw = kOffU + 4 * 16 * kTile;
 constexpr int kOffZs = kOffMw + 4 * 4 * kTile;
 constexpr int kOffMeta = kOffZs + 4 * 8 * kTile;
-constexpr int kStageBytes = kOffMeta + 4 * kTile;
+constexpr int kOffS0 = kOffMeta + 4 * kTile;
+constexpr int kStageBytes = kOffS0 + 4 * kTile;
 constexpr int kSmemBytes = kStages * kStageBytes;
 
 using tiles::cp16;
@@ -77,7 +80,6 @@ __device__ __forceinline__ void issue(const DevArrays& a, int cur, unsigned char
             cp16(st + kOffU0 + (k * kTile + t) * 16, pu0 + p);
             cp16(st + kOffX + (k * kTile + t) * 16, px1 + p);
             cp16(st + kOffU + (k * kTile + t) * 16, pu1 + p);
-            cp16(st + kOffSf + (k * kTile + t) * 16, a.sftot + ix.s0 + k);
             cp4(st + kOffMw + (k * kTile + t) * 4, mw + (p >> 1));
             meta |= (p & 1) << (4 + k);
         }
@@ -87,6 +89,7 @@ __device__ __forceinline__ void issue(const DevArrays& a, int cur, unsigned char
     cp8(st + kOffZs + (2 * kTile + t) * 8, a.zvol + z);
     cp8(st + kOffZs + (3 * kTile + t) * 8, a.zp + z);
     reinterpret_cast<int*>(st + kOffMeta)[t] = meta;
+    reinterpret_cast<int*>(st + kOffS0)[t] = ix.s0;
 }
 
 __device__ __forceinline__ double2 mk2(double x, double y) { return make_double2(x, y); }
@@ -186,10 +189,12 @@ __device__ __forceinline__ double zone_core(const DevArrays& a, const HydroConst
     return fabs((zvol - zvol0) / zvol0);
 }
 
-// The staged layout above, slot t of stage st.
+// The staged layout above, slot t of stage st; sfg: the zone's sfp + sfq
+// (global memory).
 struct StagedIn {
     const unsigned char* st;
     int t, meta;
+    const double2* sfg;
     __device__ __forceinline__ double2 x(int k) const {
         return reinterpret_cast<const double2*>(st + kOffX)[k * kTile + t];
     }
@@ -202,9 +207,7 @@ struct StagedIn {
     __device__ __forceinline__ double x0x(int k) const {
         return reinterpret_cast<const double*>(st + kOffX0x)[k * kTile + t];
     }
-    __device__ __forceinline__ double2 sf(int k) const {
-        return reinterpret_cast<const double2*>(st + kOffSf)[k * kTile + t];
-    }
+    __device__ __forceinline__ double2 sf(int k) const { return sfg[k]; }
     __device__ __forceinline__ unsigned mask(int k) const {
         const uint32_t w = reinterpret_cast<const uint32_t*>(st + kOffMw)[k * kTile + t];
         return (w >> (((meta >> (4 + k)) & 1) * 16)) & 0xffffu;
@@ -221,7 +224,7 @@ template <bool kQuads, bool kMixed>
 __device__ __forceinline__ double zone(const DevArrays& a, const HydroConst& c, const unsigned char* st, int t,
                                        int64_t z, double dt, double dtinv, int& nbad) {
     const int meta = reinterpret_cast<const int*>(st + kOffMeta)[t];
-    const StagedIn in{st, t, meta};
+    const StagedIn in{st, t, meta, a.sftot + reinterpret_cast<const int*>(st + kOffS0)[t]};
     return zone_core<kQuads, kMixed>(a, c, meta & 15, in, z, dt, dtinv, nbad);
 }
 
