@@ -8,9 +8,11 @@
 // sfq, and per zone four scalars.  Loaded straight into registers by four
 // lanes per zone (a chain of two dependent memory latencies, ~36 shuffles
 // per lane) it ran at 31% of peak DRAM throughput; here the zone-tile
-// driver of zone_tiles.cuh stages them in shared memory, one thread per
-// zone.  On the B200 more resident CTAs beat deeper pipelines (1024^2
-// Sedov: 1 stage and 10 CTAs of 64 per SM 56 us, 2 stages 59 us, 3 stages
+// driver of zone_tiles.cuh stages the gathered point data and the zone
+// scalars in shared memory, one thread per zone, and each thread reads its
+// sides' sfp + sfq (contiguous) from global memory.  On the B200 more
+// resident CTAs beat deeper pipelines (1024^2 Sedov, with sfp + sfq still
+// staged: 1 stage and 10 CTAs of 64 per SM 56 us, 2 stages 59 us, 3 stages
 // 72 us), so the default is one stage.
 //
 // The zone arithmetic is the four-lane pass C's, one zone per thread:

@@ -113,6 +113,20 @@ def test_rect_numbering_matches_reference_layout():
     np.testing.assert_array_equal(m.array("px")[6], [2.0, 1.0])
 
 
+@pytest.mark.parametrize("params", ["3 2 3.0 2.0", "1 5", "7 1", "16 9 1.0 2.0"])
+def test_rect_point_indices_follow_from_the_zone_index(params):
+    """The FP64 pass A and the batch read a rect mesh's points without
+    mapsp1: side 4z + k of zone z = (i, j) starts at point
+    j (nzx + 1) + i + {0, 1, nzx + 2, nzx + 1}[k].  Checked against the
+    mesh's own mapsp1 for every zone."""
+    m = pb.Mesh(deck=pb.Deck(text=f"cstop 1\nmeshtype rect\nmeshparams {params}\n"))
+    nzx = int(params.split()[0])
+    z = np.arange(m.numz)
+    p0 = (z // nzx) * (nzx + 1) + z % nzx
+    want = p0[:, None] + np.array([0, 1, nzx + 2, nzx + 1])[None, :]
+    np.testing.assert_array_equal(m.array("mapsp1").reshape(-1, 4), want)
+
+
 def test_pie_mesh_structure():
     m = pb.Mesh(deck=pb.Deck(path=golden("nohsmall.pnt")))   # pie 2 x 20
     z = m.array("znump")
