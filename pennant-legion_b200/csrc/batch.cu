@@ -58,7 +58,10 @@ __global__ void __launch_bounds__(kBatchZT, 3) batch_pass_a(BatchDev b) {
             const int64_t z = (int64_t)zb + threadIdx.x;
             if (z >= tile.end) continue;
             double v = 1.e99;
-            if (kAllQuads || tile.quads) {
+            if (tile.nzx > 0) {   // a rect instance: point indices from the zone index
+                const RectZoneIn in(b.a, cur, z, tile.nzx, z - tile.zo, tile.po);
+                pass_a_zone_thread<4>(b.a, c, in, dt, z, 4 * z, v, nbad);
+            } else if (kAllQuads || tile.quads) {
                 pass_a_zone_thread<4>(b.a, c, cur, dt, z, 4 * z, v, nbad);
             } else {
                 const int n = b.a.znump[z];
@@ -202,6 +205,7 @@ struct pnt_batch {
     std::vector<int64_t> zoff, poff, soff;      // instance offsets (host)
     std::vector<int32_t> nz, np, ns;
     std::vector<int32_t> quads;
+    std::vector<int32_t> rect_nzx;               // zones a row of a rect-numbered quad instance (else 0)
     bool all_quads = false;                      // every instance: quads at sides 4z..4z+3
     bool mixed = false;                          // the mixed-precision cycle (every instance)
     Ctl* ctl_host = nullptr;                     // pinned [ninst]
@@ -263,7 +267,7 @@ struct pnt_batch {
             ++nlive;
             for (int64_t z = 0; z < nz[i]; z += sh.zones_per_tile)
                 zt.push_back({i, (int32_t)(zoff[i] + z), (int32_t)(zoff[i] + std::min<int64_t>(nz[i], z + sh.zones_per_tile)),
-                              quads[i]});
+                              quads[i], rect_nzx[i], (int32_t)zoff[i], (int32_t)poff[i], 0});
             for (int64_t p = 0; p < np[i]; p += ppt)
                 pt.push_back({i, (int32_t)(poff[i] + p), (int32_t)(poff[i] + std::min<int64_t>(np[i], p + ppt)), quads[i]});
         }
@@ -495,6 +499,7 @@ pnt_status pnt_batch_create(const pnt_mesh* const* meshes, const pnt_params* par
             // the quad fast path indexes sides as 4z, which holds while every
             // earlier instance is all-quad too
             bt->quads.push_back(m.all_quads && NS == 4 * NZ ? 1 : 0);
+            bt->rect_nzx.push_back(bt->quads.back() ? m.rect_nzx : 0);
             NZ += m.numz;
             NP += m.nump;
             NS += m.nums;

@@ -14,6 +14,10 @@ struct Tile {
     int32_t beg;    // first zone (zone tiles) or point (point tiles), global
     int32_t end;    // one past the last
     int32_t quads;  // the instance's zones are all quads at sides 4z..4z+3
+    int32_t nzx;    // zone tiles of a quad instance numbered as the rect generator numbers it: zones a row (else 0)
+    int32_t zo;     // the instance's first zone and first point (global)
+    int32_t po;
+    int32_t pad;
 };
 
 struct BatchDev {

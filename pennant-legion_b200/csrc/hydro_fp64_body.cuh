@@ -246,11 +246,16 @@ struct RectZoneIn {
     const DevArrays& a;
     int cur;
     int64_t z, s0, p0, npx;
-    __device__ __forceinline__ RectZoneIn(const DevArrays& a_, int cur_, int64_t z_)
-        : a(a_), cur(cur_), z(z_), s0(4 * z_), npx((int64_t)a_.rect_nzx + 1) {
-        const int64_t zj = z_ / a_.rect_nzx;
-        p0 = zj * npx + (z_ - zj * a_.rect_nzx);
+    // zone z (global) of a rect mesh of nzx zones a row whose zone zl and
+    // point 0 are the global zone z and point po (one mesh: zl = z, po = 0)
+    __device__ __forceinline__ RectZoneIn(const DevArrays& a_, int cur_, int64_t z_, int32_t nzx, int64_t zl,
+                                          int64_t po)
+        : a(a_), cur(cur_), z(z_), s0(4 * z_), npx((int64_t)nzx + 1) {
+        const int64_t zj = zl / nzx;
+        p0 = po + zj * npx + (zl - zj * nzx);
     }
+    __device__ __forceinline__ RectZoneIn(const DevArrays& a_, int cur_, int64_t z_)
+        : RectZoneIn(a_, cur_, z_, a_.rect_nzx, z_, 0) {}
     __device__ __forceinline__ int64_t p(int k) const {
         return p0 + (k == 1 ? 1 : (k == 2 ? npx + 1 : (k == 3 ? npx : 0)));
     }
