@@ -78,13 +78,14 @@ __global__ void __launch_bounds__(kZoneThreadsZT, PNT_PASS_A_ZT_MIN_BLOCKS) pass
     block_to_cycle<true, kZoneThreadsZT>(a.cyc_red, zdthyd, nbad);
 }
 
+template <bool kRect>
 __global__ void __launch_bounds__(kPointThreads) pass_b(DevArrays a, HydroConst c) {
     pdl_wait();
     const Ctl* ctl = a.ctl;
     if (skip_cycle(ctl)) return;
     const int64_t p = (int64_t)blockIdx.x * kPointThreads + threadIdx.x;
     if (p >= a.nump) return;
-    pass_b_point(a, c, ctl->cycle & 1, ctl->dt, p);
+    pass_b_point<kRect>(a, c, ctl->cycle & 1, ctl->dt, p);
 }
 
 // Multi-piece runs: the corner values the neighbours need, and the end of
@@ -138,7 +139,8 @@ cudaError_t launch_cycle_fp64(const DevArrays& a, const HydroConst& c, cudaStrea
         if (ev) cudaEventRecord(ev[2], stream);   // no closure pass
     }
     if (phases & kPhaseAdvance) {
-        const cudaError_t eb = launch_pdl(pass_b, pb, kPointThreads, 0, stream, a, c);
+        const cudaError_t eb =
+            launch_pdl(a.rect_nzx > 0 ? pass_b<true> : pass_b<false>, pb, kPointThreads, 0, stream, a, c);
         if (e == cudaSuccess) e = eb;
         if (ev) cudaEventRecord(ev[3], stream);
         launch_pass_c(a, c, false, stream);   // its last CTA ends the cycle

@@ -441,19 +441,57 @@ __device__ __forceinline__ void advance_point(const HydroConst& c, double dt, un
            __dadd_rn(x0.y, __dmul_rn(__dadd_rn(u0.y, u.y), dth)));
 }
 
+// The corners of point p = (i, j) of a rect mesh (nzx zones a row, nzy
+// rows) in ascending side order, as the point-to-corner CSR lists them:
+// side 2 of the zone below-left, 3 of the zone below, 1 of the zone to the
+// left, 0 of the zone (sides 4z + k start at (i, j), (i+1, j), (i+1, j+1),
+// (i, j+1)).  With Z the zone below-left these are 4Z + 2 < 4Z + 7 <
+// 4(Z + nzx) + 1 < 4(Z + nzx + 1) when all four exist (nzx >= 2); a point
+// on the boundary keeps the same order over fewer.  Returns their count.
+__device__ __forceinline__ int rect_point_corners(int32_t nzx, int32_t nzy, int64_t p, int64_t* s) {
+    const int64_t npx = (int64_t)nzx + 1;
+    const int64_t j = p / npx, i = p - j * npx;
+    int n = 0;
+    if (j > 0) {
+        if (i > 0) s[n++] = 4 * ((j - 1) * nzx + i - 1) + 2;
+        if (i < nzx) s[n++] = 4 * ((j - 1) * nzx + i) + 3;
+    }
+    if (j < nzy) {
+        if (i > 0) s[n++] = 4 * (j * nzx + i - 1) + 1;
+        if (i < nzx) s[n++] = 4 * (j * nzx + i);
+    }
+    return n;
+}
+
+// kRect: a rect mesh (a.rect_nzx > 0), the point's corners from its index
+// instead of the CSR (the same sides in the same order).
+template <bool kRect = false>
 __device__ __forceinline__ void pass_b_point(const DevArrays& a, const HydroConst& c, int cur, double dt,
                                              int64_t p) {
     const double2 x0 = a.px[cur][p];
     const double2 u0 = a.pu[cur][p];
     // corner mass and force, ascending side order from zero (Hydro.cc:1100-1116, :1175-1192)
-    const int32_t o0 = a.poff[p], o1 = a.poff[p + 1];
     double m = 0.;
     double2 f = mk(0., 0.);
-    for (int32_t i = o0; i < o1; ++i) {
-        const int32_t s = __ldg(a.pcorner + i);
-        m = __dadd_rn(m, a.cmass[s]);
-        const double2 cf = a.cforce[s];
-        f = mk(__dadd_rn(f.x, cf.x), __dadd_rn(f.y, cf.y));
+    if (kRect) {
+        int64_t sc[4];
+        const int n = rect_point_corners(a.rect_nzx, a.numz / a.rect_nzx, p, sc);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (q < n) {
+                m = __dadd_rn(m, a.cmass[sc[q]]);
+                const double2 cf = a.cforce[sc[q]];
+                f = mk(__dadd_rn(f.x, cf.x), __dadd_rn(f.y, cf.y));
+            }
+        }
+    } else {
+        const int32_t o0 = a.poff[p], o1 = a.poff[p + 1];
+        for (int32_t i = o0; i < o1; ++i) {
+            const int32_t s = __ldg(a.pcorner + i);
+            m = __dadd_rn(m, a.cmass[s]);
+            const double2 cf = a.cforce[s];
+            f = mk(__dadd_rn(f.x, cf.x), __dadd_rn(f.y, cf.y));
+        }
     }
     double2 x, u;
     advance_point(c, dt, a.bcmask[p], m, f, x0, u0, x, u);

@@ -883,18 +883,34 @@ __global__ void
 // ---------------------------------------------------------------------
 // Pass B, mixed: FP32 corner inputs summed in FP64
 // ---------------------------------------------------------------------
+// kRect: a rect mesh, the point's corners from its index
+// (fp64::rect_point_corners: the CSR's sides in the CSR's order).
+template <bool kRect = false>
 __device__ __forceinline__ void pass_b_mixed_point(const DevArrays& a, const HydroConst& c, int cur, double dt,
                                                    int64_t p) {
     const double2 x0 = a.px[cur][p];
     const double2 u0 = a.pu[cur][p];
-    const int32_t o0 = a.poff[p], o1 = a.poff[p + 1];
     double m = 0.;
     double2 f = mk(0., 0.);
-    for (int32_t i = o0; i < o1; ++i) {
-        const int32_t s = __ldg(a.pcorner + i);
-        m = __dadd_rn(m, (double)a.cmass_f[s]);
-        const float2 cf = a.cforce_f[s];
-        f = mk(__dadd_rn(f.x, (double)cf.x), __dadd_rn(f.y, (double)cf.y));
+    if (kRect) {
+        int64_t sc[4];
+        const int n = fp64::rect_point_corners(a.rect_nzx, a.numz / a.rect_nzx, p, sc);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (q < n) {
+                m = __dadd_rn(m, (double)a.cmass_f[sc[q]]);
+                const float2 cf = a.cforce_f[sc[q]];
+                f = mk(__dadd_rn(f.x, (double)cf.x), __dadd_rn(f.y, (double)cf.y));
+            }
+        }
+    } else {
+        const int32_t o0 = a.poff[p], o1 = a.poff[p + 1];
+        for (int32_t i = o0; i < o1; ++i) {
+            const int32_t s = __ldg(a.pcorner + i);
+            m = __dadd_rn(m, (double)a.cmass_f[s]);
+            const float2 cf = a.cforce_f[s];
+            f = mk(__dadd_rn(f.x, (double)cf.x), __dadd_rn(f.y, (double)cf.y));
+        }
     }
     double2 x, u;
     fp64::advance_point(c, dt, a.bcmask[p], m, f, x0, u0, x, u);
@@ -902,13 +918,14 @@ __device__ __forceinline__ void pass_b_mixed_point(const DevArrays& a, const Hyd
     a.pu[cur ^ 1][p] = u;
 }
 
+template <bool kRect>
 __global__ void __launch_bounds__(kPointThreads) pass_b_mixed(DevArrays a, HydroConst c) {
     pdl_wait();
     const Ctl* ctl = a.ctl;
     if (skip_cycle(ctl)) return;
     const int64_t p = (int64_t)blockIdx.x * kPointThreads + threadIdx.x;
     if (p >= a.nump) return;
-    pass_b_mixed_point(a, c, ctl->cycle & 1, ctl->dt, p);
+    pass_b_mixed_point<kRect>(a, c, ctl->cycle & 1, ctl->dt, p);
 }
 
 // ---------------------------------------------------------------------
@@ -1022,7 +1039,8 @@ cudaError_t launch_cycle_mixed_impl(const DevArrays& a, const HydroConst& c, cud
         if (ev) cudaEventRecord(ev[2], stream);
     }
     if (phases & kPhaseAdvance) {
-        chk(launch_pdl(pass_b_mixed, pb, kPointThreads, 0, stream, a, c));
+        chk(launch_pdl(a.rect_nzx > 0 ? pass_b_mixed<true> : pass_b_mixed<false>, pb, kPointThreads, 0, stream, a,
+                       c));
         if (ev) cudaEventRecord(ev[3], stream);
         launch_pass_c(a, c, true, stream);   // its last CTA ends the cycle
         if (ev) cudaEventRecord(ev[4], stream);

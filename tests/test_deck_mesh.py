@@ -127,6 +127,33 @@ def test_rect_point_indices_follow_from_the_zone_index(params):
     np.testing.assert_array_equal(m.array("mapsp1").reshape(-1, 4), want)
 
 
+@pytest.mark.parametrize("params", ["3 2 3.0 2.0", "1 5", "7 1", "16 9 1.0 2.0"])
+def test_rect_point_corners_follow_from_the_point_index(params):
+    """The point passes read a rect mesh's corners without the CSR: point
+    (i, j) gathers side 2 of the zone below-left, 3 of the zone below, 1 of
+    the zone to the left and 0 of its own zone, those that exist, in that
+    order.  Checked against the mesh's CSR (ascending side order) for every
+    point."""
+    m = pb.Mesh(deck=pb.Deck(text=f"cstop 1\nmeshtype rect\nmeshparams {params}\n"))
+    nzx = int(params.split()[0])
+    nzy = m.numz // nzx
+    off, sides = m.point_corners()
+    for p in range(m.nump):
+        j, i = divmod(p, nzx + 1)
+        want = []
+        if j > 0:
+            if i > 0:
+                want.append(4 * ((j - 1) * nzx + i - 1) + 2)
+            if i < nzx:
+                want.append(4 * ((j - 1) * nzx + i) + 3)
+        if j < nzy:
+            if i > 0:
+                want.append(4 * (j * nzx + i - 1) + 1)
+            if i < nzx:
+                want.append(4 * (j * nzx + i))
+        assert list(sides[off[p]:off[p + 1]]) == want, (p, i, j)
+
+
 def test_pie_mesh_structure():
     m = pb.Mesh(deck=pb.Deck(path=golden("nohsmall.pnt")))   # pie 2 x 20
     z = m.array("znump")
