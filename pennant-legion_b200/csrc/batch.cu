@@ -222,6 +222,7 @@ struct pnt_batch {
     cudaGraphExec_t graph = nullptr;
     int graph_cycles = 8;
     int32_t live = 0;                            // instances in the current work lists
+    std::vector<char> listed;                    // [ninst] the instance is in the current work lists
 
     ~pnt_batch() {
         int prev = -1;
@@ -261,10 +262,12 @@ struct pnt_batch {
         std::vector<int32_t> tb(ninst + 1, 0);
         const int ppt = kBatchThreads * 4;   // points per point tile
         int32_t nlive = 0;
+        listed.assign(ninst, 0);
         for (int i = 0; i < ninst; ++i) {
             tb[i] = (int32_t)zt.size();
             if (ctl_host[i].done) continue;
             ++nlive;
+            listed[i] = 1;
             for (int64_t z = 0; z < nz[i]; z += sh.zones_per_tile)
                 zt.push_back({i, (int32_t)(zoff[i] + z), (int32_t)(zoff[i] + std::min<int64_t>(nz[i], z + sh.zones_per_tile)),
                               quads[i], rect_nzx[i], (int32_t)zoff[i], (int32_t)poff[i], 0});
@@ -363,6 +366,21 @@ struct pnt_batch {
         CUDA_TRY(cudaStreamSynchronize(stream));
         *out = *running_host;
         return PNT_OK;
+    }
+
+    // Share of the listed zones that belong to finished instances (ctl_host
+    // current).  Their tiles cost little (each CTA sees the instance done
+    // and returns), so the lists are rebuilt only once they hold a quarter
+    // of the listed zones: every rebuild drains the stream, reallocates the
+    // lists and captures a new graph.
+    double finished_share() const {
+        int64_t all = 0, fin = 0;
+        for (int i = 0; i < ninst; ++i) {
+            if (i >= (int)listed.size() || !listed[i]) continue;
+            all += nz[i];
+            if (ctl_host[i].done) fin += nz[i];
+        }
+        return all > 0 ? (double)fin / (double)all : 0.;
     }
 
     pnt_status fetch_ctls() {
@@ -704,8 +722,10 @@ pnt_status pnt_batch_run(pnt_batch* bt, int32_t max_cycles, int32_t* running_lef
     int running = 0;
     pnt_status st = bt->running(&running);
     while (!st && running > 0 && (max_cycles <= 0 || done_cycles < max_cycles)) {
-        // drop finished instances from the work lists
-        if (running < bt->live && (st = bt->fetch_ctls()) == PNT_OK) st = bt->build_tiles(bt->shape);
+        // drop finished instances from the work lists once they hold a
+        // quarter of the listed zones
+        if (running < bt->live && (st = bt->fetch_ctls()) == PNT_OK && bt->finished_share() >= 0.25)
+            st = bt->build_tiles(bt->shape);
         if (st) break;
         const int chunk = max_cycles > 0 ? (int)std::min<int64_t>(64, max_cycles - done_cycles) : 64;
         if ((st = bt->enqueue(chunk))) break;
